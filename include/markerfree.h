@@ -1,0 +1,192 @@
+/* markerfree.h — C ABI of the B200 projection-matching alignment library.
+ *
+ * The reference program (ratolon/Markerfree) has no library API: its boundary is
+ * the command line and the files (MRC stack, .rawtlt, .txt/.xf), and inside it the
+ * C++ classes PreProcess, Transform, CalcTIltAxis, FindOffset, ProjAlign and
+ * CorrTomoStack, which all mutate one shared AlignParam.  This header exposes the
+ * same units one-for-one over plain pointers and sizes, so that a host program
+ * (the bundled command-line tool, a ctypes/cffi binding, or another aligner) can
+ * drive the pipeline stage by stage or as a whole.
+ *
+ * Conventions
+ *  - Every function returns MF_OK (0) or a negative mf_status; the message of the
+ *    last failure on the calling thread is returned by mf_last_error().
+ *  - Host arrays are owned by the caller.  Device memory is owned by the library
+ *    (one mf_context per GPU, one stream per context).
+ *  - Images are row-major float32, x fastest; stacks are z-major (nz, ny, nx).
+ *  - Angles are degrees; shifts are in pixels of the un-binned input stack.
+ *  - A context is not thread-safe; use one context per host thread.
+ */
+#ifndef MARKERFREE_H
+#define MARKERFREE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MF_API __attribute__((visibility("default")))
+#else
+#define MF_API
+#endif
+
+typedef enum {
+  MF_OK = 0,
+  MF_ERR_ARG = -1,       /* invalid argument (size, null pointer, range) */
+  MF_ERR_CUDA = -2,      /* CUDA runtime error */
+  MF_ERR_CUFFT = -3,     /* cuFFT error */
+  MF_ERR_IO = -4,        /* file cannot be opened, read or written */
+  MF_ERR_FORMAT = -5,    /* unsupported MRC mode / malformed file */
+  MF_ERR_STATE = -6,     /* call out of order (e.g. DoIt before setup) */
+  MF_ERR_NOMEM = -7,     /* device or host allocation failed / budget exceeded */
+  MF_ERR_GEOMETRY = -8   /* no neighbouring tilt within range of a held-out tilt */
+} mf_status;
+
+/* AlignParam (Markerfree/src/method/Util.h:14-21): per-tilt shift and tilt-axis
+ * angle plus the global tilt-angle offset.  Arrays hold nz entries each. */
+typedef struct {
+  float* shift_x;
+  float* shift_y;
+  float* rotate;
+  float angle_offset;
+} mf_align_param;
+
+/* Command-line options that reach the alignment (Markerfree/src/main/opts.h:16-41,
+ * -g O,P,Z,T,A,B,G / -p / -s).  `thickness` (T) is parsed but unused, as in the
+ * reference. */
+typedef struct {
+  float offset;      /* O: tilt-angle offset; 0 = search it (FindOffset)        */
+  float pitch_angle; /* P: tilt-axis angle; 0 = search it (Transform+axis)      */
+  float zshift;      /* Z: initial rotation-centre z                            */
+  int thickness;     /* T: unused                                               */
+  int align_z;       /* A: slab thickness for projection matching; 0 = no align */
+  int out_bin;       /* B: binning of the output stack                          */
+  int gpu;           /* G: CUDA device ordinal                                  */
+  int nproj;         /* -p: neighbours back-projected per held-out tilt         */
+  int save_mode;     /* -s: 0 = .txt, 1 = .xf                                   */
+} mf_options;
+
+/* Precision of the re-projection operands (the corrected stack rows and the
+ * back-projection operator).  Accumulation is always FP32; peak fitting, shift
+ * accumulation and the rotation-centre normal equation are FP64. */
+typedef enum { MF_PREC_FP32 = 0, MF_PREC_BF16 = 1, MF_PREC_FP16 = 2 } mf_precision;
+
+typedef struct mf_context mf_context;
+typedef struct mf_series mf_series;
+
+/* ---- errors ------------------------------------------------------------- */
+MF_API const char* mf_last_error(void);
+MF_API const char* mf_version(void);
+
+/* ---- context (replaces main.cpp:26 cudaSetDevice and the per-class plans) - */
+MF_API int mf_context_create(int gpu, mf_context** out);
+MF_API void mf_context_destroy(mf_context* ctx);
+/* Blocks until all work queued on the context's stream has finished. */
+MF_API int mf_context_sync(mf_context* ctx);
+/* Count of library kernel launches issued on this context so far (graph
+ * launches count every kernel node once per replay). */
+MF_API int64_t mf_context_kernel_launches(mf_context* ctx);
+
+/* ---- series: device-resident pre-processed stack --------------------------
+ * Replaces Process::ReadStack + PreProcess::SetPositive/MassNormalization
+ * (Markerfree/src/main/Process.cpp:129-236, Markerfree/src/method/Preprocess.cu:103-177):
+ * the raw stack (file order) is reordered to ascending angles, made positive and
+ * mass-normalised on the GPU and kept in HBM in place of the scratch buf.mrc. */
+MF_API int mf_series_create(mf_context* ctx, const float* raw_stack, int nx, int ny, int nz,
+                            const float* file_angles, mf_series** out);
+/* Same, from a device buffer already holding the raw stack (file order). */
+MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw_stack, int nx, int ny,
+                                   int nz, const float* file_angles, mf_series** out);
+MF_API void mf_series_destroy(mf_series* s);
+MF_API int mf_series_set_precision(mf_series* s, mf_precision p);
+/* Copies the pre-processed stack (nz*ny*nx floats) to host memory. */
+MF_API int mf_series_get_stack(mf_series* s, float* host_out);
+/* Angles used by the alignment stages (ascending, offset applied by the caller). */
+MF_API int mf_series_set_angles(mf_series* s, const float* angles);
+MF_API int mf_series_get_angles(mf_series* s, float* angles_out);
+MF_API int mf_series_set_param(mf_series* s, const mf_align_param* p);
+MF_API int mf_series_get_param(mf_series* s, mf_align_param* p);
+
+/* ---- stages --------------------------------------------------------------- */
+/* Transform::Setup + DoIt (Markerfree/src/method/Transform.cpp:55-128): stretch
+ * cross-correlation of every tilt against its neighbour nearer zero tilt, shifts
+ * accumulated outward.  The series keeps the Transform state between calls. */
+MF_API int mf_transform_doit(mf_series* s, float* max_err);
+/* CalcTIltAxis::DoIt (Markerfree/src/method/Rotate.cu:333-378): common-line search
+ * over `num` candidate axes spanning `range` degrees; sets rotate[] for all tilts. */
+MF_API int mf_tilt_axis(mf_series* s, float range, int num, float* axis_out);
+/* FindOffset::DoIt (Markerfree/src/method/FindOffset.cu:85-96): adds the best of
+ * 31 one-degree tilt-angle offsets to param.angle_offset. */
+MF_API int mf_find_offset(mf_series* s, float* offset_out);
+/* ProjAlign::Setup (Markerfree/src/method/ProjAlign.cpp:126-203). */
+MF_API int mf_projalign_setup(mf_series* s, float zshift, int align_z, int nproj);
+/* ProjAlign::DoIt (Markerfree/src/method/ProjAlign.cpp:205-257): one projection-
+ * matching pass over all tilts; returns the largest measured shift (px). */
+MF_API int mf_projalign_doit(mf_series* s, float* max_err);
+/* Rotation-centre z of the last pass (ProjAlign.cpp:537-564). */
+MF_API int mf_projalign_z0(mf_series* s, float* z0);
+/* Process::mCoarseAlign (Markerfree/src/main/Process.cpp:238-270); applies the
+ * offset to the series' angles as the reference does. */
+MF_API int mf_coarse_align(mf_series* s, float pitch_angle, float offset);
+/* Process::mProjAlign + ProjAlignOnce (Process.cpp:272-319). */
+MF_API int mf_proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes);
+/* Process::CorrectStack (Process.cpp:329-372): rotate, shift and bin every tilt;
+ * writes nz * (ny/out_bin/2*2) * (nx/out_bin/2*2) floats to host_out. */
+MF_API int mf_correct_stack(mf_series* s, int out_bin, float* host_out);
+/* Size of the output stack of mf_correct_stack. */
+MF_API void mf_binned_size(int nx, int ny, int bin, int* xb, int* yb);
+
+/* Process::DoIt minus file I/O (Process.cpp:34-92): pre-process, coarse-align,
+ * projection-match and write the aligned stack (if aligned_out != NULL).
+ * param arrays must hold nz entries; `passes` (optional) gets the DoIt count. */
+MF_API int mf_align(mf_context* ctx, const float* raw_stack, int nx, int ny, int nz,
+                    const float* file_angles, const mf_options* opt, mf_align_param* param,
+                    float* aligned_out, int* passes);
+
+/* ---- single kernels on caller-owned device memory (same stream semantics:
+ * the call is ordered on the context stream and returns after queuing). ------ */
+/* CorrTomoStack::mCorrectProj (Markerfree/src/method/CorrStack.cu:370-397) for one
+ * projection: d_proj (ny x nx) -> d_out (ny/bin/2*2 x nx/bin/2*2). */
+MF_API int mf_dev_correct_proj(mf_context* ctx, const float* d_proj, int nx, int ny,
+                               float shift_x, float shift_y, float tilt_axis, int only_shift,
+                               int bin, int random_fill, int rweight, float* d_out);
+/* CalcReprojFBP::FindProjRange (Markerfree/src/method/CalcReproj.cu:281-334). */
+MF_API int mf_find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
+                              int nproj, int* range2);
+/* CalcReprojFBP::DoIt (CalcReproj.cu:255-311): back-project tilts [istart, iend] of
+ * the corrected stack d_corr (nz x yb x xb) into a 2*xb x thickness slab per row
+ * and re-project it at angles[iproj] into d_out (yb x xb).  method 0 = exact
+ * per-sample gather, 1 = banded operator (the production path). */
+MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb, int nz,
+                            const float* angles, int iproj, int istart, int iend, int thickness,
+                            int method, float* d_out);
+/* ProjAlign::MeaAlignProj + PAFindPeak (ProjAlign.cpp:321-453): shift (binned px)
+ * of d_proj against d_reproj, both yb x xb. */
+MF_API int mf_dev_measure_shift(mf_context* ctx, const float* d_reproj, const float* d_proj,
+                                int xb, int yb, float* shift2, float* peak);
+
+/* ---- files (MrcStackM, Process::ReadAngles, SaveParam) ---------------------- */
+/* MRC header fields (Markerfree/src/mrc/mrcheader.h:24-96); modes 0, 1, 2 read. */
+MF_API int mf_mrc_info(const char* path, int* nx, int* ny, int* nz, int* mode);
+MF_API int mf_mrc_read(const char* path, float* out);
+/* Float32 MRC with the reference's header (InitializeHeader + UpdateHeader:
+ * statistics of the middle slice only, mrcstack.cpp:421-501). */
+MF_API int mf_mrc_write(const char* path, const float* data, int nx, int ny, int nz);
+/* Whitespace-separated floats (Process.cpp:186-206); *n gets the count read. */
+MF_API int mf_read_angles(const char* path, float* out, int max, int* n);
+/* Process::CollectParam + SaveParam::GetParam(bin=1, mode, inv)
+ * (Markerfree/src/main/Process.cpp:399-418, Markerfree/src/method/SaveParam.cpp:122-183):
+ * writes <out>.txt (mode 0) or <out>.xf (mode 1), ".mrc" in the output path
+ * replaced; file_angles are the angles in file order (reversed here when they
+ * descend, which also reverses the .xf rows). */
+MF_API int mf_save_param(const char* output_path, int mode, const mf_align_param* p,
+                         const float* file_angles, int nz, int raw_nx, int raw_ny, int out_bin,
+                         float elapsed_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MARKERFREE_H */

@@ -1,0 +1,366 @@
+"""B200 projection-matching alignment (ctypes binding of libmfalign.so).
+
+The library is the product: hand-written sm_100a CUDA kernels plus cuFFT behind
+the C ABI declared in include/markerfree.h.  This module loads it from
+markerfree_b200/_build/ and mirrors the reference's units of work:
+
+    Series          pre-processed, device-resident tilt series (PreProcess + buf.mrc)
+    Series.transform_doit / tilt_axis / find_offset / coarse_align
+    Series.projalign_setup / projalign_doit / proj_align / correct_stack
+    align()         Process::DoIt minus file I/O
+    dev_*()         single kernels on caller-owned device memory
+
+There is no CPU fallback: if the library or a GPU is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libmfalign.so")
+CLI_PATH = os.path.join(_HERE, "_build", "Markerfree")
+
+MF_OK = 0
+PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+
+
+class MfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"markerfree error {code}: {msg}")
+        self.code = code
+
+
+class AlignParamC(ctypes.Structure):
+    _fields_ = [("shift_x", _c_float_p), ("shift_y", _c_float_p), ("rotate", _c_float_p),
+                ("angle_offset", ctypes.c_float)]
+
+
+class OptionsC(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_float), ("pitch_angle", ctypes.c_float),
+                ("zshift", ctypes.c_float), ("thickness", ctypes.c_int),
+                ("align_z", ctypes.c_int), ("out_bin", ctypes.c_int), ("gpu", ctypes.c_int),
+                ("nproj", ctypes.c_int), ("save_mode", ctypes.c_int)]
+
+
+# (name, restype, argtypes) of every entry point in include/markerfree.h
+SIGNATURES = [
+    ("mf_last_error", ctypes.c_char_p, []),
+    ("mf_version", ctypes.c_char_p, []),
+    ("mf_context_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_context_destroy", None, [ctypes.c_void_p]),
+    ("mf_context_sync", ctypes.c_int, [ctypes.c_void_p]),
+    ("mf_context_kernel_launches", ctypes.c_int64, [ctypes.c_void_p]),
+    ("mf_series_create", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, _f32p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_series_create_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, _f32p,
+                                               ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_series_destroy", None, [ctypes.c_void_p]),
+    ("mf_series_set_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("mf_series_get_stack", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_series_set_angles", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_series_get_angles", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_series_set_param", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AlignParamC)]),
+    ("mf_series_get_param", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AlignParamC)]),
+    ("mf_transform_doit", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
+    ("mf_tilt_axis", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int, _c_float_p]),
+    ("mf_find_offset", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
+    ("mf_projalign_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int,
+                                          ctypes.c_int]),
+    ("mf_projalign_doit", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
+    ("mf_projalign_z0", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
+    ("mf_coarse_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float]),
+    ("mf_proj_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                     _c_int_p]),
+    ("mf_correct_stack", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _f32p]),
+    ("mf_binned_size", None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p]),
+    ("mf_align", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                _f32p, ctypes.POINTER(OptionsC), ctypes.POINTER(AlignParamC),
+                                ctypes.c_void_p, _c_int_p]),
+    ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    ("mf_find_proj_range", ctypes.c_int, [_f32p, ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int,
+                                          _i32p]),
+    ("mf_dev_reproject", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p]),
+    ("mf_dev_measure_shift", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_int, _f32p, _c_float_p]),
+    ("mf_mrc_info", ctypes.c_int, [ctypes.c_char_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    ("mf_mrc_read", ctypes.c_int, [ctypes.c_char_p, _f32p]),
+    ("mf_mrc_write", ctypes.c_int, [ctypes.c_char_p, _f32p, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int]),
+    ("mf_read_angles", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, _c_int_p]),
+    ("mf_save_param", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(AlignParamC),
+                                     _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_float]),
+]
+
+_lib = None
+
+
+def lib():
+    """Load libmfalign.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m markerfree_b200.build` "
+                              "(or __graft_entry__.build()) first")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != MF_OK:
+        raise MfError(rc, lib().mf_last_error().decode(errors="replace"))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def binned_size(nx: int, ny: int, b: int):
+    xb, yb = ctypes.c_int(), ctypes.c_int()
+    lib().mf_binned_size(nx, ny, b, ctypes.byref(xb), ctypes.byref(yb))
+    return xb.value, yb.value
+
+
+class Param:
+    """AlignParam (Markerfree/src/method/Util.h:14-21) on host arrays."""
+
+    def __init__(self, nz: int):
+        self.shift_x = np.zeros(nz, np.float32)
+        self.shift_y = np.zeros(nz, np.float32)
+        self.rotate = np.zeros(nz, np.float32)
+        self.angle_offset = 0.0
+
+    def c(self) -> AlignParamC:
+        return AlignParamC(self.shift_x.ctypes.data_as(_c_float_p),
+                           self.shift_y.ctypes.data_as(_c_float_p),
+                           self.rotate.ctypes.data_as(_c_float_p), float(self.angle_offset))
+
+
+class Context:
+    """One GPU and one stream (the reference's cudaSetDevice, main.cpp:26)."""
+
+    def __init__(self, gpu: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().mf_context_create(gpu, ctypes.byref(h)))
+        self.h = h
+
+    def sync(self):
+        _check(lib().mf_context_sync(self.h))
+
+    def kernel_launches(self) -> int:
+        return int(lib().mf_context_kernel_launches(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mf_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Series:
+    """A pre-processed tilt series kept in HBM (replaces buf.mrc)."""
+
+    def __init__(self, ctx: Context, raw_stack, file_angles):
+        raw = _f32(raw_stack)
+        self.nz, self.ny, self.nx = raw.shape
+        self.ctx = ctx
+        self.file_angles = _f32(file_angles)[: self.nz]
+        h = ctypes.c_void_p()
+        _check(lib().mf_series_create(ctx.h, raw, self.nx, self.ny, self.nz, self.file_angles,
+                                      ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mf_series_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- state --
+    def stack(self):
+        out = np.empty((self.nz, self.ny, self.nx), np.float32)
+        _check(lib().mf_series_get_stack(self.h, out))
+        return out
+
+    @property
+    def angles(self):
+        a = np.empty(self.nz, np.float32)
+        _check(lib().mf_series_get_angles(self.h, a))
+        return a
+
+    @angles.setter
+    def angles(self, a):
+        _check(lib().mf_series_set_angles(self.h, _f32(a)))
+
+    def get_param(self) -> Param:
+        p = Param(self.nz)
+        c = p.c()
+        _check(lib().mf_series_get_param(self.h, ctypes.byref(c)))
+        p.angle_offset = c.angle_offset
+        return p
+
+    def set_param(self, p: Param):
+        c = p.c()
+        _check(lib().mf_series_set_param(self.h, ctypes.byref(c)))
+
+    def set_precision(self, prec: int):
+        _check(lib().mf_series_set_precision(self.h, prec))
+
+    # -- stages --
+    def transform_doit(self) -> float:
+        e = ctypes.c_float()
+        _check(lib().mf_transform_doit(self.h, ctypes.byref(e)))
+        return e.value
+
+    def tilt_axis(self, rng: float, num: int = 100) -> float:
+        a = ctypes.c_float()
+        _check(lib().mf_tilt_axis(self.h, rng, num, ctypes.byref(a)))
+        return a.value
+
+    def find_offset(self) -> float:
+        o = ctypes.c_float()
+        _check(lib().mf_find_offset(self.h, ctypes.byref(o)))
+        return o.value
+
+    def coarse_align(self, pitch_angle: float = 0.0, offset: float = 0.0):
+        _check(lib().mf_coarse_align(self.h, pitch_angle, offset))
+
+    def projalign_setup(self, zshift: float = 0.0, align_z: int = 600, nproj: int = 10):
+        _check(lib().mf_projalign_setup(self.h, zshift, align_z, nproj))
+
+    def projalign_doit(self) -> float:
+        e = ctypes.c_float()
+        _check(lib().mf_projalign_doit(self.h, ctypes.byref(e)))
+        return e.value
+
+    @property
+    def z0(self) -> float:
+        z = ctypes.c_float()
+        _check(lib().mf_projalign_z0(self.h, ctypes.byref(z)))
+        return z.value
+
+    def proj_align(self, zshift: float = 0.0, align_z: int = 600, nproj: int = 10) -> int:
+        n = ctypes.c_int()
+        _check(lib().mf_proj_align(self.h, zshift, align_z, nproj, ctypes.byref(n)))
+        return n.value
+
+    def correct_stack(self, out_bin: int = 1):
+        xo, yo = binned_size(self.nx, self.ny, out_bin)
+        out = np.empty((self.nz, yo, xo), np.float32)
+        _check(lib().mf_correct_stack(self.h, out_bin, out))
+        return out
+
+
+def align(ctx: Context, raw_stack, file_angles, offset=0.0, pitch_angle=0.0, zshift=0.0,
+          align_z=600, out_bin=1, nproj=10, want_stack=True):
+    """Process::DoIt minus file I/O.  Returns (Param, aligned stack or None, passes)."""
+    raw = _f32(raw_stack)
+    nz, ny, nx = raw.shape
+    p = Param(nz)
+    c = p.c()
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    out = None
+    ptr = None
+    if want_stack:
+        xo, yo = binned_size(nx, ny, out_bin)
+        out = np.empty((nz, yo, xo), np.float32)
+        ptr = out.ctypes.data_as(ctypes.c_void_p)
+    n = ctypes.c_int()
+    _check(lib().mf_align(ctx.h, raw, nx, ny, nz, _f32(file_angles)[:nz], ctypes.byref(o),
+                          ctypes.byref(c), ptr, ctypes.byref(n)))
+    p.angle_offset = c.angle_offset
+    return p, out, n.value
+
+
+def find_proj_range(angles, skip, iproj, nproj):
+    a = _f32(angles)
+    r = np.zeros(2, np.int32)
+    _check(lib().mf_find_proj_range(a, len(a), np.ascontiguousarray(skip, np.uint8), iproj,
+                                     nproj, r))
+    return int(r[0]), int(r[1])
+
+
+def _ptr(t):
+    """Device pointer of a torch CUDA tensor (or an int address)."""
+    if isinstance(t, int):
+        return ctypes.c_void_p(t)
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def dev_correct_proj(ctx: Context, d_proj, nx, ny, shift_x, shift_y, tilt_axis, only_shift,
+                     binning, random_fill, rweight, d_out):
+    _check(lib().mf_dev_correct_proj(ctx.h, _ptr(d_proj), nx, ny, shift_x, shift_y, tilt_axis,
+                                     int(only_shift), binning, int(random_fill), int(rweight),
+                                     _ptr(d_out)))
+
+
+def dev_reproject(ctx: Context, d_corr, xb, yb, nz, angles, iproj, istart, iend, thickness,
+                  method, d_out):
+    _check(lib().mf_dev_reproject(ctx.h, _ptr(d_corr), xb, yb, nz, _f32(angles), iproj, istart,
+                                  iend, thickness, method, _ptr(d_out)))
+
+
+def dev_measure_shift(ctx: Context, d_reproj, d_proj, xb, yb):
+    sh = np.zeros(2, np.float32)
+    pk = ctypes.c_float()
+    _check(lib().mf_dev_measure_shift(ctx.h, _ptr(d_reproj), _ptr(d_proj), xb, yb, sh,
+                                      ctypes.byref(pk)))
+    return float(sh[0]), float(sh[1]), pk.value
+
+
+# -- files --
+def mrc_read(path: str):
+    nx, ny, nz, mode = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().mf_mrc_info(path.encode(), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz),
+                             ctypes.byref(mode)))
+    out = np.empty((nz.value, ny.value, nx.value), np.float32)
+    _check(lib().mf_mrc_read(path.encode(), out))
+    return out, mode.value
+
+
+def mrc_write(path: str, data):
+    d = _f32(data)
+    nz, ny, nx = d.shape
+    _check(lib().mf_mrc_write(path.encode(), d, nx, ny, nz))
+
+
+def read_angles(path: str):
+    n = ctypes.c_int()
+    _check(lib().mf_read_angles(path.encode(), None, 0, ctypes.byref(n)))
+    out = np.empty(n.value, np.float32)
+    _check(lib().mf_read_angles(path.encode(), out.ctypes.data_as(ctypes.c_void_p), n.value,
+                                ctypes.byref(n)))
+    return out
+
+
+def save_param(output_path: str, mode: int, p: Param, file_angles, raw_nx, raw_ny, out_bin=1,
+               elapsed_s=0.0):
+    c = p.c()
+    a = _f32(file_angles)
+    _check(lib().mf_save_param(output_path.encode(), mode, ctypes.byref(c), a, len(a), raw_nx,
+                               raw_ny, out_bin, elapsed_s))

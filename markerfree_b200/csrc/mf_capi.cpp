@@ -1,0 +1,403 @@
+// extern "C" entry points (include/markerfree.h).
+#include <cstring>
+#include <new>
+
+#include "mf_series.hpp"
+#include "mf_xcorr.hpp"
+
+namespace mf {
+const char* last_error();
+}
+
+using namespace mf;
+
+#define MF_GUARD_BEGIN try {
+#define MF_GUARD_END                                                      \
+  }                                                                       \
+  catch (const std::bad_alloc&) {                                         \
+    return set_error(MF_ERR_NOMEM, "host allocation failed");             \
+  }                                                                       \
+  catch (...) {                                                           \
+    return set_error(MF_ERR_STATE, "unexpected exception in the library"); \
+  }
+
+static int use_device(mf_context* ctx) {
+  if (!ctx) return set_error(MF_ERR_ARG, "null context");
+  MF_CHECK_CUDA(cudaSetDevice(ctx->c.gpu));
+  return MF_OK;
+}
+
+static mf_context::Scratch* scratch_of(mf_context* ctx) { return &ctx->scratch; }
+
+extern "C" {
+
+MF_API const char* mf_last_error(void) { return mf::last_error(); }
+MF_API const char* mf_version(void) { return "markerfree-b200 0.1 (sm_100a)"; }
+
+MF_API int mf_context_create(int gpu, mf_context** out) {
+  MF_GUARD_BEGIN
+  if (!out) return set_error(MF_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  MF_CHECK_CUDA(cudaGetDeviceCount(&n));
+  if (gpu < 0 || gpu >= n) return set_error(MF_ERR_ARG, "GPU %d not present (%d visible)", gpu, n);
+  MF_CHECK_CUDA(cudaSetDevice(gpu));
+  mf_context* ctx = new mf_context();
+  ctx->c.gpu = gpu;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, gpu) == cudaSuccess) ctx->c.sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return set_error(MF_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  *out = ctx;
+  return MF_OK;
+  MF_GUARD_END
+}
+
+MF_API void mf_context_destroy(mf_context* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->c.gpu);
+  cudaStreamSynchronize(ctx->c.stream);
+  delete ctx;
+}
+
+MF_API int mf_context_sync(mf_context* ctx) {
+  MF_TRY(use_device(ctx));
+  MF_CHECK_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  return MF_OK;
+}
+
+MF_API int64_t mf_context_kernel_launches(mf_context* ctx) { return ctx ? ctx->c.launches : 0; }
+
+// ---------------------------------------------------------------------------
+static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_device, int nx,
+                                int ny, int nz, const float* file_angles, mf_series** out) {
+  if (!out) return set_error(MF_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  MF_TRY(use_device(ctx));
+  if (!raw || !file_angles) return set_error(MF_ERR_ARG, "null stack or angles");
+  if (nx < 8 || ny < 8 || nz < 2)
+    return set_error(MF_ERR_ARG, "stack %d x %d x %d too small (need >= 8 x 8 x 2)", nx, ny, nz);
+  mf_series* s = new mf_series();
+  int rc = series_init(s, ctx, nx, ny, nz, file_angles);
+  size_t pix = (size_t)nx * ny;
+  if (rc == MF_OK) rc = s->stack.alloc(sizeof(float) * pix * nz);
+  if (rc == MF_OK) {
+    // SetPositive writes slice a to index nz-1-a when the angles descend
+    bool rev = file_angles[0] > file_angles[1];
+    cudaStream_t st = ctx->c.stream;
+    for (int a = 0; a < nz && rc == MF_OK; ++a) {
+      int i = rev ? nz - 1 - a : a;
+      cudaError_t e = cudaMemcpyAsync(s->stack.as<float>() + (size_t)i * pix, raw + (size_t)a * pix,
+                                      sizeof(float) * pix,
+                                      raw_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      st);
+      if (e != cudaSuccess) rc = set_error(MF_ERR_CUDA, "stack upload: %s", cudaGetErrorString(e));
+    }
+  }
+  if (rc == MF_OK)
+    rc = preprocess_device(&ctx->c, s->stack.as<float>(), nx, ny, nz, file_angles, ctx->c.stream);
+  if (rc != MF_OK) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return MF_OK;
+}
+
+MF_API int mf_series_create(mf_context* ctx, const float* raw, int nx, int ny, int nz,
+                            const float* file_angles, mf_series** out) {
+  MF_GUARD_BEGIN
+  return series_create_common(ctx, raw, false, nx, ny, nz, file_angles, out);
+  MF_GUARD_END
+}
+
+MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw, int nx, int ny, int nz,
+                                   const float* file_angles, mf_series** out) {
+  MF_GUARD_BEGIN
+  return series_create_common(ctx, d_raw, true, nx, ny, nz, file_angles, out);
+  MF_GUARD_END
+}
+
+MF_API void mf_series_destroy(mf_series* s) {
+  if (!s) return;
+  if (s->ctx) {
+    cudaSetDevice(s->ctx->c.gpu);
+    cudaStreamSynchronize(s->ctx->c.stream);
+  }
+  delete s;
+}
+
+MF_API int mf_series_set_precision(mf_series* s, mf_precision p) {
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  if (p != MF_PREC_FP32 && p != MF_PREC_BF16 && p != MF_PREC_FP16)
+    return set_error(MF_ERR_ARG, "unknown precision %d", (int)p);
+  s->precision = p;
+  return MF_OK;
+}
+
+MF_API int mf_series_get_stack(mf_series* s, float* out) {
+  if (!s || !out) return set_error(MF_ERR_ARG, "null argument");
+  MF_TRY(use_device(s->ctx));
+  MF_CHECK_CUDA(cudaMemcpyAsync(out, s->stack.p, sizeof(float) * (size_t)s->nx * s->ny * s->nz,
+                                cudaMemcpyDeviceToHost, s->ctx->c.stream));
+  MF_CHECK_CUDA(cudaStreamSynchronize(s->ctx->c.stream));
+  return MF_OK;
+}
+
+MF_API int mf_series_set_angles(mf_series* s, const float* a) {
+  if (!s || !a) return set_error(MF_ERR_ARG, "null argument");
+  s->angles.assign(a, a + s->nz);
+  return MF_OK;
+}
+
+MF_API int mf_series_get_angles(mf_series* s, float* a) {
+  if (!s || !a) return set_error(MF_ERR_ARG, "null argument");
+  memcpy(a, s->angles.data(), sizeof(float) * s->nz);
+  return MF_OK;
+}
+
+MF_API int mf_series_set_param(mf_series* s, const mf_align_param* p) {
+  if (!s || !p || !p->shift_x || !p->shift_y || !p->rotate)
+    return set_error(MF_ERR_ARG, "null argument");
+  s->sx.assign(p->shift_x, p->shift_x + s->nz);
+  s->sy.assign(p->shift_y, p->shift_y + s->nz);
+  s->rot.assign(p->rotate, p->rotate + s->nz);
+  s->angle_offset = p->angle_offset;
+  return MF_OK;
+}
+
+MF_API int mf_series_get_param(mf_series* s, mf_align_param* p) {
+  if (!s || !p || !p->shift_x || !p->shift_y || !p->rotate)
+    return set_error(MF_ERR_ARG, "null argument");
+  memcpy(p->shift_x, s->sx.data(), sizeof(float) * s->nz);
+  memcpy(p->shift_y, s->sy.data(), sizeof(float) * s->nz);
+  memcpy(p->rotate, s->rot.data(), sizeof(float) * s->nz);
+  p->angle_offset = s->angle_offset;
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+MF_API int mf_transform_doit(mf_series* s, float* max_err) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return transform_doit(s, max_err);
+  MF_GUARD_END
+}
+
+MF_API int mf_tilt_axis(mf_series* s, float range, int num, float* axis_out) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return tilt_axis(s, range, num, axis_out);
+  MF_GUARD_END
+}
+
+MF_API int mf_find_offset(mf_series* s, float* offset_out) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return find_offset(s, offset_out);
+  MF_GUARD_END
+}
+
+MF_API int mf_projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return projalign_setup(s, zshift, align_z, nproj);
+  MF_GUARD_END
+}
+
+MF_API int mf_projalign_doit(mf_series* s, float* max_err) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return projalign_doit(s, max_err);
+  MF_GUARD_END
+}
+
+MF_API int mf_projalign_z0(mf_series* s, float* z0) {
+  if (!s || !z0) return set_error(MF_ERR_ARG, "null argument");
+  if (!s->pa.ready) return set_error(MF_ERR_STATE, "projection matching is not set up");
+  *z0 = s->pa.z0;
+  return MF_OK;
+}
+
+MF_API int mf_coarse_align(mf_series* s, float pitch_angle, float offset) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return coarse_align(s, pitch_angle, offset);
+  MF_GUARD_END
+}
+
+MF_API int mf_proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes) {
+  MF_GUARD_BEGIN
+  if (!s) return set_error(MF_ERR_ARG, "null series");
+  MF_TRY(use_device(s->ctx));
+  return proj_align(s, zshift, align_z, nproj, passes);
+  MF_GUARD_END
+}
+
+MF_API void mf_binned_size(int nx, int ny, int bin, int* xb, int* yb) {
+  if (bin < 1) bin = 1;
+  if (xb) *xb = nx / bin / 2 * 2;
+  if (yb) *yb = ny / bin / 2 * 2;
+}
+
+MF_API int mf_correct_stack(mf_series* s, int out_bin, float* host_out) {
+  MF_GUARD_BEGIN
+  if (!s || !host_out) return set_error(MF_ERR_ARG, "null argument");
+  MF_TRY(use_device(s->ctx));
+  int xo, yo;
+  mf_binned_size(s->nx, s->ny, out_bin, &xo, &yo);
+  size_t n = (size_t)xo * yo * s->nz;
+  DevBuf out;
+  MF_TRY(out.alloc(sizeof(float) * n));
+  MF_TRY(correct_stack_device(s, out_bin, out.as<float>()));
+  MF_CHECK_CUDA(cudaMemcpyAsync(host_out, out.p, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                                s->ctx->c.stream));
+  MF_CHECK_CUDA(cudaStreamSynchronize(s->ctx->c.stream));
+  return MF_OK;
+  MF_GUARD_END
+}
+
+MF_API int mf_align(mf_context* ctx, const float* raw, int nx, int ny, int nz,
+                    const float* file_angles, const mf_options* opt, mf_align_param* param,
+                    float* aligned_out, int* passes) {
+  MF_GUARD_BEGIN
+  if (!opt || !param) return set_error(MF_ERR_ARG, "null options or parameters");
+  if (opt->nproj <= 0) return set_error(MF_ERR_ARG, "nProj must be > 0.");
+  if (opt->out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
+  mf_series* s = nullptr;
+  MF_TRY(mf_series_create(ctx, raw, nx, ny, nz, file_angles, &s));
+  int rc = MF_OK;
+  int np = 0;
+  if (opt->align_z != 0) {
+    rc = coarse_align(s, opt->pitch_angle, opt->offset);
+    if (rc == MF_OK) rc = proj_align(s, opt->zshift, opt->align_z, opt->nproj, &np);
+  }
+  if (rc == MF_OK && aligned_out) rc = mf_correct_stack(s, opt->out_bin, aligned_out);
+  if (rc == MF_OK) rc = mf_series_get_param(s, param);
+  if (passes) *passes = np;
+  mf_series_destroy(s);
+  return rc;
+  MF_GUARD_END
+}
+
+// ---------------------------------------------------------------------------
+MF_API int mf_dev_correct_proj(mf_context* ctx, const float* d_proj, int nx, int ny,
+                               float shift_x, float shift_y, float tilt_axis, int only_shift,
+                               int bin, int random_fill, int rweight, float* d_out) {
+  MF_GUARD_BEGIN
+  MF_TRY(use_device(ctx));
+  if (!d_proj || !d_out || bin < 1) return set_error(MF_ERR_ARG, "invalid argument");
+  int xb = nx / bin / 2 * 2, yb = ny / bin / 2 * 2;
+  if (xb < 2 || yb < 2) return set_error(MF_ERR_ARG, "image too small for binning %d", bin);
+  cudaStream_t st = ctx->c.stream;
+  if (!rweight)
+    return launch_correct_one(&ctx->c, d_proj, nx, ny, shift_x, shift_y, tilt_axis, only_shift,
+                              bin, random_fill, d_out, xb, st);
+  int pad = (xb / 2 + 1) * 2, cmp = xb / 2 + 1;
+  mf_context::Scratch* S = scratch_of(ctx);
+  MF_TRY(S->a.alloc(sizeof(float) * (size_t)pad * yb));
+  MF_TRY(launch_correct_one(&ctx->c, d_proj, nx, ny, shift_x, shift_y, tilt_axis, only_shift, bin,
+                            random_fill, S->a.as<float>(), pad, st));
+  cufftHandle f, i;
+  MF_TRY(ctx->plan({0, xb, yb, yb}, &f));
+  MF_TRY(ctx->plan({1, xb, yb, yb}, &i));
+  MF_CHECK_CUFFT(cufftExecR2C(f, S->a.as<cufftReal>(), S->a.as<cufftComplex>()));
+  MF_TRY(launch_rweight(&ctx->c, S->a.as<cufftComplex>(), cmp, yb, st));
+  MF_CHECK_CUFFT(cufftExecC2R(i, S->a.as<cufftComplex>(), d_out));
+  return MF_OK;
+  MF_GUARD_END
+}
+
+MF_API int mf_find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
+                              int nproj, int* range2) {
+  if (!angles || !skip || !range2 || iproj < 0 || iproj >= nz || nproj <= 0)
+    return set_error(MF_ERR_ARG, "invalid argument");
+  find_proj_range(angles, nz, skip, iproj, nproj, range2);
+  return MF_OK;
+}
+
+MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb, int nz,
+                            const float* angles, int iproj, int istart, int iend, int thickness,
+                            int method, float* d_out) {
+  MF_GUARD_BEGIN
+  MF_TRY(use_device(ctx));
+  if (!d_corr || !angles || !d_out) return set_error(MF_ERR_ARG, "null argument");
+  if (istart < 0 || iend < istart || iend >= nz || iproj < 0 || iproj >= nz || thickness < 2 ||
+      xb < 2 || yb < 1)
+    return set_error(MF_ERR_ARG, "invalid re-projection range or size");
+  cudaStream_t st = ctx->c.stream;
+  ReprojGeom g;
+  reproj_geometry(angles, iproj, istart, iend, xb, yb, thickness, &g);
+  mf_context::Scratch* S = scratch_of(ctx);
+  MF_TRY(S->b.alloc(sizeof(float) * g.bp.size()));
+  MF_CHECK_CUDA(cudaMemcpyAsync(S->b.p, g.bp.data(), sizeof(float) * g.bp.size(),
+                                cudaMemcpyHostToDevice, st));
+  size_t pix = (size_t)xb * yb;
+  if (method == 0) {
+    MF_TRY(launch_reproject_exact(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0, g.nk,
+                                  g.fcos, g.fsin, g.ray_len, g.thick, nullptr, d_out, st));
+  } else {
+    ReprojOp op;
+    MF_TRY(build_reproj_op(&ctx->c, g, &op, st));
+    int ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
+    MF_TRY(S->c.alloc(sizeof(int) * ytiles));
+    MF_CHECK_CUDA(cudaMemsetAsync(S->c.p, 0, sizeof(int) * ytiles, st));
+    MF_TRY(launch_reproject_apply(&ctx->c, op, d_corr, pix, S->c.as<int>(), d_out, st));
+    MF_TRY(launch_reproject_exact(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0, g.nk,
+                                  g.fcos, g.fsin, g.ray_len, g.thick, S->c.as<int>(), d_out, st));
+  }
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+  MF_GUARD_END
+}
+
+MF_API int mf_dev_measure_shift(mf_context* ctx, const float* d_reproj, const float* d_proj,
+                                int xb, int yb, float* shift2, float* peak) {
+  MF_GUARD_BEGIN
+  MF_TRY(use_device(ctx));
+  if (!d_reproj || !d_proj || !shift2 || xb < 8 || yb < 8 || (xb & 1))
+    return set_error(MF_ERR_ARG, "invalid argument");
+  cudaStream_t st = ctx->c.stream;
+  const int pad = (xb / 2 + 1) * 2, cmp = pad / 2;
+  const size_t ppix = (size_t)pad * yb;
+  mf_context::Scratch* S = scratch_of(ctx);
+  MF_TRY(S->a.alloc(sizeof(float) * ppix * 2));
+  MF_TRY(S->d.alloc(sizeof(double2) * kMomentParts * 2 + sizeof(float2) * (kPeakParts + 2) + 64));
+  double2* mpart = S->d.as<double2>();
+  float2* stats = reinterpret_cast<float2*>(mpart + kMomentParts * 2);
+  float2* ppart = stats + 2;
+  float* outv = reinterpret_cast<float*>(ppart + kPeakParts);
+  float* cc = S->a.as<float>();
+  const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
+  MF_TRY(norm_mask_pad(&ctx->c, d_reproj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad,
+                       (float)yb, 4.0f, cc, mpart, stats, st));
+  MF_TRY(norm_mask_pad(&ctx->c, d_proj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad,
+                       (float)yb, 4.0f, cc + ppix, mpart + kMomentParts, stats + 1, st));
+  cufftHandle f, i;
+  MF_TRY(ctx->plan({2, xb, yb, 2}, &f));
+  MF_TRY(ctx->plan({3, xb, yb, 1}, &i));
+  MF_CHECK_CUFFT(cufftExecR2C(f, cc, (cufftComplex*)cc));
+  MF_TRY(xcorr_filter(&ctx->c, (cufftComplex*)cc, 0, nullptr, (cufftComplex*)(cc + ppix), 0, 1,
+                      cmp, yb, 500.0f, 1.0f, st));
+  MF_CHECK_CUFFT(cufftExecC2R(i, (cufftComplex*)(cc + ppix), cc + ppix));
+  MF_TRY(pa_peak_only(&ctx->c, cc + ppix, pad, xb, yb, ppart, outv, st));
+  float h[3];
+  MF_CHECK_CUDA(cudaMemcpyAsync(h, outv, sizeof(h), cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  shift2[0] = h[0];
+  shift2[1] = h[1];
+  if (peak) *peak = h[2];
+  return MF_OK;
+  MF_GUARD_END
+}
+
+}  // extern "C"
+

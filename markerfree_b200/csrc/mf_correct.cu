@@ -1,0 +1,307 @@
+// Stack correction and pre-processing kernels.
+//
+// Reference: Markerfree/src/method/CorrStack.cu (mGCorrect + mGRandom :116-179,
+// mGBinImage :40-63, GRWeight :431-446) and Markerfree/src/method/Preprocess.cu.
+// The reference resamples into a padded buffer, bins it in a second kernel,
+// R-weights it with batched 1-D cuFFTs and un-pads it with one cudaMemcpy per
+// row.  Here resampling and binning are one kernel that writes straight into the
+// row layout the FFT wants, and the inverse FFT writes the dense corrected stack.
+#include "mf_internal.hpp"
+
+namespace mf {
+
+// CorrStack.cu:116-140
+__device__ __forceinline__ float corr_random(int x, int y, int in_x, int in_y,
+                                             const float* __restrict__ img) {
+  if (x < 0) x = -x;
+  if (y < 0) y = -y;
+  if (x >= in_x) x = in_x - 1 - (x % in_x);
+  if (y >= in_y) y = in_y - 1 - (y % in_y);
+  const int win = 51, size = win * win;
+  unsigned int next = (unsigned int)(y * in_x + x);
+  for (int i = 0; i < 20; ++i) {
+    next = (next * 19u + 57u) % (unsigned int)size;
+    int ix = (int)(next % (unsigned int)size) - win / 2 + x;
+    if (ix < 0 || ix >= in_x) continue;
+    int iy = (int)(next / (unsigned int)win) - win / 2 + y;
+    if (iy < 0 || iy >= in_y) continue;
+    return __ldg(img + (size_t)iy * in_x + ix);
+  }
+  return __ldg(img + (size_t)y * in_x + x);
+}
+
+// CorrStack.cu:151-179 for one resampled pixel (X, Y) of an out_x x in_y grid.
+__device__ __forceinline__ float corr_pixel(const float* __restrict__ img, int in_x, int in_y,
+                                            int X, int Y, int out_x, float sx, float sy,
+                                            float cs, float sn, bool random_fill) {
+  float ax = __fsub_rn(__fadd_rn((float)X, 0.5f), __fmul_rn((float)out_x, 0.5f));
+  float ay = __fsub_rn(__fadd_rn((float)Y, 0.5f), __fmul_rn((float)in_y, 0.5f));
+  float t = __fsub_rn(__fmul_rn(ax, cs), __fmul_rn(ay, sn));
+  ay = __fadd_rn(__fmul_rn(ax, sn), __fmul_rn(ay, cs));
+  ax = t;
+  ax = __fadd_rn(ax, __fadd_rn(sx, __fmul_rn((float)in_x, 0.5f)));
+  ay = __fadd_rn(ay, __fadd_rn(sy, __fmul_rn((float)in_y, 0.5f)));
+  int ix = (int)__fadd_rn(ax, 0.5f);
+  int iy = (int)__fadd_rn(ay, 0.5f);
+  if (ix >= 0 && ix < in_x && iy >= 0 && iy < in_y) return __ldg(img + (size_t)iy * in_x + ix);
+  if (random_fill) return corr_random(ix, iy, in_x, in_y, img);
+  return kSentinel;
+}
+
+struct CorrArgs {
+  const float* stack;
+  int nx, ny;
+  size_t pix;
+  const int* tilts;  // tilt index per blockIdx.z (nullptr: blockIdx.z itself)
+  const float* sx;
+  const float* sy;
+  const float* rot;
+  float one_sx, one_sy, one_rot;  // used when sx == nullptr
+  int only_shift, bin, random_fill;
+  int out_x, xb, yb, binx, biny;
+  float* out;
+  int out_row_stride;
+  size_t out_tilt_stride;
+};
+
+__global__ void k_correct_bin(CorrArgs a) {
+  __shared__ float s_cs, s_sn, s_sx, s_sy;
+  const int j = blockIdx.z;
+  const int z = a.tilts ? a.tilts[j] : j;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    float rot = a.sx ? a.rot[z] : a.one_rot;
+    float axis = a.only_shift ? 0.0f : rot;
+    axis = (float)((double)axis * kD2R);  // CorrStack.cu:376-378
+    s_cs = (float)cos((double)axis);
+    s_sn = (float)sin((double)axis);
+    s_sx = a.sx ? a.sx[z] : a.one_sx;
+    s_sy = a.sx ? a.sy[z] : a.one_sy;
+  }
+  __syncthreads();
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= a.xb || by >= a.yb) return;
+  const float* img = a.stack + (size_t)z * a.pix;
+  float res;
+  if (a.bin == 1) {
+    res = corr_pixel(img, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn, a.random_fill);
+  } else {
+    float sum = 0.0f;
+    bool bad = false;
+    for (int iy = 0; iy < a.biny && !bad; ++iy) {
+      for (int ix = 0; ix < a.binx; ++ix) {
+        float v = corr_pixel(img, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x, s_sx,
+                             s_sy, s_cs, s_sn, a.random_fill);
+        if (v < -1e10f) {
+          bad = true;
+          break;
+        }
+        sum = __fadd_rn(sum, v);
+      }
+    }
+    res = bad ? kSentinel : sum;
+  }
+  a.out[(size_t)j * a.out_tilt_stride + (size_t)by * a.out_row_stride + bx] = res;
+}
+
+static void fill_sizes(CorrArgs* a, int nx, int ny, int bin) {
+  int pad_x = (nx / 2 + 1) * 2;
+  a->out_x = (pad_x / 2 - 1) * 2;  // CorrStack.cu:204
+  a->xb = nx / bin / 2 * 2;        // CorrStack.cu:72-73
+  a->yb = ny / bin / 2 * 2;
+  a->binx = a->out_x / a->xb;  // CorrStack.cu:99-100
+  a->biny = ny / a->yb;
+}
+
+int launch_correct_bin(Context* c, const float* stack, int nx, int ny, const int* d_tilts,
+                       int ntilts, const float* d_sx, const float* d_sy, const float* d_rot,
+                       int only_shift, int bin, int random_fill, float* out, int out_row_stride,
+                       size_t out_tilt_stride, cudaStream_t st) {
+  CorrArgs a{};
+  a.stack = stack;
+  a.nx = nx;
+  a.ny = ny;
+  a.pix = (size_t)nx * ny;
+  a.tilts = d_tilts;
+  a.sx = d_sx;
+  a.sy = d_sy;
+  a.rot = d_rot;
+  a.only_shift = only_shift;
+  a.bin = bin;
+  a.random_fill = random_fill;
+  fill_sizes(&a, nx, ny, bin);
+  a.out = out;
+  a.out_row_stride = out_row_stride;
+  a.out_tilt_stride = out_tilt_stride;
+  dim3 blk(32, 8), grd((a.xb + 31) / 32, (a.yb + 7) / 8, ntilts);
+  k_correct_bin<<<grd, blk, 0, st>>>(a);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int launch_correct_one(Context* c, const float* img, int nx, int ny, float sx, float sy,
+                       float axis_deg, int only_shift, int bin, int random_fill, float* out,
+                       int out_row_stride, cudaStream_t st) {
+  CorrArgs a{};
+  a.stack = img;
+  a.nx = nx;
+  a.ny = ny;
+  a.pix = (size_t)nx * ny;
+  a.one_sx = sx;
+  a.one_sy = sy;
+  a.one_rot = axis_deg;
+  a.only_shift = only_shift;
+  a.bin = bin;
+  a.random_fill = random_fill;
+  fill_sizes(&a, nx, ny, bin);
+  a.out = out;
+  a.out_row_stride = out_row_stride;
+  a.out_tilt_stride = 0;
+  dim3 blk(32, 8), grd((a.xb + 31) / 32, (a.yb + 7) / 8, 1);
+  k_correct_bin<<<grd, blk, 0, st>>>(a);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// CorrStack.cu:431-446: spectrum / N times 2r (0.55 + 0.45 cos 2 pi r), r = k / N.
+__global__ void k_rweight(cufftComplex* spec, int cmp, int rows) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cmp || row >= rows) return;
+  size_t i = (size_t)row * cmp + x;
+  float fN = 2 * ((float)cmp - 1.0f);
+  cufftComplex v = spec[i];
+  v.x = __fdiv_rn(v.x, fN);
+  v.y = __fdiv_rn(v.y, fN);
+  float r = __fdiv_rn((float)x, fN);
+  float cw = (float)cos((double)__fmul_rn(6.2831852f, r));
+  r = __fmul_rn(__fmul_rn(2.0f, r), __fadd_rn(0.55f, __fmul_rn(0.45f, cw)));
+  v.x = __fmul_rn(v.x, r);
+  v.y = __fmul_rn(v.y, r);
+  spec[i] = v;
+}
+
+int launch_rweight(Context* c, cufftComplex* spec, int cmp, int rows, cudaStream_t st) {
+  dim3 blk(128, 2), grd((cmp + 127) / 128, (rows + 1) / 2);
+  k_rweight<<<grd, blk, 0, st>>>(spec, cmp, rows);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pre-processing (Preprocess.cu:103-250).
+// Per-block minimum over valid pixels of a range of slices.
+__global__ void k_block_min(const float* __restrict__ p, size_t n, float* __restrict__ part) {
+  __shared__ float s[256];
+  float m = 1e20f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float v = p[i];
+    if (v < -1e10f) continue;
+    m = fminf(m, v);
+  }
+  s[threadIdx.x] = m;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) s[threadIdx.x] = fminf(s[threadIdx.x], s[threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+// One block per slice: FP64 sum and count of (v - min) over the central box.
+__global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny, float sub,
+                           int subtract, double* __restrict__ sums, int* __restrict__ counts) {
+  __shared__ double s_sum[256];
+  __shared__ int s_cnt[256];
+  const int z = blockIdx.x;
+  const int x0 = nx * 1 / 6, y0 = ny * 1 / 6, w = nx * 4 / 6, h = ny * 4 / 6;
+  const float* f = stack + (size_t)z * nx * ny;
+  double acc = 0.0;
+  int cnt = 0;
+  for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+    int y = i / w, x = i % w;
+    float v = f[(size_t)(y + y0) * nx + x0 + x];
+    if (subtract && !(v < -1e10f)) v = __fsub_rn(v, sub);
+    if (v <= -1e20f) continue;
+    acc += v;
+    cnt++;
+  }
+  s_sum[threadIdx.x] = acc;
+  s_cnt[threadIdx.x] = cnt;
+  __syncthreads();
+  for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
+    if (threadIdx.x < hh) {
+      s_sum[threadIdx.x] += s_sum[threadIdx.x + hh];
+      s_cnt[threadIdx.x] += s_cnt[threadIdx.x + hh];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sums[z] = s_sum[0];
+    counts[z] = s_cnt[0];
+  }
+}
+
+// out = (v - min) * scale[z], skipping sentinels as Subtract and mScale do.
+__global__ void k_positive_scale(float* __restrict__ stack, size_t pix, int nz, float sub,
+                                 int subtract, const float* __restrict__ scale) {
+  size_t n = pix * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float v = stack[i];
+    if (subtract && !(v < -1e10f)) v = __fsub_rn(v, sub);
+    if (!(v <= -1e20f)) v = __fmul_rn(v, scale[i / pix]);
+    stack[i] = v;
+  }
+}
+
+int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
+                      const float* file_angles, cudaStream_t st) {
+  size_t pix = (size_t)nx * ny;
+  size_t n = pix * nz;
+  const int nb = 1024;
+  DevBuf part, sums, counts, scale;
+  MF_TRY(part.alloc(sizeof(float) * nb));
+  MF_TRY(sums.alloc(sizeof(double) * nz));
+  MF_TRY(counts.alloc(sizeof(int) * nz));
+  MF_TRY(scale.alloc(sizeof(float) * nz));
+  k_block_min<<<nb, 256, 0, st>>>(d_stack, n, part.as<float>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  std::vector<float> hp(nb);
+  MF_CHECK_CUDA(cudaMemcpyAsync(hp.data(), part.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  float mn = 1e30f;  // SetPositive: fStackMin starts at 1e30, slice minima start at 1e20
+  for (float v : hp) mn = std::fmin(mn, v);
+  if (mn > 1e20f) mn = 1e20f;
+  int subtract = !(mn >= 0);
+  k_box_mean<<<nz, 256, 0, st>>>(d_stack, nx, ny, mn, subtract, sums.as<double>(),
+                                  counts.as<int>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  std::vector<double> hs(nz);
+  std::vector<int> hc(nz);
+  MF_CHECK_CUDA(cudaMemcpyAsync(hs.data(), sums.p, sizeof(double) * nz, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int) * nz, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  std::vector<float> mean(nz), sc(nz);
+  for (int i = 0; i < nz; ++i) mean[i] = hc[i] == 0 ? 0.0f : (float)(hs[i] / hc[i]);
+  // the zero tilt is looked up in the file-order angles (Preprocess.cu:168)
+  int zero = frame_idx_from_tilt(nz, file_angles, 0.0f);
+  float ref = mean[zero];
+  if (ref > 1000.0f) ref = 1000.0f;
+  for (int i = 0; i < nz; ++i) sc[i] = ref / (mean[i] + 0.00001f);
+  MF_CHECK_CUDA(cudaMemcpyAsync(scale.p, sc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  k_positive_scale<<<c->sm_count * 8, 256, 0, st>>>(d_stack, pix, nz, mn, subtract,
+                                                     scale.as<float>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+}  // namespace mf

@@ -1,0 +1,653 @@
+// Alignment stages on a device-resident series.
+//
+// Reference: Markerfree/src/main/Process.cpp (pipeline and schedule),
+// Markerfree/src/method/ProjAlign.cpp (projection matching), Transform.cpp and
+// FindOffset.cu (coarse stages), Rotate.cu (tilt axis), CorrStack.cu (correction).
+// The reference re-reads every slice from a scratch MRC on disk for every
+// correction and drives the GPU with one synchronous call per image row.  Here
+// the pre-processed stack stays in HBM, a projection-matching pass is a fixed
+// sequence of kernels and cuFFT calls captured once into a CUDA graph, and only
+// the pass's largest shift, the rotation-centre z and the shifts come back to
+// the host after each pass.
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+
+#include "mf_series.hpp"
+#include "mf_xcorr.hpp"
+
+using namespace mf;
+
+mf_context::~mf_context() {
+  for (auto& kv : plans) cufftDestroy(kv.second);
+  plans.clear();
+  if (c.stream) cudaStreamDestroy(c.stream);
+}
+
+int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
+  auto it = plans.find(key);
+  if (it != plans.end()) {
+    *out = it->second;
+    return MF_OK;
+  }
+  // key: kind (0 rows R2C in place, 1 rows C2R out of place, 2 2-D R2C in place,
+  //            3 2-D C2R in place), nx, ny, batch
+  long long kind = key[0];
+  int nx = (int)key[1], ny = (int)key[2], batch = (int)key[3];
+  int pad = (nx / 2 + 1) * 2, cmp = nx / 2 + 1;
+  cufftHandle h;
+  cufftResult r;
+  if (kind == 0) {
+    int n[1] = {nx}, inem[1] = {pad}, onem[1] = {cmp};
+    r = cufftPlanMany(&h, 1, n, inem, 1, pad, onem, 1, cmp, CUFFT_R2C, batch);
+  } else if (kind == 1) {
+    int n[1] = {nx}, inem[1] = {cmp}, onem[1] = {nx};
+    r = cufftPlanMany(&h, 1, n, inem, 1, cmp, onem, 1, nx, CUFFT_C2R, batch);
+  } else if (kind == 2) {
+    int n[2] = {ny, nx}, inem[2] = {ny, pad}, onem[2] = {ny, cmp};
+    r = cufftPlanMany(&h, 2, n, inem, 1, ny * pad, onem, 1, ny * cmp, CUFFT_R2C, batch);
+  } else {
+    int n[2] = {ny, nx}, inem[2] = {ny, cmp}, onem[2] = {ny, pad};
+    r = cufftPlanMany(&h, 2, n, inem, 1, ny * cmp, onem, 1, ny * pad, CUFFT_C2R, batch);
+  }
+  if (r != CUFFT_SUCCESS)
+    return set_error(MF_ERR_CUFFT, "cufftPlanMany(kind %lld, %d x %d, batch %d) failed: %d", kind,
+                     nx, ny, batch, (int)r);
+  cufftSetStream(h, c.stream);
+  plans[key] = h;
+  *out = h;
+  return MF_OK;
+}
+
+namespace mf {
+
+ProjAlignState::~ProjAlignState() {
+  if (graph) cudaGraphExecDestroy(graph);
+  graph = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_pad_copy(const float* __restrict__ src, int w, int h, int pad,
+                           float* __restrict__ dst) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int z = blockIdx.z;
+  if (x >= pad || y >= h) return;
+  dst[((size_t)z * h + y) * pad + x] = (x < w) ? src[((size_t)z * h + y) * w + x] : 0.0f;
+}
+
+int series_init(mf_series* s, mf_context* ctx, int nx, int ny, int nz, const float* file_angles) {
+  s->ctx = ctx;
+  s->nx = nx;
+  s->ny = ny;
+  s->nz = nz;
+  s->file_angles.assign(file_angles, file_angles + nz);
+  s->angles = s->file_angles;
+  if (nz > 1 && s->angles[0] > s->angles[1]) std::reverse(s->angles.begin(), s->angles.end());
+  s->sx.assign(nz, 0.0f);
+  s->sy.assign(nz, 0.0f);
+  s->rot.assign(nz, 0.0f);
+  s->angle_offset = 0.0f;
+  MF_TRY(s->d_sx.alloc(sizeof(float) * nz));
+  MF_TRY(s->d_sy.alloc(sizeof(float) * nz));
+  MF_TRY(s->d_rot.alloc(sizeof(float) * nz));
+  MF_TRY(s->d_angles.alloc(sizeof(float) * nz));
+  return MF_OK;
+}
+
+}  // namespace mf
+
+int mf_series::upload_params() {
+  cudaStream_t st = ctx->c.stream;
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_sx.p, sx.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_sy.p, sy.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_rot.p, rot.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_angles.p, angles.data(), sizeof(float) * nz,
+                                cudaMemcpyHostToDevice, st));
+  return MF_OK;
+}
+
+int mf_series::download_shifts() {
+  cudaStream_t st = ctx->c.stream;
+  MF_CHECK_CUDA(cudaMemcpyAsync(sx.data(), d_sx.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(sy.data(), d_sy.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+namespace mf {
+
+// ---------------------------------------------------------------------------
+// Transform::DoIt (Transform.cpp:91-188), all tilt pairs batched.
+int transform_doit(mf_series* s, float* max_err_out) {
+  Context* c = &s->ctx->c;
+  cudaStream_t st = c->stream;
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  TransformState& T = s->tr;
+  if (!T.ready) {
+    int bx = (int)((float)nx / 1024.0f + 0.1f), by = (int)((float)ny / 1024.0f + 0.1f);
+    T.bin = std::max(1, std::max(bx, by));
+    T.xb = nx / T.bin / 2 * 2;
+    T.yb = ny / T.bin / 2 * 2;
+    T.pshx.assign(nz, 0.0f);
+    T.pshy.assign(nz, 0.0f);
+    T.ready = true;
+  }
+  const int xb = T.xb, yb = T.yb, pad = xb + 2, cmp = xb / 2 + 1;
+  const size_t bpix = (size_t)xb * yb, ppix = (size_t)pad * yb;
+  MF_TRY(s->upload_params());
+  DevBuf corr, pbuf, refs, imgs, part, stats, d_idx, d_refidx, d_mats, d_shifts, d_peakpart;
+  MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
+  MF_TRY(pbuf.alloc(sizeof(float) * ppix * nz));
+  MF_TRY(refs.alloc(sizeof(float) * ppix * nz));
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), nx, ny, nullptr, nz, s->d_sx.as<float>(),
+                            s->d_sy.as<float>(), s->d_rot.as<float>(), 1, T.bin, 1,
+                            corr.as<float>(), xb, bpix, st));
+  k_pad_copy<<<dim3((pad + 63) / 64, (yb + 3) / 4, nz), dim3(64, 4), 0, st>>>(
+      corr.as<float>(), xb, yb, pad, pbuf.as<float>());
+  c->launches++;
+  // pairs
+  std::vector<int> img_idx, ref_idx;
+  std::vector<float> mats;
+  for (int z = 0; z < nz; ++z) {
+    int r = find_ref_index(nz, s->angles.data(), z);
+    if (r == z) continue;
+    img_idx.push_back(z);
+    ref_idx.push_back(r);
+    double ds = std::cos(kD2R * s->angles[r]) / std::cos(kD2R * s->angles[z]);
+    float m[3];
+    stretch_matrix((float)ds, s->rot[z], m);
+    mats.insert(mats.end(), m, m + 3);
+  }
+  const int np = (int)img_idx.size();
+  float maxerr = 0.0f;
+  if (np > 0) {
+    MF_TRY(imgs.alloc(sizeof(float) * ppix * np));
+    MF_TRY(part.alloc(sizeof(double2) * kMomentParts * std::max(nz, np)));
+    MF_TRY(stats.alloc(sizeof(float2) * std::max(nz, np)));
+    MF_TRY(d_idx.alloc(sizeof(int) * np));
+    MF_TRY(d_refidx.alloc(sizeof(int) * np));
+    MF_TRY(d_mats.alloc(sizeof(float) * 3 * np));
+    MF_TRY(d_shifts.alloc(sizeof(float2) * np));
+    MF_TRY(d_peakpart.alloc(sizeof(float2) * 32 * np));
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, img_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_refidx.p, ref_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_mats.p, mats.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
+    const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
+    // references: normalise (mean, std) + round edge, all tilts
+    MF_TRY(norm_mask_pad(c, pbuf.as<float>(), pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy, msx,
+                         msy, 4.0f, refs.as<float>(), part.as<double2>(), stats.as<float2>(), st));
+    // images: stretch the padded raw copy, then normalise + round edge
+    MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
+                        np, 1, imgs.as<float>(), ppix, st));
+    MF_TRY(norm_mask_pad(c, imgs.as<float>(), pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy, msx,
+                         msy, 4.0f, imgs.as<float>(), part.as<double2>(), stats.as<float2>(), st));
+    cufftHandle fr, fi, inv;
+    MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));
+    MF_TRY(s->ctx->plan({2, xb, yb, np}, &fi));
+    MF_TRY(s->ctx->plan({3, xb, yb, np}, &inv));
+    MF_CHECK_CUFFT(cufftExecR2C(fr, refs.as<cufftReal>(), refs.as<cufftComplex>()));
+    MF_CHECK_CUFFT(cufftExecR2C(fi, imgs.as<cufftReal>(), imgs.as<cufftComplex>()));
+    float scale = (float)(1.0 / ((cmp - 1) * 2) / yb);
+    MF_TRY(xcorr_filter(c, refs.as<cufftComplex>(), ppix / 2, d_refidx.as<int>(),
+                        imgs.as<cufftComplex>(), ppix / 2, np, cmp, yb, 400.0f, scale, st));
+    MF_CHECK_CUFFT(cufftExecC2R(inv, imgs.as<cufftComplex>(), imgs.as<cufftReal>()));
+    MF_TRY(cc_peaks(c, imgs.as<float>(), ppix, pad, xb, yb, np, d_peakpart.as<float2>(),
+                    d_shifts.as<float2>(), st));
+    std::vector<float2> sh(np);
+    MF_CHECK_CUDA(cudaMemcpyAsync(sh.data(), d_shifts.p, sizeof(float2) * np, cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaStreamSynchronize(st));
+    float binx = nx * 1.0f / xb, biny = ny * 1.0f / yb;
+    for (int p = 0; p < np; ++p) {
+      int z = img_idx[p];
+      T.pshx[z] = sh[p].x * binx;
+      T.pshy[z] = sh[p].y * biny;
+      float e = (float)std::sqrt(T.pshx[z] * T.pshx[z] + T.pshy[z] * T.pshy[z]);
+      if (e > maxerr) maxerr = e;
+    }
+  }
+  // UpdateShift (Transform.cpp:130-188)
+  int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
+  for (int i = 0; i < nz; ++i) {
+    T.pshx[i] -= T.pshx[zt];
+    T.pshy[i] -= T.pshy[zt];
+  }
+  auto unstretch = [&](int ref, int f, float* sum) {
+    double ds = std::cos(s->angles[ref] * kD2R) / std::cos(s->angles[f] * kD2R);
+    double d2t = 2 * kD2R * s->rot[f];
+    double s2 = std::sin(d2t), c2 = std::cos(d2t);
+    double P = 0.5 * (ds + 1), M = 0.5 * (ds - 1);
+    float a0 = (float)(P + M * c2), a1 = (float)(1 * M * s2), a2 = (float)(P - M * c2);
+    float det = a0 * a2 - a1 * a1;
+    float m0 = a2 / det, m1 = -a1 / det, m2 = a0 / det;
+    float buf = sum[0] * m0 + sum[1] * m1;
+    sum[1] = sum[0] * m1 + sum[1] * m2;
+    sum[0] = buf;
+  };
+  float sum[2] = {0.0f, 0.0f};
+  for (int i = zt - 1; i >= 0; --i) {
+    sum[0] += T.pshx[i];
+    sum[1] += T.pshy[i];
+    unstretch(i + 1, i, sum);
+    s->sx[i] += sum[0];
+    s->sy[i] += sum[1];
+  }
+  sum[0] = sum[1] = 0.0f;
+  for (int i = zt + 1; i < nz; ++i) {
+    sum[0] += T.pshx[i];
+    sum[1] += T.pshy[i];
+    unstretch(i - 1, i, sum);
+    s->sx[i] += sum[0];
+    s->sy[i] += sum[1];
+  }
+  if (max_err_out) *max_err_out = maxerr;
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CalcTIltAxis::DoIt (Rotate.cu:333-415, 509-528)
+int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
+  if (num < 2) return set_error(MF_ERR_ARG, "tilt axis: need at least 2 candidates");
+  Context* c = &s->ctx->c;
+  const int nz = s->nz;
+  int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
+  float axis0 = s->rot[zt];
+  float step = range / (num - 1);
+  std::vector<float> cand(num);
+  cand[0] = axis0 - step * num / 2;
+  for (int i = 1; i < num; ++i) cand[i] = cand[i - 1] + step;
+  float fmin_size = 1e20f;
+  for (int i = 0; i < num; ++i) {
+    float fs = (float)std::fabs(std::sin(kD2R * cand[i]));
+    float fc = (float)std::fabs(std::cos(kD2R * cand[i]));
+    float s1 = (float)s->nx / (fs + 0.000001f);
+    float s2 = (float)s->ny / (fc + 0.000001f);
+    if (fmin_size > s1) fmin_size = s1;
+    if (fmin_size > s2) fmin_size = s2;
+  }
+  int L = (int)fmin_size;
+  L = L / 2 * 2 - 100;
+  if (L < 4) return set_error(MF_ERR_ARG, "tilt axis: image too small (line length %d)", L);
+  std::vector<float> scores;
+  MF_TRY(tilt_axis_scores(c, s->stack.as<float>(), s->nx, s->ny, nz, s->angles.data(),
+                          s->sx.data(), s->sy.data(), zt, cand.data(), num, L, &scores,
+                          c->stream));
+  int best = 0;
+  float bs = 0.0f;
+  for (int i = 0; i < num; ++i)
+    if (bs < scores[i]) {
+      bs = scores[i];
+      best = i;
+    }
+  float axis = cand[best];
+  if (axis < -45 && s->rot[0] == 0) axis += 180.0f;
+  if (axis > 135) axis -= 180.0f;
+  for (int i = 0; i < nz; ++i) s->rot[i] = axis;
+  if (axis_out) *axis_out = axis;
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FindOffset::DoIt (FindOffset.cu:85-238)
+int find_offset(mf_series* s, float* offset_out) {
+  Context* c = &s->ctx->c;
+  cudaStream_t st = c->stream;
+  const int nx = s->nx, ny = s->ny, nz = s->nz, bin = 4;
+  const int xb = nx / bin / 2 * 2, yb = ny / bin / 2 * 2;
+  if (xb < 2 || yb < 2) return set_error(MF_ERR_ARG, "find offset: image too small");
+  const size_t bpix = (size_t)xb * yb;
+  MF_TRY(s->upload_params());
+  DevBuf corr, d_pairs, d_out;
+  MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), nx, ny, nullptr, nz, s->d_sx.as<float>(),
+                            s->d_sy.as<float>(), s->d_rot.as<float>(), 0, bin, 0,
+                            corr.as<float>(), xb, bpix, st));
+  const int num = 31;
+  std::vector<float> a = s->angles;
+  std::vector<OffsetPair> pairs;
+  std::vector<int> first(num + 1, 0);
+  for (int n = 0; n < num; ++n) {
+    float off = 0.0f + (n - num / 2) * 1.0f;
+    for (int z = 0; z < nz; ++z) a[z] += off;
+    int zt = frame_idx_from_tilt(nz, a.data(), 0.0f);
+    first[n] = (int)pairs.size();
+    for (int i = 0; i < nz; ++i) {
+      if (i == zt) continue;
+      int r = (i < zt) ? i + 1 : i - 1;
+      double ds = std::cos(kD2R * a[r]) / std::cos(kD2R * a[i]);
+      float m[3];
+      stretch_matrix((float)ds, 0.0f, m);
+      pairs.push_back(OffsetPair{r, i, m[0], m[1], m[2]});
+    }
+    for (int z = 0; z < nz; ++z) a[z] -= off;
+  }
+  first[num] = (int)pairs.size();
+  const int np = (int)pairs.size();
+  MF_TRY(d_pairs.alloc(sizeof(OffsetPair) * np));
+  MF_TRY(d_out.alloc(sizeof(double) * 6 * np));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_pairs.p, pairs.data(), sizeof(OffsetPair) * np,
+                                cudaMemcpyHostToDevice, st));
+  MF_TRY(offset_moments(c, corr.as<float>(), xb, yb, d_pairs.as<OffsetPair>(), np,
+                        d_out.as<double>(), st));
+  std::vector<double> mom((size_t)6 * np);
+  MF_CHECK_CUDA(cudaMemcpyAsync(mom.data(), d_out.p, sizeof(double) * 6 * np,
+                                cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  float maxcc = 0.0f, best = 0.0f;
+  for (int n = 0; n < num; ++n) {
+    float off = 0.0f + (n - num / 2) * 1.0f;
+    float ccsum = 0.0f;
+    int count = 0;
+    for (int p = first[n]; p < first[n + 1]; ++p) {
+      float f[6];
+      for (int k = 0; k < 6; ++k) f[k] = (float)mom[(size_t)6 * p + k];
+      for (int k = 0; k < 5; ++k) f[k] /= f[5];
+      // the reference subtracts the mean itself, not its square (FindOffset.cu:214-215)
+      double s1 = f[2] - f[0], s2 = f[3] - f[1];
+      double cc = f[4] - f[0] * f[1];
+      if (s1 < 0) s1 = 0;
+      if (s2 < 0) s2 = 0;
+      s1 = std::sqrt(s1);
+      s2 = std::sqrt(s2);
+      cc = cc / (s1 * s2 + 1e-30);
+      if (cc < -1)
+        cc = -1;
+      else if (cc > 1)
+        cc = 1;
+      ccsum += (float)cc;
+      count++;
+    }
+    float mcc = ccsum / count;
+    if (mcc > maxcc) {
+      maxcc = mcc;
+      best = off;
+    }
+  }
+  s->angle_offset += best;
+  if (offset_out) *offset_out = best;
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ProjAlign::Setup / Setsize (ProjAlign.cpp:126-203) plus the precomputation
+// that the reference repeats for every pass: processing order, neighbour
+// ranges and the re-projection operators.
+int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
+  Context* c = &s->ctx->c;
+  cudaStream_t st = c->stream;
+  if (nproj <= 0) return set_error(MF_ERR_ARG, "nproj must be > 0");
+  ProjAlignState& P = s->pa;
+  if (P.graph) {
+    cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+  }
+  P.ready = false;
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  int bx = (int)((float)nx / 2048.0f + 0.5f), by = (int)((float)ny / 2048.0f + 0.5f);
+  P.bin = std::max(1, std::max(bx, by));
+  P.xb = nx / P.bin / 2 * 2;
+  P.yb = ny / P.bin / 2 * 2;
+  P.pad = (P.xb / 2 + 1) * 2;
+  P.cmp = P.pad / 2;
+  P.thick = align_z / P.bin / 2 * 2;
+  P.nproj = nproj;
+  P.z0 = zshift;
+  if (P.thick < 2) return set_error(MF_ERR_ARG, "slab thickness %d too small", P.thick);
+  const int xb = P.xb, yb = P.yb;
+  const size_t bpix = (size_t)xb * yb, ppix = (size_t)P.pad * yb;
+  MF_TRY(P.corr.alloc(sizeof(float) * bpix * nz));
+  MF_TRY(P.scratch.alloc(sizeof(float) * ppix * nz));
+  MF_TRY(P.reproj.alloc(sizeof(float) * bpix));
+  MF_TRY(P.ccbuf.alloc(sizeof(float) * ppix * 2));
+  MF_TRY(P.part.alloc(sizeof(double2) * kMomentParts * 2 + sizeof(float2) * kPeakParts));
+  MF_TRY(P.stats.alloc(sizeof(float2) * 2));
+  // outward order (ProjAlign.cpp:229-254) and neighbour ranges
+  P.zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
+  std::vector<unsigned char> skip(nz, 1);
+  skip[P.zt] = 0;
+  P.order.clear();
+  P.geom.clear();
+  P.ops.clear();
+  for (int i = 1; i < nz; ++i) {
+    for (int side = 0; side < 2; ++side) {
+      int ip = side == 0 ? P.zt + i : P.zt - i;
+      if (ip < 0 || ip >= nz) continue;
+      int rg[2];
+      find_proj_range(s->angles.data(), nz, skip.data(), ip, nproj, rg);
+      if (rg[0] < 0 || rg[1] < 0)
+        return set_error(MF_ERR_GEOMETRY,
+                         "no already-aligned tilt within 20.5 degrees of tilt %d (%.2f)", ip,
+                         s->angles[ip]);
+      ReprojGeom g;
+      reproj_geometry(s->angles.data(), ip, rg[0], rg[1], xb, yb, P.thick, &g);
+      P.order.push_back(ip);
+      P.geom.push_back(g);
+      skip[ip] = 0;
+    }
+  }
+  const int n = (int)P.order.size();
+  P.ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
+  MF_TRY(P.d_order.alloc(sizeof(int) * std::max(n, 1)));
+  MF_TRY(P.d_err.alloc(sizeof(float) * nz));
+  MF_TRY(P.d_z0.alloc(sizeof(float)));
+  MF_TRY(P.d_maxerr.alloc(sizeof(float)));
+  MF_TRY(P.d_meas.alloc(sizeof(float) * 2 * nz));
+  MF_TRY(P.d_rowflags.alloc(sizeof(int) * std::max(1, n * P.ytiles)));
+  P.bp_off.assign(n, 0);
+  std::vector<float> bp;
+  for (int k = 0; k < n; ++k) {
+    P.bp_off[k] = bp.size();
+    bp.insert(bp.end(), P.geom[k].bp.begin(), P.geom[k].bp.end());
+  }
+  MF_TRY(P.d_bp.alloc(sizeof(float) * std::max<size_t>(bp.size(), 1)));
+  if (n > 0) {
+    MF_CHECK_CUDA(cudaMemcpyAsync(P.d_order.p, P.order.data(), sizeof(int) * n,
+                                  cudaMemcpyHostToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(P.d_bp.p, bp.data(), sizeof(float) * bp.size(),
+                                  cudaMemcpyHostToDevice, st));
+  }
+  MF_CHECK_CUDA(cudaMemsetAsync(P.d_err.p, 0, sizeof(float) * nz, st));
+  MF_CHECK_CUDA(cudaMemsetAsync(P.d_meas.p, 0, sizeof(float) * 2 * nz, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(P.d_z0.p, &P.z0, sizeof(float), cudaMemcpyHostToDevice, st));
+  if (P.method == 1) {
+    for (int k = 0; k < n; ++k) {
+      P.ops.emplace_back(new ReprojOp());
+      MF_TRY(build_reproj_op(c, P.geom[k], P.ops.back().get(), st));
+    }
+  }
+  // FFT plans
+  MF_TRY(s->ctx->plan({0, xb, yb, (long long)nz * yb}, &P.rows_fwd_all));
+  MF_TRY(s->ctx->plan({1, xb, yb, (long long)nz * yb}, &P.rows_inv_all));
+  MF_TRY(s->ctx->plan({0, xb, yb, yb}, &P.rows_fwd_one));
+  MF_TRY(s->ctx->plan({1, xb, yb, yb}, &P.rows_inv_one));
+  MF_TRY(s->ctx->plan({2, xb, yb, 2}, &P.cc_fwd));
+  MF_TRY(s->ctx->plan({3, xb, yb, 1}, &P.cc_inv));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  P.ready = true;
+  return MF_OK;
+}
+
+// Queue one projection-matching pass (ProjAlign::DoItBin, ProjAlign.cpp:211-257).
+static int pa_enqueue(mf_series* s) {
+  Context* c = &s->ctx->c;
+  cudaStream_t st = c->stream;
+  ProjAlignState& P = s->pa;
+  const int nz = s->nz, xb = P.xb, yb = P.yb, pad = P.pad, cmp = P.cmp;
+  const size_t bpix = (size_t)xb * yb, ppix = (size_t)pad * yb;
+  const int n = (int)P.order.size();
+  float* corr = P.corr.as<float>();
+  float* scratch = P.scratch.as<float>();
+  float* cc = P.ccbuf.as<float>();
+  double2* mpart = P.part.as<double2>();
+  float2* ppart = reinterpret_cast<float2*>(mpart + kMomentParts * 2);
+  float2* stats = P.stats.as<float2>();
+  MF_CHECK_CUDA(cudaMemsetAsync(P.d_rowflags.p, 0, sizeof(int) * std::max(1, n * P.ytiles), st));
+  // CorrTomoStack::DoIt: resample + bin + R-weight every tilt (CorrStack.cu:353-397)
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, nullptr, nz,
+                            s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
+                            P.bin, 1, scratch, pad, ppix, st));
+  MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_all, scratch, (cufftComplex*)scratch));
+  MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, nz * yb, st));
+  MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_all, (cufftComplex*)scratch, corr));
+  // FitRotCenterZ + RemoveOffsetZ(-1)
+  MF_TRY(fit_z0(c, nz, P.zt, s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
+                s->d_rot.as<float>(), P.d_z0.as<float>(), st));
+  for (int k = 0; k < n; ++k) {
+    const int ip = P.order[k];
+    const ReprojGeom& g = P.geom[k];
+    int* rowflags = P.d_rowflags.as<int>() + (size_t)k * P.ytiles;
+    float* reproj = P.reproj.as<float>();
+    if (P.method == 1) {
+      MF_TRY(launch_reproject_apply(c, *P.ops[k], corr, bpix, rowflags, reproj, st));
+      MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
+                                    g.nk, g.fcos, g.fsin, g.ray_len, g.thick, rowflags, reproj,
+                                    st));
+    } else {
+      MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
+                                    g.nk, g.fcos, g.fsin, g.ray_len, g.thick, nullptr, reproj,
+                                    st));
+    }
+    // MeaAlignProj: PANorm both, FFT, filter, inverse FFT, peak
+    const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
+    MF_TRY(norm_mask_pad(c, reproj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad, (float)yb,
+                         4.0f, cc, mpart, stats, st));
+    MF_TRY(norm_mask_pad(c, corr + (size_t)ip * bpix, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy,
+                         (float)pad, (float)yb, 4.0f, cc + ppix, mpart + kMomentParts, stats + 1,
+                         st));
+    MF_CHECK_CUFFT(cufftExecR2C(P.cc_fwd, cc, (cufftComplex*)cc));
+    MF_TRY(xcorr_filter(c, (cufftComplex*)cc, 0, nullptr, (cufftComplex*)(cc + ppix), 0, 1, cmp,
+                        yb, 500.0f, 1.0f, st));
+    MF_CHECK_CUFFT(cufftExecC2R(P.cc_inv, (cufftComplex*)(cc + ppix), cc + ppix));
+    MF_TRY(pa_peak_update(c, cc + ppix, pad, xb, yb, ppart, ip, s->nx, s->ny,
+                          s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
+                          s->d_rot.as<float>(), P.d_z0.as<float>(), P.d_err.as<float>(),
+                          P.d_meas.as<float>(), st));
+    // re-correct the aligned tilt (mCorrectProj)
+    MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, P.d_order.as<int>() + k, 1,
+                              s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
+                              P.bin, 1, scratch, pad, ppix, st));
+    MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_one, scratch, (cufftComplex*)scratch));
+    MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, yb, st));
+    MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_one, (cufftComplex*)scratch, corr + (size_t)ip * bpix));
+  }
+  MF_TRY(max_err(c, P.d_err.as<float>(), P.d_order.as<int>(), n, P.d_maxerr.as<float>(), st));
+  return MF_OK;
+}
+
+int projalign_doit(mf_series* s, float* max_err_out) {
+  ProjAlignState& P = s->pa;
+  if (!P.ready) return set_error(MF_ERR_STATE, "projection matching is not set up");
+  Context* c = &s->ctx->c;
+  cudaStream_t st = c->stream;
+  MF_TRY(s->upload_params());
+  if (P.use_graph && !P.graph) {
+    // Capture once; the graph reads parameters from device memory, so every
+    // later pass replays it unchanged.
+    int64_t l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = pa_enqueue(s);
+    cudaError_t ec = cudaStreamEndCapture(st, &g);
+    P.graph_kernels = c->launches - l0;
+    c->launches = l0;
+    if (rc != MF_OK || ec != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      P.use_graph = false;  // run eagerly from now on
+    } else {
+      cudaError_t ei = cudaGraphInstantiate(&P.graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) {
+        cudaGetLastError();
+        P.graph = nullptr;
+        P.use_graph = false;
+      }
+    }
+  }
+  if (P.graph) {
+    MF_CHECK_CUDA(cudaGraphLaunch(P.graph, st));
+    c->launches += P.graph_kernels;
+  } else {
+    MF_TRY(pa_enqueue(s));
+  }
+  float res[2];
+  MF_CHECK_CUDA(cudaMemcpyAsync(&res[0], P.d_maxerr.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(&res[1], P.d_z0.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+  MF_TRY(s->download_shifts());
+  P.z0 = res[1];
+  if (max_err_out) *max_err_out = res[0];
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Process::mCoarseAlign (Process.cpp:238-270)
+int coarse_align(mf_series* s, float pitch_angle, float offset) {
+  if (pitch_angle == 0) {
+    s->tr.ready = false;
+    for (int i = 1; i <= 3; ++i) {
+      float e, ax;
+      MF_TRY(transform_doit(s, &e));
+      MF_TRY(tilt_axis(s, 180.0f / i, 100, &ax));
+    }
+  } else {
+    for (int i = 0; i < s->nz; ++i) s->rot[i] = pitch_angle;
+  }
+  if (offset == 0) {
+    float o;
+    MF_TRY(find_offset(s, &o));
+  } else {
+    s->angle_offset = offset;
+  }
+  for (int z = 0; z < s->nz; ++z) s->angles[z] += s->angle_offset;
+  return MF_OK;
+}
+
+// Process::mProjAlign + ProjAlignOnce (Process.cpp:272-319)
+int proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes) {
+  for (int i = 0; i < s->nz; ++i) {
+    s->sx[i] = 0.0f;
+    s->sy[i] = 0.0f;
+  }
+  MF_TRY(projalign_setup(s, zshift, align_z, nproj));
+  int np = 0;
+  auto once = [&]() -> int {
+    float last;
+    MF_TRY(projalign_doit(s, &last));
+    np++;
+    for (int i = 1; i < 10; ++i) {
+      float e;
+      MF_TRY(projalign_doit(s, &e));
+      np++;
+      if (e <= last) {
+        if (e < 2.0f) break;
+        last = e;
+      }
+    }
+    return MF_OK;
+  };
+  MF_TRY(once());
+  for (int i = 1; i <= 4; ++i) {
+    float ax;
+    MF_TRY(tilt_axis(s, 20.0f / i, 100, &ax));
+    if (i == 1) MF_TRY(once());
+  }
+  MF_TRY(once());
+  if (passes) *passes = np;
+  return MF_OK;
+}
+
+// Process::CorrectStack (Process.cpp:329-372) into device memory.
+int correct_stack_device(mf_series* s, int out_bin, float* d_out) {
+  Context* c = &s->ctx->c;
+  if (out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
+  int xo = s->nx / out_bin / 2 * 2, yo = s->ny / out_bin / 2 * 2;
+  if (xo < 2 || yo < 2) return set_error(MF_ERR_ARG, "output binning too large");
+  MF_TRY(s->upload_params());
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, nullptr, s->nz,
+                            s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
+                            out_bin, 1, d_out, xo, (size_t)xo * yo, c->stream));
+  return MF_OK;
+}
+
+}  // namespace mf

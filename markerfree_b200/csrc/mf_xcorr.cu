@@ -1,0 +1,549 @@
+// Cross-correlation kernels around cuFFT: normalise/mask/pad, spectrum filter,
+// peak search with sub-pixel fit, and the per-tilt parameter update.
+//
+// Reference: Markerfree/src/method/CalcCC.cu (GSum2D/GSum1D :48-92, GConv,
+// GWiener, GCenterOrigin :95-135, GNormalize :137-147, GStretchRandom :149-171,
+// GRoundEdge :173-195, FindPeak :381-435) and ProjAlign.cpp (PANorm :373-390,
+// PAFindPeak :403-453, ClacAlignProj :259-319, FitRotCenterZ/RemoveOffsetZ
+// :537-579).  The reference copies every cross-correlation map to the host and
+// scans it on one CPU thread; here the arg-max, the parabolic fit and the
+// parameter update run on the GPU and nothing leaves the device.
+#include "mf_internal.hpp"
+#include "mf_xcorr.hpp"
+
+namespace mf {
+
+constexpr int kRedBlocks = 64;  // partial-sum blocks per image (fixed: deterministic)
+
+// Masked moments: part[img][blk] = (sum v, sum v^2) over valid pixels.
+__global__ void k_moments(const float* __restrict__ src, int w, int h, int stride,
+                          size_t img_stride, double2* __restrict__ part) {
+  __shared__ double s1[256], s2[256];
+  const float* p = src + (size_t)blockIdx.y * img_stride;
+  double a = 0.0, b = 0.0;
+  const size_t n = (size_t)w * h;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int y = (int)(i / w), x = (int)(i % w);
+    float v = p[(size_t)y * stride + x];
+    if (v < -1e10f) continue;
+    a += v;
+    b += (double)__fmul_rn(v, v);
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
+    if (threadIdx.x < hh) {
+      s1[threadIdx.x] += s1[threadIdx.x + hh];
+      s2[threadIdx.x] += s2[threadIdx.x + hh];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(s1[0], s2[0]);
+}
+
+// stats[img] = (mean, std).  with_std = 0: std = 1 (PANorm); 1: CalcCC::mNormalize.
+__global__ void k_moments_final(const double2* __restrict__ part, int nblk, int w, int h,
+                                int with_std, float2* __restrict__ stats) {
+  if (threadIdx.x != 0) return;
+  const double2* p = part + (size_t)blockIdx.x * nblk;
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < nblk; ++i) {
+    a += p[i].x;
+    b += p[i].y;
+  }
+  double n = (double)w * (double)h;
+  float mean = (float)(a / n);
+  float sd = 1.0f;
+  if (with_std) {
+    float m2 = (float)(b / n);
+    sd = __fsub_rn(m2, __fmul_rn(mean, mean));
+    sd = (sd <= 0.0f) ? 0.0f : sqrtf(sd);
+  }
+  stats[blockIdx.x] = make_float2(mean, sd);
+}
+
+// Normalise with stats, apply GRoundEdge, zero the pad columns; reads rows of
+// `src_stride` floats (first w used) and writes rows of `pad` floats.
+__global__ void k_norm_mask(const float* __restrict__ src, int src_stride, size_t src_img_stride,
+                            int w, int h, int pad, size_t dst_img_stride,
+                            const float2* __restrict__ stats, float cx, float cy, float msx,
+                            float msy, float power, float* __restrict__ dst) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int img = blockIdx.z;
+  if (x >= pad || y >= h) return;
+  float* d = dst + (size_t)img * dst_img_stride + (size_t)y * pad + x;
+  if (x >= w) {
+    *d = 0.0f;
+    return;
+  }
+  float v = src[(size_t)img * src_img_stride + (size_t)y * src_stride + x];
+  float2 st = stats[img];
+  if (!(v < -1e10f)) v = __fdiv_rn(__fsub_rn(v, st.x), st.y);  // GNormalize
+  if (v < -1e10f) {                                             // GRoundEdge
+    *d = 0.0f;
+    return;
+  }
+  float fx = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)x, cx))), msx);
+  float fy = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)y, cy))), msy);
+  float fr = sqrtf(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)));
+  if (fr >= 1.0f) {
+    *d = 0.0f;
+    return;
+  }
+  fr = __fmul_rn(0.5f, __fsub_rn(1.0f, (float)cos((double)__fmul_rn(3.1415926f, fr))));
+  fr = __fsub_rn(1.0f, powf(fr, power));
+  *d = __fmul_rn(v, fr);
+}
+
+int norm_mask_pad(Context* c, const float* src, int src_stride, size_t src_img_stride, int w,
+                  int h, int pad, size_t dst_img_stride, int nimg, int with_std, float cx,
+                  float cy, float msx, float msy, float power, float* dst, double2* d_part,
+                  float2* d_stats, cudaStream_t st) {
+  dim3 g1(kRedBlocks, nimg);
+  k_moments<<<g1, 256, 0, st>>>(src, w, h, src_stride, src_img_stride, d_part);
+  k_moments_final<<<nimg, 32, 0, st>>>(d_part, kRedBlocks, w, h, with_std, d_stats);
+  dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
+  k_norm_mask<<<grd, blk, 0, st>>>(src, src_stride, src_img_stride, w, h, pad, dst_img_stride,
+                                   d_stats, cx, cy, msx, msy, power, dst);
+  c->launches += 3;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// conj(R) * I, B-factor / amplitude (Wiener-like) filter and origin centring,
+// written over I.  `scale` reproduces GMultiplyFactor (1/N after each R2C) when
+// != 1.  Pair p uses ref spectrum ref + idx[p]*ref_stride (idx[p] = p when idx is
+// null) and image img + p*img_stride.
+__global__ void k_xcorr_filter(const cufftComplex* __restrict__ ref, size_t ref_stride,
+                               const int* __restrict__ ref_idx, cufftComplex* __restrict__ img,
+                               size_t img_stride, int cmp, int ny, float bfactor, float scale) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cmp || y >= ny) return;
+  size_t i = (size_t)y * cmp + x;
+  const int ri = ref_idx ? ref_idx[blockIdx.z] : (int)blockIdx.z;
+  cufftComplex A = ref[(size_t)ri * ref_stride + i];
+  cufftComplex* Bp = img + (size_t)blockIdx.z * img_stride + i;
+  cufftComplex B = *Bp;
+  if (scale != 1.0f) {
+    A.x = __fmul_rn(A.x, scale);
+    A.y = __fmul_rn(A.y, scale);
+    B.x = __fmul_rn(B.x, scale);
+    B.y = __fmul_rn(B.y, scale);
+  }
+  float re = __fadd_rn(__fmul_rn(A.x, B.x), __fmul_rn(A.y, B.y));
+  float im = __fsub_rn(__fmul_rn(A.x, B.y), __fmul_rn(A.y, B.x));
+  int yy = y;
+  if (yy > ny / 2) yy -= ny;
+  float fnx = __fmul_rn(2.0f, (float)(cmp - 1));
+  float filt = __fdiv_rn(__fmul_rn(-2.0f, bfactor),
+                         __fadd_rn(__fmul_rn(fnx, fnx), (float)(ny * ny)));
+  float k2 = (float)((unsigned)(x * x) + (unsigned)(yy * yy));
+  filt = (float)exp((double)__fmul_rn(filt, k2));
+  float amp = sqrtf(__fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im)));
+  filt = __fdiv_rn(filt, sqrtf(__fadd_rn(amp, 0.01f)));
+  re = __fmul_rn(re, filt);
+  im = __fmul_rn(im, filt);
+  if ((x + y) & 1) {
+    re = -re;
+    im = -im;
+  }
+  *Bp = make_cuComplex(re, im);
+}
+
+int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,
+                 cufftComplex* img, size_t img_stride, int npairs, int cmp, int ny, float bfactor,
+                 float scale, cudaStream_t st) {
+  dim3 blk(64, 4), grd((cmp + 63) / 64, (ny + 3) / 4, npairs);
+  k_xcorr_filter<<<grd, blk, 0, st>>>(ref, ref_stride, d_ref_idx, img, img_stride, cmp, ny,
+                                      bfactor, scale);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Arg-max over a window [sx, ex) x [sy, ey) of a real map (row stride `stride`).
+// Ties go to the smallest row-major index, as in the reference's scan.
+__device__ __forceinline__ bool better(float v, int i, float bv, int bi) {
+  return v > bv || (v == bv && i < bi);
+}
+
+__global__ void k_peak_partial(const float* __restrict__ map, size_t map_stride, int stride,
+                               int sx, int ex, int sy, int ey, float2* __restrict__ part) {
+  __shared__ float sv[256];
+  __shared__ int si[256];
+  const float* m = map + (size_t)blockIdx.y * map_stride;
+  const int w = ex - sx;
+  const int n = w * (ey - sy);
+  float bv = -INFINITY;
+  int bi = INT_MAX;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int y = sy + i / w, x = sx + i % w;
+    int li = y * stride + x;
+    float v = m[li];
+    if (better(v, li, bv, bi)) {
+      bv = v;
+      bi = li;
+    }
+  }
+  sv[threadIdx.x] = bv;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h && better(sv[threadIdx.x + h], si[threadIdx.x + h], sv[threadIdx.x],
+                                  si[threadIdx.x])) {
+      sv[threadIdx.x] = sv[threadIdx.x + h];
+      si[threadIdx.x] = si[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = make_float2(sv[0], __int_as_float(si[0]));
+}
+
+__device__ void reduce_partials(const float2* p, int n, float* bv, int* bi) {
+  float v = -INFINITY;
+  int idx = INT_MAX;
+  for (int i = 0; i < n; ++i) {
+    float pv = p[i].x;
+    int pi = __float_as_int(p[i].y);
+    if (better(pv, pi, v, idx)) {
+      v = pv;
+      idx = pi;
+    }
+  }
+  *bv = v;
+  *bi = idx;
+}
+
+// Integer peak from the reduced linear index.  When no pixel of the window
+// compared as a maximum (all NaN) the reference keeps its initial peak (0, 0),
+// whose neighbours lie outside the map; the window's first pixel is used instead.
+__device__ __forceinline__ void pa_window_peak(int bi, int stride, int xb, int yb, int* px,
+                                               int* py) {
+  if (bi == INT_MAX) {
+    int sx = xb / 20, sy = yb / 20;
+    *px = sx < 3 ? 3 : sx;
+    *py = sy < 3 ? 3 : sy;
+    return;
+  }
+  *px = bi % stride;
+  *py = bi / stride;
+}
+
+// ProjAlign.cpp:427-453: parabolic sub-pixel fit (FP64) around the integer peak.
+__device__ void pa_fit(const float* m, int stride, int px, int py, double* dx, double* dy,
+                       double* peak) {
+  int ic = py * stride + px;
+  float cxp = m[ic + 1], cxm = m[ic - 1], cyp = m[ic + stride], cym = m[ic - stride],
+        cc = m[ic];
+  double a = (double)__fadd_rn(cxp, cxm) * 0.5 - (double)cc;
+  double b = (double)__fsub_rn(cxp, cxm) * 0.5;
+  double c = (double)__fadd_rn(cyp, cym) * 0.5 - (double)cc;
+  double d = (double)__fsub_rn(cyp, cym) * 0.5;
+  double ddx = -b / (2 * a + 1e-30);
+  double ddy = -d / (2 * c + 1e-30);
+  if (fabs(ddx) > 1) ddx = 0;
+  if (fabs(ddy) > 1) ddy = 0;
+  *dx = ddx;
+  *dy = ddy;
+  *peak = a * ddx * ddx + b * ddx + c * ddy * ddy + d * ddy + (double)cc;
+}
+
+__device__ __forceinline__ void rot_shift(float in0, float in1, float angle_deg, float* o0,
+                                          float* o1) {
+  float c = (float)cos((double)angle_deg * kD2R);
+  float s = (float)sin((double)angle_deg * kD2R);
+  float sx = __fsub_rn(__fmul_rn(in0, c), __fmul_rn(in1, s));
+  float sy = __fadd_rn(__fmul_rn(in0, s), __fmul_rn(in1, c));
+  *o0 = sx;
+  *o1 = sy;
+}
+
+// ProjAlign.cpp:631-639
+__device__ __forceinline__ void z_induced(float z0, float angle, float rot, float* s0,
+                                          float* s1) {
+  *s0 = 0.0f;
+  *s1 = 0.0f;
+  if (z0 == 0.0f) return;
+  float t = (float)((double)angle * kD2R);
+  float a = (float)(-(double)z0 * sin((double)t));
+  rot_shift(a, 0.0f, rot, s0, s1);
+}
+
+// Final peak + ClacAlignProj update (ProjAlign.cpp:259-319) for held-out tilt ip.
+__global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int xb, int yb,
+                                 const float2* __restrict__ part, int nparts, int ip, int nx,
+                                 int ny, const float* __restrict__ angles, float* __restrict__ sx,
+                                 float* __restrict__ sy, const float* __restrict__ rot,
+                                 const float* __restrict__ z0p, float* __restrict__ err,
+                                 float* __restrict__ meas) {
+  if (threadIdx.x != 0) return;
+  float bv;
+  int bi;
+  reduce_partials(part, nparts, &bv, &bi);
+  int px = 0, py = 0;
+  pa_window_peak(bi, stride, xb, yb, &px, &py);
+  double dx, dy, pk;
+  pa_fit(map, stride, px, py, &dx, &dy, &pk);
+  float pkx = (float)(px + dx), pky = (float)(py + dy);
+  float shx = __fsub_rn(pkx, (float)(xb / 2));
+  float shy = __fsub_rn(pky, (float)(yb / 2));
+  float binx = __fdiv_rn((float)nx, (float)xb), biny = __fdiv_rn((float)ny, (float)yb);
+  float a0 = __fmul_rn(shx, binx), a1 = __fmul_rn(shy, biny);
+  float fs = __fadd_rn(__fmul_rn(a0, a0), __fmul_rn(a1, a1));
+  fs = sqrtf(fs);
+  float r = rot[ip];
+  rot_shift(a0, a1, r, &a0, &a1);
+  float i0, i1;
+  z_induced(*z0p, angles[ip], r, &i0, &i1);
+  a0 = __fadd_rn(a0, i0);
+  a1 = __fadd_rn(a1, i1);
+  sx[ip] = __fadd_rn(sx[ip], a0);
+  sy[ip] = __fadd_rn(sy[ip], a1);
+  err[ip] = fs;
+  if (meas) {
+    meas[2 * ip] = shx;
+    meas[2 * ip + 1] = shy;
+  }
+}
+
+int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
+                   int ip, int nx, int ny, const float* d_angles, float* d_sx, float* d_sy,
+                   const float* d_rot, const float* d_z0, float* d_err, float* d_meas,
+                   cudaStream_t st) {
+  int sx = xb / 20, sy = yb / 20;
+  if (sx < 3) sx = 3;
+  if (sy < 3) sy = 3;
+  int ex = xb - sx, ey = yb - sy;
+  const int nb = 64;
+  k_peak_partial<<<dim3(nb, 1), 256, 0, st>>>(map, 0, stride, sx, ex, sy, ey, d_part);
+  k_pa_peak_update<<<1, 32, 0, st>>>(map, stride, xb, yb, d_part, nb, ip, nx, ny, d_angles, d_sx,
+                                     d_sy, d_rot, d_z0, d_err, d_meas);
+  c->launches += 2;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Plain peak (PAFindPeak) returning the binned shift and peak value into out[3].
+__global__ void k_pa_peak_only(const float* __restrict__ map, int stride, int xb, int yb,
+                               const float2* __restrict__ part, int nparts, float* out) {
+  if (threadIdx.x != 0) return;
+  float bv;
+  int bi;
+  reduce_partials(part, nparts, &bv, &bi);
+  int px, py;
+  pa_window_peak(bi, stride, xb, yb, &px, &py);
+  double dx, dy, pk;
+  pa_fit(map, stride, px, py, &dx, &dy, &pk);
+  out[0] = __fsub_rn((float)(px + dx), (float)(xb / 2));
+  out[1] = __fsub_rn((float)(py + dy), (float)(yb / 2));
+  out[2] = (float)pk;
+}
+
+int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
+                 float* d_out, cudaStream_t st) {
+  int sx = xb / 20, sy = yb / 20;
+  if (sx < 3) sx = 3;
+  if (sy < 3) sy = 3;
+  const int nb = 64;
+  k_peak_partial<<<dim3(nb, 1), 256, 0, st>>>(map, 0, stride, sx, xb - sx, sy, yb - sy, d_part);
+  k_pa_peak_only<<<1, 32, 0, st>>>(map, stride, xb, yb, d_part, nb, d_out);
+  c->launches += 2;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// CalcCC::FindPeak (CalcCC.cu:381-435) for many maps: central 80% window, peak
+// clamped to [1, w-2] x [1, h-2], fit in float-promoted arithmetic.
+__global__ void k_cc_peak_final(const float* __restrict__ maps, size_t map_stride, int stride,
+                                int w, int h, const float2* __restrict__ part, int nparts,
+                                float2* __restrict__ shifts) {
+  if (threadIdx.x != 0) return;
+  const float* m = maps + (size_t)blockIdx.x * map_stride;
+  float bv;
+  int bi;
+  reduce_partials(part + (size_t)blockIdx.x * nparts, nparts, &bv, &bi);
+  int px = 0, py = 0;
+  if (bi != INT_MAX) {
+    px = bi % stride;
+    py = bi / stride;
+  }
+  if (px < 1)
+    px = 1;
+  else if (px > w - 2)
+    px = w - 2;
+  if (py < 1)
+    py = 1;
+  else if (py > h - 2)
+    py = h - 2;
+  int ic = py * stride + px;
+  float cc = m[ic];
+  double a = (double)__fsub_rn(__fmul_rn(__fadd_rn(m[ic + 1], m[ic - 1]), 0.5f), cc);
+  double b = (double)__fmul_rn(__fsub_rn(m[ic + 1], m[ic - 1]), 0.5f);
+  double c = (double)__fsub_rn(__fmul_rn(__fadd_rn(m[ic + stride], m[ic - stride]), 0.5f), cc);
+  double d = (double)__fmul_rn(__fsub_rn(m[ic + stride], m[ic - stride]), 0.5f);
+  double dx = -b / (2 * a + 1e-30), dy = -d / (2 * c + 1e-30);
+  if (fabs(dx) > 1) dx = 0;
+  if (fabs(dy) > 1) dy = 0;
+  shifts[blockIdx.x] = make_float2(__fsub_rn((float)(px + dx), (float)(w / 2)),
+                                   __fsub_rn((float)(py + dy), (float)(h / 2)));
+}
+
+int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w, int h, int nmaps,
+             float2* d_part, float2* d_shifts, cudaStream_t st) {
+  int ssx = w * 8 / 20 * 2, ssy = h * 8 / 20 * 2;
+  int sx = (w - ssx) / 2, sy = (h - ssy) / 2;
+  const int nb = 32;
+  k_peak_partial<<<dim3(nb, nmaps), 256, 0, st>>>(maps, map_stride, stride, sx, sx + ssx, sy,
+                                                  sy + ssy, d_part);
+  k_cc_peak_final<<<nmaps, 32, 0, st>>>(maps, map_stride, stride, w, h, d_part, nb, d_shifts);
+  c->launches += 2;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FitRotCenterZ + RemoveOffsetZ(-1) (ProjAlign.cpp:537-579, 641-657); the
+// reference's uninitialised accumulator dA is taken as 0.
+__global__ void k_fit_z0(int nz, int zt, const float* __restrict__ angles, float* sx, float* sy,
+                         const float* __restrict__ rot, float* z0p) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float s0x, s0y;
+  rot_shift(sx[zt], sy[zt], -rot[zt], &s0x, &s0y);
+  float cent0 = (float)((double)s0x / cos((double)angles[zt] * kD2R));
+  double dA = 0.0, dB = 0.0;
+  for (int i = 0; i < nz; ++i) {
+    float r0, r1;
+    rot_shift(sx[i], sy[i], -rot[i], &r0, &r1);
+    double ds = sin((double)angles[i] * kD2R), dc = cos((double)angles[i] * kD2R);
+    dA += ((double)cent0 * dc - (double)r0) * ds;
+    dB += ds * ds;
+  }
+  float z0 = (float)(dA / (dB + 1e-30));
+  *z0p = z0;
+  if (z0 == 0.0f) return;
+  for (int i = 0; i < nz; ++i) {
+    if (i == zt) continue;
+    float a, b;
+    z_induced(z0, angles[i], rot[i], &a, &b);
+    sx[i] = __fadd_rn(sx[i], __fmul_rn(a, -1.0f));
+    sy[i] = __fadd_rn(sy[i], __fmul_rn(b, -1.0f));
+  }
+}
+
+int fit_z0(Context* c, int nz, int zt, const float* d_angles, float* d_sx, float* d_sy,
+           const float* d_rot, float* d_z0, cudaStream_t st) {
+  k_fit_z0<<<1, 32, 0, st>>>(nz, zt, d_angles, d_sx, d_sy, d_rot, d_z0);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// max over err[i] for i in list (the DoIt return value), initial -1e20.
+__global__ void k_max_err(const float* __restrict__ err, const int* __restrict__ order, int n,
+                          float* out) {
+  if (threadIdx.x != 0) return;
+  float m = -1e20f;
+  for (int i = 0; i < n; ++i) {
+    float e = err[order[i]];
+    if (e > m) m = e;
+  }
+  *out = m;
+}
+
+int max_err(Context* c, const float* d_err, const int* d_order, int n, float* d_out,
+            cudaStream_t st) {
+  k_max_err<<<1, 32, 0, st>>>(d_err, d_order, n, d_out);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stretch about the tilt axis (CalcCC.cu:8-46, 149-171).  One map per z slice of
+// the grid; matrices m[3*j..].  Rows of `stride` floats, `gw` columns computed.
+__device__ __forceinline__ float stretch_random(float X, float Y, int width, int height,
+                                                int grid_x, const float* in) {
+  int x = (int)fabsf(X), y = (int)fabsf(Y);
+  if (x >= width) x = width - 1 - (x % (width - 1));
+  if (y >= height) y = height - 1 - (y % (height - 1));
+  const int win = 31, size = win * win;
+  unsigned int next = (unsigned int)(y * width + x);
+  for (int i = 0; i < size; ++i) {
+    next = (next * 7u) % (unsigned int)size;
+    int ix = (int)(next % (unsigned int)size) - win / 2 + x;
+    if (ix < 0 || ix >= width) continue;
+    int iy = (int)(next / (unsigned int)win) - win / 2 + y;
+    if (iy < 0 || iy >= height) continue;
+    return in[iy * width + ix];
+  }
+  return in[height / 2 * width + grid_x / 2];
+}
+
+__device__ __forceinline__ float stretch_pixel(const float* in, int x, int y, int gw, int h,
+                                               int stride, float m0, float m1, float m2,
+                                               bool randfill) {
+  float X = __fadd_rn(__fsub_rn((float)x, __fmul_rn(0.5f, (float)gw)), 0.5f);
+  float Y = (float)((double)y - 0.5 * (double)h + 0.5);
+  float buf = __fadd_rn(__fmul_rn(X, m0), __fmul_rn(Y, m1));
+  Y = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(X, m1), __fmul_rn(Y, m2)), __fmul_rn(0.5f, (float)h)),
+                0.5f);
+  X = __fsub_rn(__fadd_rn(buf, __fmul_rn(0.5f, (float)gw)), 0.5f);
+  if (X >= 0.0f && X < (float)(gw - 1) && Y >= 0.0f && Y < (float)(h - 1)) {
+    int ix = (int)X, iy = (int)Y;
+    int i = iy * stride + ix;
+    float fx = __fsub_rn(X, (float)ix), fy = __fsub_rn(Y, (float)iy);
+    float f2 = __fsub_rn(1.0f, fx), f3 = __fsub_rn(1.0f, fy);
+    float v = __fmul_rn(__fmul_rn(in[i], f2), f3);
+    v = __fadd_rn(v, __fmul_rn(__fmul_rn(in[i + 1], fx), f3));
+    v = __fadd_rn(v, __fmul_rn(__fmul_rn(in[i + stride], f2), fy));
+    v = __fadd_rn(v, __fmul_rn(__fmul_rn(in[i + stride + 1], fx), fy));
+    return v;
+  }
+  if (randfill) return stretch_random(X, Y, stride, h, gw, in);
+  return kSentinel;
+}
+
+__global__ void k_stretch(const float* __restrict__ src, size_t src_img_stride,
+                          const int* __restrict__ src_idx, int gw, int h, int stride,
+                          const float* __restrict__ mats, int randfill, float* __restrict__ dst,
+                          size_t dst_img_stride) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int j = blockIdx.z;
+  if (x >= gw || y >= h) return;
+  const float* in = src + (size_t)src_idx[j] * src_img_stride;
+  const float* m = mats + 3 * j;
+  dst[(size_t)j * dst_img_stride + (size_t)y * stride + x] =
+      stretch_pixel(in, x, y, gw, h, stride, m[0], m[1], m[2], randfill != 0);
+}
+
+int stretch_many(Context* c, const float* src, size_t src_img_stride, const int* d_src_idx,
+                 int gw, int h, int stride, const float* d_mats, int n, int randfill, float* dst,
+                 size_t dst_img_stride, cudaStream_t st) {
+  dim3 blk(64, 4), grd((gw + 63) / 64, (h + 3) / 4, n);
+  k_stretch<<<grd, blk, 0, st>>>(src, src_img_stride, d_src_idx, gw, h, stride, d_mats, randfill,
+                                 dst, dst_img_stride);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// CalcCC::Stretch matrix (CalcCC.cu:318-332); the stretch factor arrives as float.
+void stretch_matrix(float dstretch, float tilt_axis, float* m) {
+  double d2t = 2 * kD2R * (double)tilt_axis;
+  double s2 = std::sin(d2t), c2 = std::cos(d2t);
+  double P = 0.5 * ((double)dstretch + 1), M = 0.5 * ((double)dstretch - 1);
+  float a0 = (float)(P + M * c2), a1 = (float)(1 * M * s2), a2 = (float)(P - M * c2);
+  float det = a0 * a2 - a1 * a1;
+  m[0] = a2 / det;
+  m[1] = -a1 / det;
+  m[2] = a0 / det;
+}
+
+}  // namespace mf

@@ -1,0 +1,53 @@
+// Launch wrappers of mf_xcorr.cu, mf_correct.cu (pre-processing), mf_axis.cu
+// and mf_offset.cu.
+#pragma once
+#include "mf_internal.hpp"
+
+namespace mf {
+
+int norm_mask_pad(Context* c, const float* src, int src_stride, size_t src_img_stride, int w,
+                  int h, int pad, size_t dst_img_stride, int nimg, int with_std, float cx,
+                  float cy, float msx, float msy, float power, float* dst, double2* d_part,
+                  float2* d_stats, cudaStream_t st);
+constexpr int kMomentParts = 64;
+
+int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,
+                 cufftComplex* img, size_t img_stride, int npairs, int cmp, int ny, float bfactor,
+                 float scale, cudaStream_t st);
+int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
+                   int ip, int nx, int ny, const float* d_angles, float* d_sx, float* d_sy,
+                   const float* d_rot, const float* d_z0, float* d_err, float* d_meas,
+                   cudaStream_t st);
+int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
+                 float* d_out, cudaStream_t st);
+int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w, int h, int nmaps,
+             float2* d_part, float2* d_shifts, cudaStream_t st);
+constexpr int kPeakParts = 64;
+int fit_z0(Context* c, int nz, int zt, const float* d_angles, float* d_sx, float* d_sy,
+           const float* d_rot, float* d_z0, cudaStream_t st);
+int max_err(Context* c, const float* d_err, const int* d_order, int n, float* d_out,
+            cudaStream_t st);
+int stretch_many(Context* c, const float* src, size_t src_img_stride, const int* d_src_idx,
+                 int gw, int h, int stride, const float* d_mats, int n, int randfill, float* dst,
+                 size_t dst_img_stride, cudaStream_t st);
+void stretch_matrix(float dstretch, float tilt_axis, float* m);
+
+int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
+                      const float* file_angles, cudaStream_t st);
+
+// Common-line tilt-axis search over all tilts (Rotate.cu).  Scores (num floats)
+// are returned to the host; the caller applies the arg-max rule.
+struct AxisPlanCache;
+int tilt_axis_scores(Context* c, const float* stack, int nx, int ny, int nz, const float* angles,
+                     const float* sx, const float* sy, int zt, const float* rot_cand, int num,
+                     int line_len, std::vector<float>* scores, cudaStream_t st);
+
+// Tilt-angle offset search (FindOffset.cu): sums[6] per (offset, pair).
+struct OffsetPair {
+  int ref, img;
+  float m0, m1, m2;
+};
+int offset_moments(Context* c, const float* corr, int w, int h, const OffsetPair* d_pairs,
+                   int npairs, double* d_out, cudaStream_t st);
+
+}  // namespace mf

@@ -1,0 +1,125 @@
+"""Run the reference program on seeded synthetic series and keep its outputs.
+
+Test-fixture generator.  It needs the reference binary built by
+oracle/ref/build_ref.sh (oracle/_ref/Markerfree) and one GPU.  For each case it
+writes the series as an MRC (mode 2) + .rawtlt, runs the reference with the
+case's flags, and stores in OUTDIR/<case>/:
+    ref.txt        the reference's parameter file
+    ref.log        its stdout (per-pass measured shifts, Z centre, tilt axes)
+    aligned.npz    per-slice sum / sum of squares of the aligned stack and a
+                   64x64 crop of the middle slice
+    case.json      the generator arguments and flags
+
+The tilt-angle offset search of the reference (FindOffset.cu:85-238) reduces with
+a __syncthreads() inside a divergent branch (FindOffset.cu:57-65), which CUDA
+leaves undefined and which may hang a GPU, so every case passes a non-zero offset
+(-g O,... with O = 1e-4 degrees) and the search is never run.
+
+usage: python tests/golden/make_reference_golden.py OUTDIR [case ...]
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from markerfree_b200 import synth  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "Markerfree")
+
+CASES = {
+    # name: (generator kwargs, thickness, nproj, timeout s)
+    "c1s256": (dict(nx=256, ny=256, vol_z=64, n_blobs=80, seed=1101, snr=0.5,
+                    shift_sd=3.0), 60, 10, 600),
+    "c1s256b": (dict(nx=256, ny=192, vol_z=48, n_blobs=60, seed=1102, snr=0.2,
+                     tilt_step=2.0, tilt_min=-50, tilt_max=50, axis=93.0, shift_sd=4.0),
+                40, 6, 600),
+    "cfg1": (dict(nx=512, ny=512, vol_z=128, n_blobs=200, seed=1001, snr=0.1,
+                  shift_sd=4.0), 100, 10, 1200),
+}
+
+
+def write_mrc(path, stack, mode=2):
+    nz, ny, nx = stack.shape
+    hdr = np.zeros(256, np.int32)
+    hdr[0:4] = [nx, ny, nz, mode]
+    hdr[7:10] = [nx, ny, nz]
+    f = hdr.view(np.float32)
+    f[10:13] = [nx, ny, nz]
+    f[13:16] = [90, 90, 90]
+    hdr[16:19] = [1, 2, 3]
+    data = stack.astype(np.int16 if mode == 1 else np.float32)
+    f[19], f[20], f[21] = float(data.min()), float(data.max()), float(data.mean())
+    raw = bytearray(hdr.tobytes())
+    raw[208:212] = b"MAP "
+    raw[212:216] = bytes([0x44, 0x44, 0, 0])
+    with open(path, "wb") as fh:
+        fh.write(bytes(raw))
+        fh.write(data.tobytes())
+
+
+def read_mrc_float(path):
+    with open(path, "rb") as fh:
+        hdr = np.frombuffer(fh.read(1024), np.int32)
+        nx, ny, nz, mode = (int(v) for v in hdr[:4])
+        nxt = int(hdr[23])
+        fh.seek(1024 + nxt)
+        data = np.frombuffer(fh.read(), np.float32, count=nx * ny * nz)
+    return data.reshape(nz, ny, nx)
+
+
+def run_case(outdir, name):
+    kw, thick, nproj, tmo = CASES[name]
+    s = synth.make_series(thickness=thick, nproj=nproj, **kw)
+    d = os.path.join(outdir, name)
+    os.makedirs(d, exist_ok=True)
+    mrc = os.path.join(d, "in.mrc")
+    tlt = os.path.join(d, "in.rawtlt")
+    write_mrc(mrc, s.stack)
+    with open(tlt, "w") as fh:
+        for a in s.angles:
+            fh.write(f"{a:.2f}\n")
+    out = os.path.join(d, "out.mrc")
+    cmd = [REF_BIN, "-i", mrc, "-o", out, "-a", tlt, "-g", f"0.0001,0,0,0,{thick},1,0",
+           "-p", str(nproj), "-s", "0"]
+    t0 = time.time()
+    with open(os.path.join(d, "ref.log"), "w") as log:
+        rc = subprocess.call(cmd, stdout=log, stderr=subprocess.STDOUT, timeout=tmo)
+    wall = time.time() - t0
+    if rc == 0 and os.path.exists(out):
+        al = read_mrc_float(out)
+        mid = al.shape[0] // 2
+        cy, cx = al.shape[1] // 2, al.shape[2] // 2
+        np.savez_compressed(os.path.join(d, "aligned.npz"),
+                            slice_sum=al.astype(np.float64).sum((1, 2)),
+                            slice_sq=(al.astype(np.float64) ** 2).sum((1, 2)),
+                            crop=al[mid, cy - 32:cy + 32, cx - 32:cx + 32].copy())
+        os.rename(os.path.join(d, "out.txt"), os.path.join(d, "ref.txt"))
+        os.remove(out)
+    os.remove(mrc)
+    with open(os.path.join(d, "case.json"), "w") as fh:
+        json.dump({"generator": kw, "thickness": thick, "nproj": nproj, "cmd": cmd[1:],
+                   "rc": rc, "wall_s": wall}, fh, indent=1)
+    print(name, "rc", rc, "wall", round(wall, 2), flush=True)
+    return rc
+
+
+def main():
+    outdir = sys.argv[1]
+    names = sys.argv[2:] or list(CASES)
+    rc = 0
+    for n in names:
+        rc |= run_case(outdir, n)
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,246 @@
+"""CUDA kernels against the CPU oracle on identical inputs (GPU).
+
+Index work (resampling, binning, nearest-neighbour bins, ray cells, sentinel
+masks, peak positions) must agree exactly; FP32 values computed through cuFFT or
+in a different summation order agree to a stated relative L2 tolerance.
+"""
+import numpy as np
+import pytest
+
+from markerfree_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_FFT = 2e-5      # values that went through cuFFT (FP32) vs the oracle's FP64 FFT
+REL_L2_SUM = 1e-5      # FP32 sums in another order
+SHIFT_TOL = 0.01       # px, sub-pixel peak positions
+
+
+def rel_l2(a, b, mask=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def to_dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+
+
+def small_series(nx=160, ny=128, nz=15, step=4.0, seed=5, axis=86.0):
+    s = synth.make_series(nx=nx, ny=ny, vol_z=40, n_blobs=60, tilt_min=-step * (nz // 2),
+                          tilt_max=step * (nz // 2), tilt_step=step, axis=axis, shift_sd=3.0,
+                          snr=1.0, seed=seed, thickness=30)
+    return s
+
+
+@pytest.fixture(scope="module")
+def series():
+    return small_series()
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("binning,only_shift,random_fill", [
+    (1, False, True), (1, True, True), (2, False, True), (2, False, False), (4, False, False),
+    (3, False, True)])
+def test_correct_proj_exact(ctx, mflib, series, binning, only_shift, random_fill):
+    import torch
+    img = series.stack[3]
+    ny, nx = img.shape
+    xb, yb = O.binned_size(nx, ny, binning)
+    for sx, sy, ax in [(2.3, -7.6, 86.0), (-30.5, 11.5, 93.7), (0.0, 0.0, 0.0), (61.2, -80.9, 45.0)]:
+        want = O.correct_proj(img, sx, sy, ax, only_shift=only_shift, binning=binning,
+                              random_fill=random_fill, rweight=False)
+        d_in = to_dev(img)
+        d_out = torch.empty((yb, xb), dtype=torch.float32, device="cuda")
+        mflib.dev_correct_proj(ctx, d_in, nx, ny, sx, sy, ax, only_shift, binning, random_fill,
+                               False, d_out)
+        ctx.sync()
+        got = d_out.cpu().numpy()
+        assert np.array_equal(got, want), (sx, sy, ax, np.abs(got - want).max())
+
+
+def test_correct_proj_rweight(ctx, mflib, series):
+    import torch
+    img = series.stack[5]
+    ny, nx = img.shape
+    want = O.correct_proj(img, 1.5, -2.5, 85.0, binning=1, rweight=True)
+    d_out = torch.empty(want.shape, dtype=torch.float32, device="cuda")
+    mflib.dev_correct_proj(ctx, to_dev(img), nx, ny, 1.5, -2.5, 85.0, False, 1, True, True, d_out)
+    ctx.sync()
+    assert rel_l2(d_out.cpu().numpy(), want) < REL_L2_FFT
+
+
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def corr_stack(series):
+    nz = series.stack.shape[0]
+    rng = np.random.default_rng(11)
+    out = []
+    for z in range(nz):
+        out.append(O.correct_proj(series.stack[z], float(rng.normal(0, 2)), float(rng.normal(0, 2)),
+                                  86.0, binning=1, rweight=True))
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("iproj,thick", [(9, 30), (13, 30), (4, 12), (1, 40), (7, 2)])
+@pytest.mark.parametrize("method", [0, 1])
+def test_reproject_matches_oracle(ctx, mflib, series, corr_stack, iproj, thick, method):
+    import torch
+    nz, yb, xb = corr_stack.shape
+    ang = series.angles
+    skip = np.ones(nz, np.uint8)
+    zt = O.frame_idx_from_tilt(ang)
+    lo, hi = sorted((zt, iproj))
+    skip[lo:hi + 1] = 0
+    skip[iproj] = 1
+    i0, i1 = O.find_proj_range(ang, skip, iproj, 10)
+    assert i0 >= 0
+    want = O.reproject(corr_stack, ang, iproj, i0, i1, thick)
+    d_corr = to_dev(corr_stack)
+    d_out = torch.empty((yb, xb), dtype=torch.float32, device="cuda")
+    mflib.dev_reproject(ctx, d_corr, xb, yb, nz, ang, iproj, i0, i1, thick, method, d_out)
+    got = d_out.cpu().numpy()
+    valid = want > -1e10
+    assert np.array_equal(got > -1e10, valid)
+    assert valid.any()
+    assert rel_l2(got, want, valid) < REL_L2_SUM
+
+
+def test_reproject_sentinel_rows_fall_back_to_exact(ctx, mflib, series, corr_stack):
+    import torch
+    nz, yb, xb = corr_stack.shape
+    ang = series.angles
+    c = corr_stack.copy()
+    c[8, 70, 40:60] = -1e30   # invalid pixels in a neighbour row
+    c[6, 3, :] = -1e30        # a whole invalid row
+    skip = np.ones(nz, np.uint8)
+    skip[6:9] = 0
+    i0, i1 = O.find_proj_range(ang, skip, 9, 10)
+    want = O.reproject(c, ang, 9, i0, i1, 30)
+    d_out = torch.empty((yb, xb), dtype=torch.float32, device="cuda")
+    mflib.dev_reproject(ctx, to_dev(c), xb, yb, nz, ang, 9, i0, i1, 30, 1, d_out)
+    got = d_out.cpu().numpy()
+    valid = want > -1e10
+    assert np.array_equal(got > -1e10, valid)
+    assert rel_l2(got, want, valid) < REL_L2_SUM
+
+
+# ---------------------------------------------------------------------------
+def test_measure_shift_matches_oracle(ctx, mflib, series, corr_stack):
+    nz, yb, xb = corr_stack.shape
+    ang = series.angles
+    skip = np.ones(nz, np.uint8)
+    skip[5:9] = 0
+    i0, i1 = O.find_proj_range(ang, skip, 9, 10)
+    rep = O.reproject(corr_stack, ang, 9, i0, i1, 30)
+    for shift in [(0, 0), (3, -2), (-5, 4)]:
+        img = np.roll(corr_stack[9], shift, axis=(0, 1))
+        wx, wy, wp = O.measure_shift(rep, img)
+        gx, gy, gp = mflib.dev_measure_shift(ctx, to_dev(rep), to_dev(img), xb, yb)
+        assert abs(gx - wx) < SHIFT_TOL and abs(gy - wy) < SHIFT_TOL, (gx, gy, wx, wy)
+        assert abs(gp - wp) <= 1e-4 * abs(wp) + 1e-3
+
+
+# ---------------------------------------------------------------------------
+def test_preprocess_matches_oracle(ctx, mflib, series):
+    raw = series.stack.copy()
+    raw -= raw.min() + 3.0  # negative values: the positivity shift runs
+    want = O.preprocess(raw, series.angles)
+    s = mflib.Series(ctx, raw, series.angles)
+    got = s.stack()
+    assert rel_l2(got, want) < 1e-6
+    # descending angle file: stack reversed
+    want_r = O.preprocess(raw[::-1].copy(), series.angles[::-1].copy())
+    s2 = mflib.Series(ctx, raw[::-1].copy(), series.angles[::-1].copy())
+    assert rel_l2(s2.stack(), want_r) < 1e-6
+    assert np.allclose(s2.angles, np.sort(series.angles))
+
+
+def test_projalign_pass_matches_oracle(ctx, mflib, series):
+    nz = series.stack.shape[0]
+    st = O.preprocess(series.stack, series.angles)
+    s = mflib.Series(ctx, series.stack, series.angles)
+    p = mflib.Param(nz)
+    p.rotate[:] = 86.0
+    s.set_param(p)
+    po = O.Param(nz)
+    po.rotate[:] = 86.0
+    pa = O.ProjAlign(st, series.angles, po, 0.0, 30, 10)
+    s.projalign_setup(0.0, 30, 10)
+    for k in range(2):
+        e_o = pa.doit()
+        e_g = s.projalign_doit()
+        g = s.get_param()
+        assert abs(e_g - e_o) < 0.02, (k, e_g, e_o)
+        assert abs(s.z0 - pa.z0) < 0.02
+        assert np.abs(g.shift_x - po.shift_x).max() < 0.02
+        assert np.abs(g.shift_y - po.shift_y).max() < 0.02
+
+
+def test_transform_and_axis_match_oracle(ctx, mflib):
+    s0 = small_series(nx=256, ny=256, nz=21, step=3.0, seed=8)
+    nz = s0.stack.shape[0]
+    st = O.preprocess(s0.stack, s0.angles)
+    po = O.Param(nz)
+    t = O.Transform(st, s0.angles, po)
+    s = mflib.Series(ctx, s0.stack, s0.angles)
+    for i in (1, 2):
+        e_o = t.doit()
+        e_g = s.transform_doit()
+        g = s.get_param()
+        assert abs(e_g - e_o) < 0.02
+        assert np.abs(g.shift_x - po.shift_x).max() < 0.02
+        assert np.abs(g.shift_y - po.shift_y).max() < 0.02
+        ax_o, sc_o = O.tilt_axis_scores(st, s0.angles, po, 180.0 / i)
+        ax_g = s.tilt_axis(180.0 / i)
+        # equal unless the two best candidates are within float noise
+        top = np.sort(sc_o)[-2:]
+        if top[1] - top[0] > 1e-5:
+            assert ax_g == pytest.approx(ax_o, abs=1e-4)
+        g = s.get_param()
+        po.rotate[:] = g.rotate  # keep both on the same trajectory
+    off_o = O.find_offset(st, s0.angles, po)
+    off_g = s.find_offset()
+    assert off_g == off_o
+
+
+def test_correct_stack_matches_oracle(ctx, mflib, series):
+    nz = series.stack.shape[0]
+    st = O.preprocess(series.stack, series.angles)
+    rng = np.random.default_rng(2)
+    p = mflib.Param(nz)
+    p.shift_x[:] = rng.normal(0, 5, nz)
+    p.shift_y[:] = rng.normal(0, 5, nz)
+    p.rotate[:] = 87.3
+    po = O.Param(nz)
+    po.shift_x[:] = p.shift_x
+    po.shift_y[:] = p.shift_y
+    po.rotate[:] = p.rotate
+    s = mflib.Series(ctx, series.stack, series.angles)
+    s.set_param(p)
+    for b in (1, 2):
+        assert np.array_equal(s.correct_stack(b), O.correct_stack(st, po, b))
+
+
+# ---------------------------------------------------------------------------
+def test_errors_are_reported_not_faulted(ctx, mflib, series):
+    with pytest.raises(mflib.MfError):
+        mflib.Series(ctx, series.stack[:1], series.angles[:1])  # one tilt
+    s = mflib.Series(ctx, series.stack, series.angles)
+    with pytest.raises(mflib.MfError):
+        s.projalign_doit()  # before setup
+    with pytest.raises(mflib.MfError):
+        s.projalign_setup(0.0, 30, 0)  # nproj 0
+    with pytest.raises(mflib.MfError):
+        s.projalign_setup(0.0, 1, 10)  # slab too thin
+    # a 30-degree gap leaves a held-out tilt with no neighbour in range
+    ang = np.concatenate([np.linspace(-20, 0, 6), np.linspace(30, 50, 5)]).astype(np.float32)
+    stk = synth.make_series(nx=64, ny=64, vol_z=16, n_blobs=20, n_tilts=11, seed=3).stack
+    s3 = mflib.Series(ctx, stk, ang)
+    with pytest.raises(mflib.MfError) as ei:
+        s3.projalign_setup(0.0, 16, 10)
+    assert ei.value.code == -8
