@@ -100,6 +100,7 @@ MF_API int mf_series_create(mf_context* ctx, const float* raw_stack, int nx, int
 /* Same, from a device buffer already holding the raw stack (file order). */
 MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw_stack, int nx, int ny,
                                    int nz, const float* file_angles, mf_series** out);
+/* Destroy every series of a context before the context itself. */
 MF_API void mf_series_destroy(mf_series* s);
 MF_API int mf_series_set_precision(mf_series* s, mf_precision p);
 /* Copies the pre-processed stack (nz*ny*nx floats) to host memory. */
@@ -145,6 +146,25 @@ MF_API void mf_binned_size(int nx, int ny, int bin, int* xb, int* yb);
 MF_API int mf_align(mf_context* ctx, const float* raw_stack, int nx, int ny, int nz,
                     const float* file_angles, const mf_options* opt, mf_align_param* param,
                     float* aligned_out, int* passes);
+
+/* Same as mf_align with the raw stack and the aligned output in device memory
+ * (caller-owned, on the context's GPU); parameters are returned to the host. */
+MF_API int mf_align_device(mf_context* ctx, const float* d_raw_stack, int nx, int ny, int nz,
+                           const float* file_angles, const mf_options* opt, mf_align_param* param,
+                           float* d_aligned_out, int* passes);
+
+/* Stage timing: when enabled, every projection-matching pass records CUDA events
+ * around each held-out tilt's re-projection and cross-correlation work (also
+ * inside the captured graph).  mf_context_stage_times returns, accumulated since
+ * the last call and then reset: [0] re-projection ms, [1] re-projection
+ * launches (one per held-out tilt), [2] cross-correlation + re-correction ms,
+ * [3] passes, [4] re-projection algorithmic bytes (neighbour rows read, output
+ * written, banded operator read), [5] re-projection multiply-adds. */
+MF_API int mf_context_set_profiling(mf_context* ctx, int on);
+MF_API int mf_context_stage_times(mf_context* ctx, double* out6);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own
+ * work or timing events after the library's. */
+MF_API void* mf_context_stream(mf_context* ctx);
 
 /* ---- single kernels on caller-owned device memory (same stream semantics:
  * the call is ordered on the context stream and returns after queuing). ------ */

@@ -86,6 +86,13 @@ SIGNATURES = [
     ("mf_align", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 _f32p, ctypes.POINTER(OptionsC), ctypes.POINTER(AlignParamC),
                                 ctypes.c_void_p, _c_int_p]),
+    ("mf_align_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, _f32p, ctypes.POINTER(OptionsC),
+                                       ctypes.POINTER(AlignParamC), ctypes.c_void_p, _c_int_p]),
+    ("mf_context_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("mf_context_stage_times", ctypes.c_int, [ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_double)]),
+    ("mf_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -171,10 +178,27 @@ class Context:
     def kernel_launches(self) -> int:
         return int(lib().mf_context_kernel_launches(self.h))
 
+    def set_profiling(self, on: bool):
+        _check(lib().mf_context_set_profiling(self.h, int(bool(on))))
+
+    def stage_times(self) -> dict:
+        """Stage timing accumulated since the previous call (see set_profiling)."""
+        out = (ctypes.c_double * 6)()
+        _check(lib().mf_context_stage_times(self.h, out))
+        keys = ("reproj_ms", "reproj_launches", "xcorr_ms", "passes", "reproj_bytes",
+                "reproj_fma")
+        return dict(zip(keys, out))
+
+    def stream_ptr(self) -> int:
+        return int(lib().mf_context_stream(self.h) or 0)
+
     def close(self):
-        if getattr(self, "h", None):
-            lib().mf_context_destroy(self.h)
-            self.h = None
+        # series of this context are released first (the C API requires it)
+        for s in list(getattr(self, "_series", ())):
+            s.close()
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.mf_context_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -184,6 +208,7 @@ class Series:
     """A pre-processed tilt series kept in HBM (replaces buf.mrc)."""
 
     def __init__(self, ctx: Context, raw_stack, file_angles):
+        import weakref
         raw = _f32(raw_stack)
         self.nz, self.ny, self.nx = raw.shape
         self.ctx = ctx
@@ -192,11 +217,14 @@ class Series:
         _check(lib().mf_series_create(ctx.h, raw, self.nx, self.ny, self.nz, self.file_angles,
                                       ctypes.byref(h)))
         self.h = h
+        if not hasattr(ctx, "_series"):
+            ctx._series = weakref.WeakSet()
+        ctx._series.add(self)
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().mf_series_destroy(self.h)
-            self.h = None
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.mf_series_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -295,6 +323,35 @@ def align(ctx: Context, raw_stack, file_angles, offset=0.0, pitch_angle=0.0, zsh
                           ctypes.byref(c), ptr, ctypes.byref(n)))
     p.angle_offset = c.angle_offset
     return p, out, n.value
+
+
+def align_device(ctx: Context, d_raw, nx, ny, nz, file_angles, d_out, offset=0.0,
+                 pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10):
+    """mf_align_device: raw stack and aligned output in device memory (torch tensors or
+    addresses).  Returns (Param, passes)."""
+    p = Param(nz)
+    c = p.c()
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    n = ctypes.c_int()
+    _check(lib().mf_align_device(ctx.h, _ptr(d_raw), nx, ny, nz, _f32(file_angles)[:nz],
+                                 ctypes.byref(o), ctypes.byref(c), _ptr(d_out), ctypes.byref(n)))
+    p.angle_offset = c.angle_offset
+    return p, n.value
+
+
+def align_host_ptr(ctx: Context, raw_ptr: int, nx, ny, nz, file_angles, out_ptr: int,
+                   offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10):
+    """mf_align on caller-owned host buffers given by address (e.g. pinned memory)."""
+    p = Param(nz)
+    c = p.c()
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    n = ctypes.c_int()
+    f = lib().mf_align
+    raw_arr = np.ctypeslib.as_array(ctypes.cast(raw_ptr, _c_float_p), (nz * ny * nx,))
+    _check(f(ctx.h, raw_arr, nx, ny, nz, _f32(file_angles)[:nz], ctypes.byref(o),
+             ctypes.byref(c), ctypes.c_void_p(out_ptr), ctypes.byref(n)))
+    p.angle_offset = c.angle_offset
+    return p, n.value
 
 
 def find_proj_range(angles, skip, iproj, nproj):

@@ -49,7 +49,7 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
                         const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
                         const float* __restrict__ sxs, const float* __restrict__ sys,
                         const int* __restrict__ region, float* __restrict__ lines) {
-  int y = blockIdx.y * blockDim.y + threadIdx.x;
+  int y = blockIdx.y * blockDim.x + threadIdx.x;
   int b = blockIdx.x;
   int z = blockIdx.z;
   if (y >= L) return;

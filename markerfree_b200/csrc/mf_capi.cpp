@@ -70,6 +70,23 @@ MF_API int mf_context_sync(mf_context* ctx) {
 
 MF_API int64_t mf_context_kernel_launches(mf_context* ctx) { return ctx ? ctx->c.launches : 0; }
 
+MF_API int mf_context_set_profiling(mf_context* ctx, int on) {
+  if (!ctx) return set_error(MF_ERR_ARG, "null context");
+  ctx->c.profiling = on != 0;
+  return MF_OK;
+}
+
+MF_API int mf_context_stage_times(mf_context* ctx, double* out6) {
+  if (!ctx || !out6) return set_error(MF_ERR_ARG, "null argument");
+  for (int i = 0; i < 6; ++i) {
+    out6[i] = ctx->c.stage[i];
+    ctx->c.stage[i] = 0.0;
+  }
+  return MF_OK;
+}
+
+MF_API void* mf_context_stream(mf_context* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
 // ---------------------------------------------------------------------------
 static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_device, int nx,
                                 int ny, int nz, const float* file_angles, mf_series** out) {
@@ -122,10 +139,9 @@ MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw, int nx, 
 
 MF_API void mf_series_destroy(mf_series* s) {
   if (!s) return;
-  if (s->ctx) {
-    cudaSetDevice(s->ctx->c.gpu);
-    cudaStreamSynchronize(s->ctx->c.stream);
-  }
+  // only the device id is used: the context may already be gone
+  cudaSetDevice(s->gpu);
+  cudaDeviceSynchronize();
   delete s;
 }
 
@@ -265,26 +281,49 @@ MF_API int mf_correct_stack(mf_series* s, int out_bin, float* host_out) {
   MF_GUARD_END
 }
 
-MF_API int mf_align(mf_context* ctx, const float* raw, int nx, int ny, int nz,
-                    const float* file_angles, const mf_options* opt, mf_align_param* param,
-                    float* aligned_out, int* passes) {
-  MF_GUARD_BEGIN
+static int align_common(mf_context* ctx, const float* raw, bool on_device, int nx, int ny, int nz,
+                        const float* file_angles, const mf_options* opt, mf_align_param* param,
+                        float* out, int* passes) {
   if (!opt || !param) return set_error(MF_ERR_ARG, "null options or parameters");
   if (opt->nproj <= 0) return set_error(MF_ERR_ARG, "nProj must be > 0.");
   if (opt->out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
   mf_series* s = nullptr;
-  MF_TRY(mf_series_create(ctx, raw, nx, ny, nz, file_angles, &s));
+  MF_TRY(series_create_common(ctx, raw, on_device, nx, ny, nz, file_angles, &s));
   int rc = MF_OK;
   int np = 0;
   if (opt->align_z != 0) {
     rc = coarse_align(s, opt->pitch_angle, opt->offset);
     if (rc == MF_OK) rc = proj_align(s, opt->zshift, opt->align_z, opt->nproj, &np);
   }
-  if (rc == MF_OK && aligned_out) rc = mf_correct_stack(s, opt->out_bin, aligned_out);
+  if (rc == MF_OK && out) {
+    if (on_device) {
+      rc = correct_stack_device(s, opt->out_bin, out);
+      if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
+        rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
+    } else {
+      rc = mf_correct_stack(s, opt->out_bin, out);
+    }
+  }
   if (rc == MF_OK) rc = mf_series_get_param(s, param);
   if (passes) *passes = np;
   mf_series_destroy(s);
   return rc;
+}
+
+MF_API int mf_align(mf_context* ctx, const float* raw, int nx, int ny, int nz,
+                    const float* file_angles, const mf_options* opt, mf_align_param* param,
+                    float* aligned_out, int* passes) {
+  MF_GUARD_BEGIN
+  return align_common(ctx, raw, false, nx, ny, nz, file_angles, opt, param, aligned_out, passes);
+  MF_GUARD_END
+}
+
+MF_API int mf_align_device(mf_context* ctx, const float* d_raw, int nx, int ny, int nz,
+                           const float* file_angles, const mf_options* opt, mf_align_param* param,
+                           float* d_aligned_out, int* passes) {
+  MF_GUARD_BEGIN
+  return align_common(ctx, d_raw, true, nx, ny, nz, file_angles, opt, param, d_aligned_out,
+                      passes);
   MF_GUARD_END
 }
 

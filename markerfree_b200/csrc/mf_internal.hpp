@@ -76,6 +76,8 @@ struct Context {
   cudaStream_t stream = nullptr;
   int64_t launches = 0;  // library kernel launches queued (for reporting)
   int sm_count = 148;
+  bool profiling = false;
+  double stage[6] = {0, 0, 0, 0, 0, 0};  // see mf_context_stage_times
 };
 
 // ---- per-held-out-tilt banded re-projection operator ----------------------

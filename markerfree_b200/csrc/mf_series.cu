@@ -65,6 +65,8 @@ namespace mf {
 ProjAlignState::~ProjAlignState() {
   if (graph) cudaGraphExecDestroy(graph);
   graph = nullptr;
+  for (cudaEvent_t e : events) cudaEventDestroy(e);
+  events.clear();
 }
 
 // ---------------------------------------------------------------------------
@@ -79,6 +81,7 @@ __global__ void k_pad_copy(const float* __restrict__ src, int w, int h, int pad,
 
 int series_init(mf_series* s, mf_context* ctx, int nx, int ny, int nz, const float* file_angles) {
   s->ctx = ctx;
+  s->gpu = ctx->c.gpu;
   s->nx = nx;
   s->ny = ny;
   s->nz = nz;
@@ -450,10 +453,17 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_CHECK_CUDA(cudaMemsetAsync(P.d_err.p, 0, sizeof(float) * nz, st));
   MF_CHECK_CUDA(cudaMemsetAsync(P.d_meas.p, 0, sizeof(float) * 2 * nz, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(P.d_z0.p, &P.z0, sizeof(float), cudaMemcpyHostToDevice, st));
-  if (P.method == 1) {
-    for (int k = 0; k < n; ++k) {
+  P.reproj_bytes = 0;
+  P.reproj_fma = 0;
+  for (int k = 0; k < n; ++k) {
+    // compulsory traffic: the K neighbour images read once, the re-projection written
+    P.reproj_bytes += 4.0 * (double)bpix * (P.geom[k].nk + 1);
+    if (P.method == 1) {
       P.ops.emplace_back(new ReprojOp());
       MF_TRY(build_reproj_op(c, P.geom[k], P.ops.back().get(), st));
+      const ReprojOp& op = *P.ops.back();
+      P.reproj_bytes += (double)op.total_rows * (kOpTileX * 4 + 8);
+      P.reproj_fma += (double)yb * op.total_rows * kOpTileX;
     }
   }
   // FFT plans
@@ -493,11 +503,13 @@ static int pa_enqueue(mf_series* s) {
   // FitRotCenterZ + RemoveOffsetZ(-1)
   MF_TRY(fit_z0(c, nz, P.zt, s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
                 s->d_rot.as<float>(), P.d_z0.as<float>(), st));
+  const bool prof = c->profiling && (int)P.events.size() >= 3 * n;
   for (int k = 0; k < n; ++k) {
     const int ip = P.order[k];
     const ReprojGeom& g = P.geom[k];
     int* rowflags = P.d_rowflags.as<int>() + (size_t)k * P.ytiles;
     float* reproj = P.reproj.as<float>();
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k], st));
     if (P.method == 1) {
       MF_TRY(launch_reproject_apply(c, *P.ops[k], corr, bpix, rowflags, reproj, st));
       MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
@@ -508,6 +520,7 @@ static int pa_enqueue(mf_series* s) {
                                     g.nk, g.fcos, g.fsin, g.ray_len, g.thick, nullptr, reproj,
                                     st));
     }
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k + 1], st));
     // MeaAlignProj: PANorm both, FFT, filter, inverse FFT, peak
     const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
     MF_TRY(norm_mask_pad(c, reproj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad, (float)yb,
@@ -530,6 +543,7 @@ static int pa_enqueue(mf_series* s) {
     MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_one, scratch, (cufftComplex*)scratch));
     MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, yb, st));
     MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_one, (cufftComplex*)scratch, corr + (size_t)ip * bpix));
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k + 2], st));
   }
   MF_TRY(max_err(c, P.d_err.as<float>(), P.d_order.as<int>(), n, P.d_maxerr.as<float>(), st));
   return MF_OK;
@@ -541,7 +555,16 @@ int projalign_doit(mf_series* s, float* max_err_out) {
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   MF_TRY(s->upload_params());
-  if (P.use_graph && !P.graph) {
+  const int n = (int)P.order.size();
+  if (c->profiling && (int)P.events.size() < 3 * n) {
+    while ((int)P.events.size() < 3 * n) {
+      cudaEvent_t e;
+      MF_CHECK_CUDA(cudaEventCreate(&e));
+      P.events.push_back(e);
+    }
+  }
+  // Profiled passes run eagerly: events recorded by graph nodes cannot be timed.
+  if (P.use_graph && !P.graph && !c->profiling) {
     // Capture once; the graph reads parameters from device memory, so every
     // later pass replays it unchanged.
     int64_t l0 = c->launches;
@@ -565,7 +588,7 @@ int projalign_doit(mf_series* s, float* max_err_out) {
       }
     }
   }
-  if (P.graph) {
+  if (P.graph && !c->profiling) {
     MF_CHECK_CUDA(cudaGraphLaunch(P.graph, st));
     c->launches += P.graph_kernels;
   } else {
@@ -576,6 +599,19 @@ int projalign_doit(mf_series* s, float* max_err_out) {
   MF_CHECK_CUDA(cudaMemcpyAsync(&res[1], P.d_z0.p, sizeof(float), cudaMemcpyDeviceToHost, st));
   MF_TRY(s->download_shifts());
   P.z0 = res[1];
+  if (c->profiling && (int)P.events.size() >= 3 * n) {
+    for (int k = 0; k < n; ++k) {
+      float a = 0.0f, b = 0.0f;
+      MF_CHECK_CUDA(cudaEventElapsedTime(&a, P.events[3 * k], P.events[3 * k + 1]));
+      MF_CHECK_CUDA(cudaEventElapsedTime(&b, P.events[3 * k + 1], P.events[3 * k + 2]));
+      c->stage[0] += a;
+      c->stage[2] += b;
+    }
+    c->stage[1] += n;
+    c->stage[3] += 1;
+    c->stage[4] += P.reproj_bytes;
+    c->stage[5] += P.reproj_fma;
+  }
   if (max_err_out) *max_err_out = res[0];
   return MF_OK;
 }

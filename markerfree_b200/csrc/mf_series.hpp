@@ -40,6 +40,8 @@ struct ProjAlignState {
   cufftHandle cc_fwd = 0, cc_inv = 0;
   cudaGraphExec_t graph = nullptr;
   int64_t graph_kernels = 0;  // library kernels per replay
+  double reproj_bytes = 0, reproj_fma = 0;  // per pass, over all held-out tilts
+  std::vector<cudaEvent_t> events;  // 3 per held-out tilt when profiling
   bool use_graph = true;
   int method = 1;  // 1: banded operator with exact fallback; 0: exact gather only
   ~ProjAlignState();
@@ -55,6 +57,7 @@ struct TransformState {
 
 struct mf_series {
   mf_context* ctx = nullptr;
+  int gpu = 0;
   int nx = 0, ny = 0, nz = 0;
   mf::DevBuf stack;  // pre-processed stack, nz x ny x nx
   std::vector<float> file_angles;

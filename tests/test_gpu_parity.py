@@ -86,7 +86,7 @@ def corr_stack(series):
     return np.stack(out)
 
 
-@pytest.mark.parametrize("iproj,thick", [(9, 30), (13, 30), (4, 12), (1, 40), (7, 2)])
+@pytest.mark.parametrize("iproj,thick", [(9, 30), (13, 30), (4, 12), (1, 40), (8, 2)])
 @pytest.mark.parametrize("method", [0, 1])
 def test_reproject_matches_oracle(ctx, mflib, series, corr_stack, iproj, thick, method):
     import torch
