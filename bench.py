@@ -310,8 +310,38 @@ def run_ours(args):
     return 0
 
 
+def run_kernel_case(args):
+    """One stage of the workload on its own, for profilers (ncu -k ...): `reproject`
+    re-projects one held-out tilt (full size, 10 neighbours) with the banded
+    operator; `xcorr` measures one cross-correlation shift."""
+    import torch
+    import markerfree_b200 as mf
+    s = make_workload(args.scale)
+    nz, ny, nx = s.stack.shape
+    ctx = mf.Context(0)
+    ang = s.angles
+    zt = int(np.argmin(np.abs(ang)))
+    ip = zt + 11
+    skip = np.ones(nz, np.uint8)
+    skip[zt - 10:zt + 11] = 0
+    i0, i1 = mf.find_proj_range(ang, skip, ip, 10)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    corr = torch.randn((nz, ny, nx), generator=g, device="cuda", dtype=torch.float32)
+    out = torch.empty((ny, nx), device="cuda", dtype=torch.float32)
+    for _ in range(args.steps):
+        if args.kernel_case == "reproject":
+            mf.dev_reproject(ctx, corr, nx, ny, nz, ang, ip, i0, i1, s.thickness, 1, out)
+        else:
+            mf.dev_measure_shift(ctx, out, corr[ip], nx, ny)
+    ctx.sync()
+    print(json.dumps({"kernel_case": args.kernel_case, "range": [i0, i1], "ip": ip}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr"],
+                    help="run one stage alone (profiling)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
@@ -319,6 +349,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests only)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     args = ap.parse_args()
+    if args.kernel_case:
+        return run_kernel_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -65,14 +65,20 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   int left = (int)__fadd_rn(__fmul_rn((float)region[2 * i], fc), 0.5f);
   int right = (int)__fadd_rn(__fmul_rn((float)region[2 * i + 1], fc), 0.5f);
   // left <= 0 <= right, so one loop visits the reference's two loops in order;
-  // fy*sin and fy*cos are loop invariant with the same rounding as the reference
-  float ys = __fmul_rn(fy, fsr), yc = __fmul_rn(fy, fcr);
-  for (int x = left; x < right; ++x) {
-    float X = __fadd_rn(__fsub_rn(__fmul_rn((float)x, fcr), ys), ox);
-    float Y = __fadd_rn(__fadd_rn(__fmul_rn((float)x, fsr), yc), oy);
-    if (X < 0 || X >= width) continue;
-    if (Y < 0 || Y >= height) continue;
-    float v = __ldg(proj + (size_t)(int)Y * width + (int)X);
+  // fy*sin and fy*cos are loop invariant with the same rounding as the reference.
+  // The float copy of x is stepped by 1.0 (exact below 2^24) instead of converted,
+  // and the in-range coordinates (0 <= X < 2^23) are truncated by a round-toward-
+  // zero add of 2^23, which gives the same integer as (int)X.
+  const float ys = __fmul_rn(fy, fsr), yc = __fmul_rn(fy, fcr);
+  const float fw = (float)width, fh = (float)height;
+  float fx = (float)left;
+  for (int x = left; x < right; ++x, fx = __fadd_rn(fx, 1.0f)) {
+    float X = __fadd_rn(__fsub_rn(__fmul_rn(fx, fcr), ys), ox);
+    float Y = __fadd_rn(__fadd_rn(__fmul_rn(fx, fsr), yc), oy);
+    if (!(X >= 0.0f && X < fw && Y >= 0.0f && Y < fh)) continue;
+    int ix = __float_as_int(__fadd_rz(X, 8388608.0f)) - 0x4B000000;
+    int iy = __float_as_int(__fadd_rz(Y, 8388608.0f)) - 0x4B000000;
+    float v = __ldg(proj + (size_t)iy * width + ix);
     if (v < 0) continue;
     sum = __fadd_rn(sum, v);
     cnt++;
@@ -181,7 +187,8 @@ struct AxisBuffers {
   DevBuf cs, tcos, sx, sy, region, lines, sum, cc, score;
 };
 
-int tilt_axis_scores(Context* c, const float* stack, int nx, int ny, int nz, const float* angles,
+int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, int ny, int nz,
+                     const float* angles,
                      const float* sx, const float* sy, int zt, const float* rot_cand, int num,
                      int L, std::vector<float>* scores, cudaStream_t st) {
   const int cmp = L / 2 + 1;
@@ -214,14 +221,7 @@ int tilt_axis_scores(Context* c, const float* stack, int nx, int ny, int nz, con
   k_line_prep<<<nz * num, 256, 0, st>>>(B.lines.as<float>(), L);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
-  cufftHandle plan;
-  MF_CHECK_CUFFT(cufftPlan1d(&plan, L, CUFFT_R2C, nz * num));
-  cufftSetStream(plan, st);
-  cufftResult fr = cufftExecR2C(plan, B.lines.as<cufftReal>(), B.lines.as<cufftComplex>());
-  if (fr != CUFFT_SUCCESS) {
-    cufftDestroy(plan);
-    return set_error(MF_ERR_CUFFT, "tilt axis R2C failed: %d", (int)fr);
-  }
+  MF_CHECK_CUFFT(cufftExecR2C(plan, B.lines.as<cufftReal>(), B.lines.as<cufftComplex>()));
   const cufftComplex* spec = B.lines.as<cufftComplex>();
   k_axis_sum<<<dim3((cmp + 127) / 128, num), 128, 0, st>>>(spec, nz, num, cmp,
                                                             B.sum.as<cufftComplex>());
@@ -234,7 +234,6 @@ int tilt_axis_scores(Context* c, const float* stack, int nx, int ny, int nz, con
   MF_CHECK_CUDA(cudaMemcpyAsync(scores->data(), B.score.p, sizeof(float) * num,
                                 cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  cufftDestroy(plan);
   return MF_OK;
 }
 

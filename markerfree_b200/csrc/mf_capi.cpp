@@ -24,6 +24,7 @@ using namespace mf;
 static int use_device(mf_context* ctx) {
   if (!ctx) return set_error(MF_ERR_ARG, "null context");
   MF_CHECK_CUDA(cudaSetDevice(ctx->c.gpu));
+  set_alloc_stream(ctx->c.stream);
   return MF_OK;
 }
 
@@ -50,6 +51,12 @@ MF_API int mf_context_create(int gpu, mf_context** out) {
     delete ctx;
     return set_error(MF_ERR_CUDA, "cudaStreamCreate failed");
   }
+  // keep freed device memory in the pool for the next series
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
   *out = ctx;
   return MF_OK;
   MF_GUARD_END
@@ -59,7 +66,10 @@ MF_API void mf_context_destroy(mf_context* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->c.gpu);
   cudaStreamSynchronize(ctx->c.stream);
+  set_sync_free(true);
   delete ctx;
+  set_sync_free(false);
+  set_alloc_stream(nullptr);
 }
 
 MF_API int mf_context_sync(mf_context* ctx) {
@@ -139,9 +149,8 @@ MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw, int nx, 
 
 MF_API void mf_series_destroy(mf_series* s) {
   if (!s) return;
-  // only the device id is used: the context may already be gone
+  // buffers go back to the pool in stream order on the (still alive) context stream
   cudaSetDevice(s->gpu);
-  cudaDeviceSynchronize();
   delete s;
 }
 
@@ -384,12 +393,13 @@ MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb
     MF_TRY(launch_reproject_exact(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0, g.nk,
                                   g.fcos, g.fsin, g.ray_len, g.thick, nullptr, d_out, st));
   } else {
-    ReprojOp op;
-    MF_TRY(build_reproj_op(&ctx->c, g, &op, st));
+    ReprojOpSet set;
+    std::vector<ReprojGeom> gs(1, g);
+    MF_TRY(build_reproj_ops(&ctx->c, gs, &set, st));
     int ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
     MF_TRY(S->c.alloc(sizeof(int) * ytiles));
     MF_CHECK_CUDA(cudaMemsetAsync(S->c.p, 0, sizeof(int) * ytiles, st));
-    MF_TRY(launch_reproject_apply(&ctx->c, op, d_corr, pix, S->c.as<int>(), d_out, st));
+    MF_TRY(launch_reproject_apply(&ctx->c, set.ops[0], d_corr, pix, S->c.as<int>(), d_out, st));
     MF_TRY(launch_reproject_exact(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0, g.nk,
                                   g.fcos, g.fsin, g.ray_len, g.thick, S->c.as<int>(), d_out, st));
   }
@@ -409,17 +419,16 @@ MF_API int mf_dev_measure_shift(mf_context* ctx, const float* d_reproj, const fl
   const size_t ppix = (size_t)pad * yb;
   mf_context::Scratch* S = scratch_of(ctx);
   MF_TRY(S->a.alloc(sizeof(float) * ppix * 2));
-  MF_TRY(S->d.alloc(sizeof(double2) * kMomentParts * 2 + sizeof(float2) * (kPeakParts + 2) + 64));
+  const int mparts = moment_parts(yb) * 2;
+  MF_TRY(S->d.alloc(sizeof(double2) * mparts + sizeof(float2) * (kPeakParts + 2) + 64));
   double2* mpart = S->d.as<double2>();
-  float2* stats = reinterpret_cast<float2*>(mpart + kMomentParts * 2);
+  float2* stats = reinterpret_cast<float2*>(mpart + mparts);
   float2* ppart = stats + 2;
   float* outv = reinterpret_cast<float*>(ppart + kPeakParts);
   float* cc = S->a.as<float>();
   const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
-  MF_TRY(norm_mask_pad(&ctx->c, d_reproj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad,
-                       (float)yb, 4.0f, cc, mpart, stats, st));
-  MF_TRY(norm_mask_pad(&ctx->c, d_proj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad,
-                       (float)yb, 4.0f, cc + ppix, mpart + kMomentParts, stats + 1, st));
+  MF_TRY(norm_mask_pad(&ctx->c, d_reproj, d_proj, xb, 0, xb, yb, pad, ppix, 2, 0, mcx, mcy,
+                       (float)pad, (float)yb, 4.0f, cc, mpart, stats, st));
   cufftHandle f, i;
   MF_TRY(ctx->plan({2, xb, yb, 2}, &f));
   MF_TRY(ctx->plan({3, xb, yb, 1}, &i));

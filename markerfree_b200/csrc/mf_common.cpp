@@ -18,25 +18,40 @@ int set_error(int code, const char* fmt, ...) {
 
 const char* last_error() { return g_last_error; }
 
+static thread_local cudaStream_t g_alloc_stream = nullptr;
+static thread_local bool g_sync_free = false;
+
+void set_alloc_stream(cudaStream_t s) { g_alloc_stream = s; }
+void set_sync_free(bool on) { g_sync_free = on; }
+
 int DevBuf::alloc(size_t n) {
   if (n == 0) n = 16;
   if (p && bytes >= n) return MF_OK;
   release();
-  cudaError_t e = cudaMalloc(&p, n);
+  st = g_alloc_stream;
+  cudaError_t e = st ? cudaMallocAsync(&p, n, st) : cudaMalloc(&p, n);
   if (e != cudaSuccess) {
     p = nullptr;
     bytes = 0;
+    st = nullptr;
     cudaGetLastError();
-    return set_error(MF_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", n, cudaGetErrorString(e));
+    return set_error(MF_ERR_NOMEM, "device allocation of %zu bytes failed: %s", n,
+                     cudaGetErrorString(e));
   }
   bytes = n;
   return MF_OK;
 }
 
 void DevBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    if (st && !g_sync_free)
+      cudaFreeAsync(p, st);
+    else
+      cudaFree(p);
+  }
   p = nullptr;
   bytes = 0;
+  st = nullptr;
 }
 
 FftPlan::~FftPlan() { release(); }

@@ -47,9 +47,19 @@ inline float cos_f(float x) { return (float)std::cos((double)x); }
 inline float sin_f(float x) { return (float)std::sin((double)x); }
 
 // ---- device buffer --------------------------------------------------------
+// Buffers are allocated stream-ordered (cudaMallocAsync) on the stream of the
+// context that the current API call runs on, from the device's default pool,
+// whose release threshold the context raises so that freed memory is reused by
+// the next series instead of going back to the driver.
+void set_alloc_stream(cudaStream_t s);
+// While set, buffers are released with a synchronous cudaFree (used when the
+// owning stream may already be gone).
+void set_sync_free(bool on);
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -94,15 +104,21 @@ struct OpTile {
   int rows;  // padded number of rows
 };
 
-struct ReprojOp {
-  int ip = -1, i0 = -1, i1 = -1;
-  int xb = 0, yb = 0, thick = 0, ray_len = 0;
-  int ntiles = 0;
-  int total_rows = 0;
-  DevBuf coef;      // float [total_rows][kOpTileX]
-  DevBuf rowmap;    // int2 [total_rows] = (absolute tilt index, column)
-  DevBuf tiles;     // OpTile [ntiles]
-  DevBuf colvalid;  // int [xb]: ray validity (count >= 0.8 L)
+// One held-out tilt's operator inside a ReprojOpSet (device pointers).
+struct ReprojOpView {
+  int ip = -1, i0 = -1, nk = 0, xb = 0, yb = 0, ntiles = 0, total_rows = 0;
+  const float* coef = nullptr;      // float [rows][kOpTileX], rows indexed by OpTile::row0
+  const int2* rowmap = nullptr;     // int2 [rows] = (absolute tilt index, column)
+  const OpTile* tiles = nullptr;    // OpTile [ntiles] of this tilt
+  const int* colvalid = nullptr;    // int [xb]: ray validity (count >= 0.8 L)
+};
+
+// Operators of many held-out tilts in one set of allocations.
+struct ReprojOpSet {
+  DevBuf coef, rowmap, tiles, colvalid;
+  std::vector<ReprojOpView> ops;
+  double bytes = 0;  // compulsory bytes of one apply of every operator
+  double fma = 0;    // multiply-adds of one apply of every operator
 };
 
 // ---- kernels (launch wrappers; all ordered on `st`) -------------------------
@@ -128,8 +144,8 @@ int launch_reproject_exact(Context* c, const float* corr, int xb, int yb, size_t
                            const float* d_bp /*[nk][3] w,c,s*/, int i0, int nk, float fcos,
                            float fsin, int ray_len, int thick, const int* d_rowflags,
                            float* out, cudaStream_t st);
-constexpr int kApplyTileY = 64;
-int launch_reproject_apply(Context* c, const ReprojOp& op, const float* corr, size_t pix,
+constexpr int kApplyTileY = 128;  // rows per apply tile (and per sentinel flag)
+int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr, size_t pix,
                            int* d_rowflags, float* out, cudaStream_t st);
 
 // Host-side geometry shared by the operator builder and the exact kernel.
@@ -140,7 +156,9 @@ struct ReprojGeom {
 };
 void reproj_geometry(const float* angles, int ip, int i0, int i1, int xb, int yb, int thick,
                      ReprojGeom* g);
-int build_reproj_op(Context* c, const ReprojGeom& g, ReprojOp* op, cudaStream_t st);
+// Builds the operators of all geometries (same xb, yb) with two launches.
+int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
+                     cudaStream_t st);
 
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
                      int nproj, int* range);

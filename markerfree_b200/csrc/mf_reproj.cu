@@ -93,73 +93,93 @@ __device__ __forceinline__ int cell_bin(int ix, int iz, int W, int T, float c, f
 }
 
 // ---------------------------------------------------------------------------
-// Exact path: one thread per (detector column, row).
+// Exact path: one thread per detector column; a block covers `rows_per_block`
+// image rows.  With row flags (the fallback after the banded apply) a block
+// handles one row tile and leaves at once when that tile holds no sentinel.
 __global__ void k_reproject_exact(const float* __restrict__ corr, int xb, int yb, size_t pix,
                                   const float* __restrict__ bp, int i0, int nk, float fcos,
                                   float fsin, int L, int T, const int* __restrict__ rowflags,
-                                  float* __restrict__ out) {
-  int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y;
-  if (bx >= xb || y >= yb) return;
-  if (rowflags && rowflags[y / kApplyTileY] == 0) return;
+                                  int rows_per_block, float* __restrict__ out) {
+  if (rowflags && rowflags[blockIdx.y] == 0) return;
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bx >= xb) return;
   const int W = 2 * xb;
   const float cent = __fmul_rn((float)xb, 0.5f);
-  RayStart r = ray_start(bx, xb, W, T, fcos, fsin, L);
-  float sum = 0.0f;
-  int cnt = 0;
-  for (int j = 0; j < L; ++j) {
-    int ix, iz;
-    if (!ray_cell(r, j, W, T, fcos, fsin, &ix, &iz)) continue;
-    float fint = 0.0f, fcount = 0.0f;
-    for (int k = 0; k < nk; ++k) {
-      float w = bp[3 * k], c = bp[3 * k + 1], s = bp[3 * k + 2];
-      int b = cell_bin(ix, iz, W, T, c, s, cent, xb);
-      if (b < 0) continue;
-      float v = corr[(size_t)(i0 + k) * pix + (size_t)y * xb + b];
-      if (v < -1e10f) continue;  // mDIntProj turns it into -1e30, then skipped
-      fint = __fadd_rn(fint, __fmul_rn(__fmul_rn(v, c), w));
-      fcount = __fadd_rn(fcount, w);
+  const RayStart r = ray_start(bx, xb, W, T, fcos, fsin, L);
+  const int ya = blockIdx.y * rows_per_block, yz = min(yb, ya + rows_per_block);
+  for (int y = ya; y < yz; ++y) {
+    float sum = 0.0f;
+    int cnt = 0;
+    for (int j = 0; j < L; ++j) {
+      int ix, iz;
+      if (!ray_cell(r, j, W, T, fcos, fsin, &ix, &iz)) continue;
+      float fint = 0.0f, fcount = 0.0f;
+      for (int k = 0; k < nk; ++k) {
+        float w = bp[3 * k], c = bp[3 * k + 1], s = bp[3 * k + 2];
+        int b = cell_bin(ix, iz, W, T, c, s, cent, xb);
+        if (b < 0) continue;
+        float v = corr[(size_t)(i0 + k) * pix + (size_t)y * xb + b];
+        if (v < -1e10f) continue;  // mDIntProj turns it into -1e30, then skipped
+        fint = __fadd_rn(fint, __fmul_rn(__fmul_rn(v, c), w));
+        fcount = __fadd_rn(fcount, w);
+      }
+      float cell = (fcount < 0.001f) ? kSentinel : __fdiv_rn(fint, fcount);
+      if (cell >= -1e10f) {
+        sum = __fadd_rn(sum, cell);
+        cnt += 1;
+      }
     }
-    float cell = (fcount < 0.001f) ? kSentinel : __fdiv_rn(fint, fcount);
-    if (cell >= -1e10f) {
-      sum = __fadd_rn(sum, cell);
-      cnt += 1;
-    }
+    float res =
+        ((float)cnt < __fmul_rn(0.8f, (float)L)) ? kSentinel : __fdiv_rn(sum, (float)cnt);
+    out[(size_t)y * xb + bx] = res;
   }
-  float res = ((float)cnt < __fmul_rn(0.8f, (float)L)) ? kSentinel : __fdiv_rn(sum, (float)cnt);
-  out[(size_t)y * xb + bx] = res;
 }
 
 int launch_reproject_exact(Context* c, const float* corr, int xb, int yb, size_t pix,
                            const float* d_bp, int i0, int nk, float fcos, float fsin, int ray_len,
                            int thick, const int* d_rowflags, float* out, cudaStream_t st) {
-  dim3 blk(128, 1), grd((xb + 127) / 128, yb);
+  const int rpb = d_rowflags ? kApplyTileY : 1;
+  dim3 blk(128, 1), grd((xb + 127) / 128, (yb + rpb - 1) / rpb);
   k_reproject_exact<<<grd, blk, 0, st>>>(corr, xb, yb, pix, d_bp, i0, nk, fcos, fsin, ray_len,
-                                         thick, d_rowflags, out);
+                                         thick, d_rowflags, rpb, out);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
 }
 
 // ---------------------------------------------------------------------------
-// Operator build, pass 1: per column the number of valid ray samples and, per
+// Operator build for a set of held-out tilts (one launch per pass over all of
+// them).  Pass 1: per column the number of valid ray samples and, per
 // neighbour, the range of sinogram bins touched.
-__global__ void k_op_scan(int xb, int T, const float* __restrict__ bp, int nk, float fcos,
-                          float fsin, int L, int* __restrict__ cnt, int* __restrict__ lo,
-                          int* __restrict__ hi) {
+struct OpGeomDev {
+  int nk, ray_len, T, bp_off;  // bp_off: float offset of (w, c, s) triples
+  float fcos, fsin;
+  int lohi_off;  // int offset of this tilt's lo/hi arrays (xb * nk each)
+  int tile_off;  // first OpTile of this tilt
+  int seg_off;   // first int2 of this tilt's segment table (ntiles * nk)
+};
+
+__global__ void k_op_scan(int xb, const OpGeomDev* __restrict__ geoms,
+                          const float* __restrict__ bps, int* __restrict__ cnt,
+                          int* __restrict__ lo, int* __restrict__ hi) {
+  const OpGeomDev g = geoms[blockIdx.y];
   int bx = blockIdx.x * blockDim.x + threadIdx.x;
   if (bx >= xb) return;
+  const float* bp = bps + g.bp_off;
+  const int nk = g.nk, T = g.T, L = g.ray_len;
+  int* lo_t = lo + g.lohi_off + bx * nk;
+  int* hi_t = hi + g.lohi_off + bx * nk;
   const int W = 2 * xb;
   const float cent = __fmul_rn((float)xb, 0.5f);
-  RayStart r = ray_start(bx, xb, W, T, fcos, fsin, L);
+  RayStart r = ray_start(bx, xb, W, T, g.fcos, g.fsin, L);
   int n = 0;
   for (int k = 0; k < nk; ++k) {
-    lo[bx * nk + k] = INT_MAX;
-    hi[bx * nk + k] = -1;
+    lo_t[k] = INT_MAX;
+    hi_t[k] = -1;
   }
   for (int j = 0; j < L; ++j) {
     int ix, iz;
-    if (!ray_cell(r, j, W, T, fcos, fsin, &ix, &iz)) continue;
+    if (!ray_cell(r, j, W, T, g.fcos, g.fsin, &ix, &iz)) continue;
     float fcount = 0.0f;
     for (int k = 0; k < nk; ++k) {
       int b = cell_bin(ix, iz, W, T, bp[3 * k + 1], bp[3 * k + 2], cent, xb);
@@ -170,129 +190,185 @@ __global__ void k_op_scan(int xb, int T, const float* __restrict__ bp, int nk, f
     for (int k = 0; k < nk; ++k) {
       int b = cell_bin(ix, iz, W, T, bp[3 * k + 1], bp[3 * k + 2], cent, xb);
       if (b < 0) continue;
-      if (b < lo[bx * nk + k]) lo[bx * nk + k] = b;
-      if (b > hi[bx * nk + k]) hi[bx * nk + k] = b;
+      if (b < lo_t[k]) lo_t[k] = b;
+      if (b > hi_t[k]) hi_t[k] = b;
     }
   }
-  cnt[bx] = n;
+  cnt[(size_t)blockIdx.y * xb + bx] = n;
 }
 
 // Pass 2: accumulate coefficients.  seg[t*nk + k] = (row offset within the tile,
-// first bin).  Each thread owns one column of its tile, so there are no races.
-__global__ void k_op_fill(int xb, int T, const float* __restrict__ bp, int nk, float fcos,
-                          float fsin, int L, const int* __restrict__ cnt,
-                          const OpTile* __restrict__ tiles, const int2* __restrict__ seg,
+// first bin).  One thread per (column, neighbour): it owns that column's rows of
+// the neighbour's segment, so there are no races and the sums are in ray order.
+__global__ void k_op_fill(int xb, const OpGeomDev* __restrict__ geoms,
+                          const float* __restrict__ bps, const int* __restrict__ cnt,
+                          const OpTile* __restrict__ tiles, const int2* __restrict__ segs,
                           float* __restrict__ coef, int* __restrict__ colvalid) {
-  int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (bx >= xb) return;
-  const int n = cnt[bx];
+  const OpGeomDev g = geoms[blockIdx.z];
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (bx >= xb || k >= g.nk) return;
+  const float* bp = bps + g.bp_off;
+  const int nk = g.nk, T = g.T, L = g.ray_len;
+  const int n = cnt[(size_t)blockIdx.z * xb + bx];
   const bool valid = !((float)n < __fmul_rn(0.8f, (float)L));
-  colvalid[bx] = valid ? 1 : 0;
+  if (k == 0) colvalid[(size_t)blockIdx.z * xb + bx] = valid ? 1 : 0;
   if (!valid) return;
   const int W = 2 * xb;
   const float cent = __fmul_rn((float)xb, 0.5f);
   const int t = bx / kOpTileX, xl = bx % kOpTileX;
-  const OpTile tile = tiles[t];
+  const OpTile tile = tiles[g.tile_off + t];
+  const int2 sg = segs[g.seg_off + t * nk + k];
   const float inv_n = 1.0f / (float)n;
-  RayStart r = ray_start(bx, xb, W, T, fcos, fsin, L);
+  const float ck = bp[3 * k + 1], sk = bp[3 * k + 2], wk = bp[3 * k];
+  float* col = coef + (size_t)tile.row0 * kOpTileX + xl;
+  RayStart r = ray_start(bx, xb, W, T, g.fcos, g.fsin, L);
+  int cur = -1;
+  float acc = 0.0f;
   for (int j = 0; j < L; ++j) {
     int ix, iz;
-    if (!ray_cell(r, j, W, T, fcos, fsin, &ix, &iz)) continue;
+    if (!ray_cell(r, j, W, T, g.fcos, g.fsin, &ix, &iz)) continue;
+    int bk = cell_bin(ix, iz, W, T, ck, sk, cent, xb);
+    if (bk < 0) continue;
     float fcount = 0.0f;
-    for (int k = 0; k < nk; ++k) {
-      int b = cell_bin(ix, iz, W, T, bp[3 * k + 1], bp[3 * k + 2], cent, xb);
-      if (b >= 0) fcount = __fadd_rn(fcount, bp[3 * k]);
+    for (int q = 0; q < nk; ++q) {
+      int b = cell_bin(ix, iz, W, T, bp[3 * q + 1], bp[3 * q + 2], cent, xb);
+      if (b >= 0) fcount = __fadd_rn(fcount, bp[3 * q]);
     }
     if (fcount < 0.001f) continue;
-    for (int k = 0; k < nk; ++k) {
-      int b = cell_bin(ix, iz, W, T, bp[3 * k + 1], bp[3 * k + 2], cent, xb);
-      if (b < 0) continue;
-      int2 sg = seg[t * nk + k];
-      size_t row = (size_t)tile.row0 + sg.x + (b - sg.y);
-      float term = bp[3 * k + 1] * bp[3 * k] / fcount * inv_n;
-      coef[row * kOpTileX + xl] += term;
+    if (bk != cur) {
+      if (cur >= 0) col[(size_t)(sg.x + cur - sg.y) * kOpTileX] += acc;
+      cur = bk;
+      acc = 0.0f;
     }
+    acc += ck * wk / fcount * inv_n;
   }
+  if (cur >= 0) col[(size_t)(sg.x + cur - sg.y) * kOpTileX] += acc;
 }
 
-int build_reproj_op(Context* c, const ReprojGeom& g, ReprojOp* op, cudaStream_t st) {
-  const int xb = g.xb, nk = g.nk;
-  DevBuf d_bp, d_cnt, d_lo, d_hi;
-  MF_TRY(d_bp.alloc(sizeof(float) * g.bp.size()));
-  MF_TRY(d_cnt.alloc(sizeof(int) * xb));
-  MF_TRY(d_lo.alloc(sizeof(int) * xb * nk));
-  MF_TRY(d_hi.alloc(sizeof(int) * xb * nk));
-  MF_CHECK_CUDA(cudaMemcpyAsync(d_bp.p, g.bp.data(), sizeof(float) * g.bp.size(),
+int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
+                     cudaStream_t st) {
+  const int n = (int)geoms.size();
+  set->ops.clear();
+  set->bytes = 0;
+  set->fma = 0;
+  if (n == 0) return MF_OK;
+  const int xb = geoms[0].xb, yb = geoms[0].yb;
+  const int ntiles = (xb + kOpTileX - 1) / kOpTileX;
+  std::vector<OpGeomDev> gd(n);
+  std::vector<float> bps;
+  int lohi = 0, nkmax = 0;
+  for (int i = 0; i < n; ++i) {
+    const ReprojGeom& g = geoms[i];
+    gd[i].nk = g.nk;
+    gd[i].ray_len = g.ray_len;
+    gd[i].T = g.thick;
+    gd[i].bp_off = (int)bps.size();
+    gd[i].fcos = g.fcos;
+    gd[i].fsin = g.fsin;
+    gd[i].lohi_off = lohi;
+    gd[i].tile_off = i * ntiles;
+    gd[i].seg_off = 0;  // set below
+    bps.insert(bps.end(), g.bp.begin(), g.bp.end());
+    lohi += xb * g.nk;
+    nkmax = std::max(nkmax, g.nk);
+  }
+  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi;
+  MF_TRY(d_geom.alloc(sizeof(OpGeomDev) * n));
+  MF_TRY(d_bp.alloc(sizeof(float) * bps.size()));
+  MF_TRY(d_cnt.alloc(sizeof(int) * (size_t)n * xb));
+  MF_TRY(d_lo.alloc(sizeof(int) * (size_t)lohi));
+  MF_TRY(d_hi.alloc(sizeof(int) * (size_t)lohi));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
                                 cudaMemcpyHostToDevice, st));
-  k_op_scan<<<(xb + 127) / 128, 128, 0, st>>>(xb, g.thick, d_bp.as<float>(), nk, g.fcos, g.fsin,
-                                              g.ray_len, d_cnt.as<int>(), d_lo.as<int>(),
-                                              d_hi.as<int>());
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_bp.p, bps.data(), sizeof(float) * bps.size(),
+                                cudaMemcpyHostToDevice, st));
+  k_op_scan<<<dim3((xb + 127) / 128, n), 128, 0, st>>>(xb, d_geom.as<OpGeomDev>(),
+                                                       d_bp.as<float>(), d_cnt.as<int>(),
+                                                       d_lo.as<int>(), d_hi.as<int>());
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
-  std::vector<int> lo((size_t)xb * nk), hi((size_t)xb * nk);
-  MF_CHECK_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, sizeof(int) * lo.size(),
-                                cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, sizeof(int) * hi.size(),
-                                cudaMemcpyDeviceToHost, st));
+  std::vector<int> lo(lohi), hi(lohi);
+  MF_CHECK_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  // Tile layout.
-  const int ntiles = (xb + kOpTileX - 1) / kOpTileX;
-  std::vector<OpTile> tiles(ntiles);
-  std::vector<int2> seg((size_t)ntiles * nk);
+  // Tile layout of every tilt, rows concatenated across tilts.
+  std::vector<OpTile> tiles((size_t)n * ntiles);
+  std::vector<int2> seg;
   std::vector<int2> rowmap;
   int total = 0;
-  for (int t = 0; t < ntiles; ++t) {
-    int x0 = t * kOpTileX, x1 = std::min(xb, x0 + kOpTileX);
-    int rows = 0;
-    for (int k = 0; k < nk; ++k) {
-      int l = INT_MAX, h = -1;
-      for (int x = x0; x < x1; ++x) {
-        l = std::min(l, lo[(size_t)x * nk + k]);
-        h = std::max(h, hi[(size_t)x * nk + k]);
+  for (int i = 0; i < n; ++i) {
+    const ReprojGeom& g = geoms[i];
+    const int nk = g.nk;
+    gd[i].seg_off = (int)seg.size();
+    seg.resize(seg.size() + (size_t)ntiles * nk);
+    const int* lo_t = lo.data() + gd[i].lohi_off;
+    const int* hi_t = hi.data() + gd[i].lohi_off;
+    int first_row = total;
+    for (int t = 0; t < ntiles; ++t) {
+      int x0 = t * kOpTileX, x1 = std::min(xb, x0 + kOpTileX);
+      int rows = 0;
+      for (int k = 0; k < nk; ++k) {
+        int l = INT_MAX, h = -1;
+        for (int x = x0; x < x1; ++x) {
+          l = std::min(l, lo_t[(size_t)x * nk + k]);
+          h = std::max(h, hi_t[(size_t)x * nk + k]);
+        }
+        int2& sgk = seg[gd[i].seg_off + (size_t)t * nk + k];
+        if (h < 0) {
+          sgk = make_int2(rows, 0);
+          continue;
+        }
+        sgk = make_int2(rows, l);
+        for (int b = l; b <= h; ++b) rowmap.push_back(make_int2(g.i0 + k, b));
+        rows += h - l + 1;
       }
-      if (h < 0) {
-        seg[(size_t)t * nk + k] = make_int2(rows, 0);
-        continue;
-      }
-      seg[(size_t)t * nk + k] = make_int2(rows, l);
-      for (int b = l; b <= h; ++b) rowmap.push_back(make_int2(g.i0 + k, b));
-      rows += h - l + 1;
+      int padded = (rows + kOpChunk - 1) / kOpChunk * kOpChunk;
+      if (padded == 0) padded = kOpChunk;
+      for (int r = rows; r < padded; ++r) rowmap.push_back(make_int2(g.i0, 0));
+      tiles[(size_t)i * ntiles + t].row0 = total;
+      tiles[(size_t)i * ntiles + t].rows = padded;
+      total += padded;
     }
-    int padded = (rows + kOpChunk - 1) / kOpChunk * kOpChunk;
-    if (padded == 0) padded = kOpChunk;
-    for (int r = rows; r < padded; ++r) rowmap.push_back(make_int2(g.i0, 0));
-    tiles[t].row0 = total;
-    tiles[t].rows = padded;
-    total += padded;
+    ReprojOpView v;
+    v.ip = g.ip;
+    v.i0 = g.i0;
+    v.nk = nk;
+    v.xb = xb;
+    v.yb = yb;
+    v.ntiles = ntiles;
+    v.total_rows = total - first_row;
+    set->ops.push_back(v);
+    set->bytes += 4.0 * (double)xb * yb * (nk + 1) + (double)v.total_rows * (kOpTileX * 4 + 8);
+    set->fma += (double)yb * v.total_rows * kOpTileX;
   }
-  op->ip = g.ip;
-  op->i0 = g.i0;
-  op->i1 = g.i1;
-  op->xb = xb;
-  op->yb = g.yb;
-  op->thick = g.thick;
-  op->ray_len = g.ray_len;
-  op->ntiles = ntiles;
-  op->total_rows = total;
-  MF_TRY(op->coef.alloc(sizeof(float) * (size_t)total * kOpTileX));
-  MF_TRY(op->rowmap.alloc(sizeof(int2) * (size_t)total));
-  MF_TRY(op->tiles.alloc(sizeof(OpTile) * ntiles));
-  MF_TRY(op->colvalid.alloc(sizeof(int) * xb));
+  MF_TRY(set->coef.alloc(sizeof(float) * (size_t)total * kOpTileX));
+  MF_TRY(set->rowmap.alloc(sizeof(int2) * (size_t)total));
+  MF_TRY(set->tiles.alloc(sizeof(OpTile) * tiles.size()));
+  MF_TRY(set->colvalid.alloc(sizeof(int) * (size_t)n * xb));
   DevBuf d_seg;
   MF_TRY(d_seg.alloc(sizeof(int2) * seg.size()));
-  MF_CHECK_CUDA(cudaMemsetAsync(op->coef.p, 0, sizeof(float) * (size_t)total * kOpTileX, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(op->rowmap.p, rowmap.data(), sizeof(int2) * rowmap.size(),
+  MF_CHECK_CUDA(cudaMemsetAsync(set->coef.p, 0, sizeof(float) * (size_t)total * kOpTileX, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(set->rowmap.p, rowmap.data(), sizeof(int2) * rowmap.size(),
                                 cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(op->tiles.p, tiles.data(), sizeof(OpTile) * ntiles,
+  MF_CHECK_CUDA(cudaMemcpyAsync(set->tiles.p, tiles.data(), sizeof(OpTile) * tiles.size(),
                                 cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_seg.p, seg.data(), sizeof(int2) * seg.size(),
                                 cudaMemcpyHostToDevice, st));
-  k_op_fill<<<(xb + 127) / 128, 128, 0, st>>>(xb, g.thick, d_bp.as<float>(), nk, g.fcos, g.fsin,
-                                              g.ray_len, d_cnt.as<int>(), op->tiles.as<OpTile>(),
-                                              d_seg.as<int2>(), op->coef.as<float>(),
-                                              op->colvalid.as<int>());
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
+                                cudaMemcpyHostToDevice, st));
+  k_op_fill<<<dim3((xb + 127) / 128, nkmax, n), 128, 0, st>>>(
+      xb, d_geom.as<OpGeomDev>(), d_bp.as<float>(), d_cnt.as<int>(), set->tiles.as<OpTile>(),
+      d_seg.as<int2>(), set->coef.as<float>(), set->colvalid.as<int>());
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
+  for (int i = 0; i < n; ++i) {
+    ReprojOpView& v = set->ops[i];
+    v.coef = set->coef.as<float>();
+    v.rowmap = set->rowmap.as<int2>();
+    v.tiles = set->tiles.as<OpTile>() + (size_t)i * ntiles;
+    v.colvalid = set->colvalid.as<int>() + (size_t)i * xb;
+  }
   // the temporaries are freed when this returns; wait for the kernels using them
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;
@@ -300,86 +376,111 @@ int build_reproj_op(Context* c, const ReprojGeom& g, ReprojOp* op, cudaStream_t 
 
 // ---------------------------------------------------------------------------
 // Operator apply: out[y][x] = sum_r A[y][r] * B_t[r][x] with A gathered from the
-// neighbour rows through rowmap.  64 x 64 output tile per CTA, 256 threads with
-// a 4 x 4 register micro-tile each.
-__global__ void __launch_bounds__(256) k_op_apply(const float* __restrict__ corr, int xb, int yb,
-                                                  size_t pix, const float* __restrict__ coef,
-                                                  const int2* __restrict__ rowmap,
-                                                  const OpTile* __restrict__ tiles,
-                                                  const int* __restrict__ colvalid,
-                                                  int* __restrict__ rowflags,
-                                                  float* __restrict__ out) {
-  __shared__ __align__(16) float As[kOpChunk][kApplyTileY];
-  __shared__ __align__(16) float Bs[kOpChunk][kOpTileX];
+// neighbour rows through rowmap.  One CTA computes a kApplyTileY x kOpTileX
+// (128 x 64) output tile with 256 threads, each an 8 x 4 register tile.  Operator
+// rows are consumed kOpChunk at a time through two shared-memory buffers; the
+// next chunk's global loads are issued before the current chunk's FMAs, so
+// memory latency hides behind arithmetic.  Every loaded neighbour value is
+// tested for the -1e30 sentinel; a hit flags the row tile for the exact path.
+constexpr int kApplyThreads = 256;
+constexpr int kAPerThread = kOpChunk * kApplyTileY / kApplyThreads;  // 8
+
+__global__ void __launch_bounds__(kApplyThreads, 2)
+    k_op_apply(const float* __restrict__ corr, int xb, int yb, size_t pix,
+               const float* __restrict__ coef, const int2* __restrict__ rowmap,
+               const OpTile* __restrict__ tiles, const int* __restrict__ colvalid,
+               int* __restrict__ rowflags, float* __restrict__ out) {
+  __shared__ __align__(16) float As[2][kOpChunk][kApplyTileY];
+  __shared__ __align__(16) float Bs[2][kOpChunk][kOpTileX];
   __shared__ int s_flag;
   const int t = blockIdx.x;
   const int y0 = blockIdx.y * kApplyTileY;
   const int x0 = t * kOpTileX;
   const OpTile tile = tiles[t];
   const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
+  const int tx = tid % 16, ty = tid / 16;  // 16 x 4 columns, 16 x 8 rows
   if (tid == 0) s_flag = 0;
-  float acc[4][4];
+  float acc[8][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
   const int lr = tid % kOpChunk;  // operator row this thread loads for A
-  const int ly = tid / kOpChunk;  // base row of y
+  const int ly = tid / kOpChunk;  // first y row it loads (then every 16th)
   bool bad = false;
-  __syncthreads();
-  for (int r0 = 0; r0 < tile.rows; r0 += kOpChunk) {
+  float ra[kAPerThread];
+  float4 rb;
+  auto load_chunk = [&](int r0) {
     const int row = tile.row0 + r0;
-    int2 rm = rowmap[row + lr];
+    const int2 rm = __ldg(rowmap + row + lr);
     const float* src = corr + (size_t)rm.x * pix + rm.y;
 #pragma unroll
-    for (int q = 0; q < kApplyTileY / 16; ++q) {
-      int yy = ly + 16 * q;
-      int y = y0 + yy;
-      float v = 0.0f;
-      if (y < yb) {
-        v = __ldg(src + (size_t)y * xb);
-        bad |= (v < -1e10f);
-      }
-      As[lr][yy] = v;
+    for (int q = 0; q < kAPerThread; ++q) {
+      const int y = y0 + ly + 16 * q;
+      ra[q] = (y < yb) ? __ldg(src + (size_t)y * xb) : 0.0f;
     }
-    const float4* cb = reinterpret_cast<const float4*>(coef + (size_t)row * kOpTileX);
-    reinterpret_cast<float4*>(&Bs[0][0])[tid] = __ldg(cb + tid);
-    __syncthreads();
+    rb = __ldg(reinterpret_cast<const float4*>(coef + (size_t)row * kOpTileX) + tid);
+  };
+  auto store_chunk = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < kAPerThread; ++q) {
+      As[buf][lr][ly + 16 * q] = ra[q];
+      bad |= (ra[q] < -1e10f);
+    }
+    reinterpret_cast<float4*>(&Bs[buf][0][0])[tid] = rb;
+  };
+  const int nchunks = tile.rows / kOpChunk;
+  load_chunk(0);
+  store_chunk(0);
+  __syncthreads();
+  for (int c = 0; c < nchunks; ++c) {
+    const int buf = c & 1;
+    if (c + 1 < nchunks) load_chunk((c + 1) * kOpChunk);
 #pragma unroll
     for (int rr = 0; rr < kOpChunk; ++rr) {
-      float4 a = *reinterpret_cast<const float4*>(&As[rr][ty * 4]);
-      float4 b = *reinterpret_cast<const float4*>(&Bs[rr][tx * 4]);
-      float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][rr][ty * 8]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][rr][ty * 8 + 4]);
+      const float4 b = *reinterpret_cast<const float4*>(&Bs[buf][rr][tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
+    if (c + 1 < nchunks) store_chunk(buf ^ 1);
     __syncthreads();
   }
   if (bad) s_flag = 1;
   __syncthreads();
   if (tid == 0 && s_flag) atomicOr(&rowflags[blockIdx.y], 1);
+  const int xc = x0 + tx * 4;
+  int cv[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int y = y0 + ty * 4 + i;
+  for (int j = 0; j < 4; ++j) cv[j] = (xc + j < xb) ? colvalid[xc + j] : 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int y = y0 + ty * 8 + i;
     if (y >= yb) continue;
+    float v[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int x = x0 + tx * 4 + j;
-      if (x >= xb) continue;
-      out[(size_t)y * xb + x] = colvalid[x] ? acc[i][j] : kSentinel;
+    for (int j = 0; j < 4; ++j) v[j] = cv[j] ? acc[i][j] : kSentinel;
+    float* o = out + (size_t)y * xb + xc;
+    if (xc + 3 < xb && ((xb & 3) == 0)) {
+      *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (xc + j < xb) o[j] = v[j];
     }
   }
 }
 
-int launch_reproject_apply(Context* c, const ReprojOp& op, const float* corr, size_t pix,
+int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr, size_t pix,
                            int* d_rowflags, float* out, cudaStream_t st) {
   dim3 grd(op.ntiles, (op.yb + kApplyTileY - 1) / kApplyTileY);
-  k_op_apply<<<grd, 256, 0, st>>>(corr, op.xb, op.yb, pix, op.coef.as<float>(),
-                                  op.rowmap.as<int2>(), op.tiles.as<OpTile>(),
-                                  op.colvalid.as<int>(), d_rowflags, out);
+  k_op_apply<<<grd, 256, 0, st>>>(corr, op.xb, op.yb, pix, op.coef, op.rowmap, op.tiles,
+                                  op.colvalid, d_rowflags, out);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

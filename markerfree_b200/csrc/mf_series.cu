@@ -44,6 +44,9 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   } else if (kind == 1) {
     int n[1] = {nx}, inem[1] = {cmp}, onem[1] = {nx};
     r = cufftPlanMany(&h, 1, n, inem, 1, cmp, onem, 1, nx, CUFFT_C2R, batch);
+  } else if (kind == 4) {
+    // 1-D R2C in place with the default padded layout (tilt-axis lines)
+    r = cufftPlan1d(&h, nx, CUFFT_R2C, batch);
   } else if (kind == 2) {
     int n[2] = {ny, nx}, inem[2] = {ny, pad}, onem[2] = {ny, cmp};
     r = cufftPlanMany(&h, 2, n, inem, 1, ny * pad, onem, 1, ny * cmp, CUFFT_R2C, batch);
@@ -167,7 +170,7 @@ int transform_doit(mf_series* s, float* max_err_out) {
   float maxerr = 0.0f;
   if (np > 0) {
     MF_TRY(imgs.alloc(sizeof(float) * ppix * np));
-    MF_TRY(part.alloc(sizeof(double2) * kMomentParts * std::max(nz, np)));
+    MF_TRY(part.alloc(sizeof(double2) * moment_parts(yb) * std::max(nz, np)));
     MF_TRY(stats.alloc(sizeof(float2) * std::max(nz, np)));
     MF_TRY(d_idx.alloc(sizeof(int) * np));
     MF_TRY(d_refidx.alloc(sizeof(int) * np));
@@ -179,13 +182,15 @@ int transform_doit(mf_series* s, float* max_err_out) {
     MF_CHECK_CUDA(cudaMemcpyAsync(d_mats.p, mats.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
     const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
     // references: normalise (mean, std) + round edge, all tilts
-    MF_TRY(norm_mask_pad(c, pbuf.as<float>(), pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy, msx,
-                         msy, 4.0f, refs.as<float>(), part.as<double2>(), stats.as<float2>(), st));
+    MF_TRY(norm_mask_pad(c, pbuf.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy,
+                         msx, msy, 4.0f, refs.as<float>(), part.as<double2>(), stats.as<float2>(),
+                         st));
     // images: stretch the padded raw copy, then normalise + round edge
     MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
                         np, 1, imgs.as<float>(), ppix, st));
-    MF_TRY(norm_mask_pad(c, imgs.as<float>(), pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy, msx,
-                         msy, 4.0f, imgs.as<float>(), part.as<double2>(), stats.as<float2>(), st));
+    MF_TRY(norm_mask_pad(c, imgs.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy,
+                         msx, msy, 4.0f, imgs.as<float>(), part.as<double2>(), stats.as<float2>(),
+                         st));
     cufftHandle fr, fi, inv;
     MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));
     MF_TRY(s->ctx->plan({2, xb, yb, np}, &fi));
@@ -273,7 +278,9 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
   L = L / 2 * 2 - 100;
   if (L < 4) return set_error(MF_ERR_ARG, "tilt axis: image too small (line length %d)", L);
   std::vector<float> scores;
-  MF_TRY(tilt_axis_scores(c, s->stack.as<float>(), s->nx, s->ny, nz, s->angles.data(),
+  cufftHandle plan;
+  MF_TRY(s->ctx->plan({4, L, 0, (long long)nz * num}, &plan));
+  MF_TRY(tilt_axis_scores(c, plan, s->stack.as<float>(), s->nx, s->ny, nz, s->angles.data(),
                           s->sx.data(), s->sy.data(), zt, cand.data(), num, L, &scores,
                           c->stream));
   int best = 0;
@@ -403,7 +410,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_TRY(P.scratch.alloc(sizeof(float) * ppix * nz));
   MF_TRY(P.reproj.alloc(sizeof(float) * bpix));
   MF_TRY(P.ccbuf.alloc(sizeof(float) * ppix * 2));
-  MF_TRY(P.part.alloc(sizeof(double2) * kMomentParts * 2 + sizeof(float2) * kPeakParts));
+  MF_TRY(P.part.alloc(sizeof(double2) * moment_parts(yb) * 2 + sizeof(float2) * kPeakParts));
   MF_TRY(P.stats.alloc(sizeof(float2) * 2));
   // outward order (ProjAlign.cpp:229-254) and neighbour ranges
   P.zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
@@ -411,7 +418,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   skip[P.zt] = 0;
   P.order.clear();
   P.geom.clear();
-  P.ops.clear();
+  P.ops.ops.clear();
   for (int i = 1; i < nz; ++i) {
     for (int side = 0; side < 2; ++side) {
       int ip = side == 0 ? P.zt + i : P.zt - i;
@@ -455,16 +462,13 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_CHECK_CUDA(cudaMemcpyAsync(P.d_z0.p, &P.z0, sizeof(float), cudaMemcpyHostToDevice, st));
   P.reproj_bytes = 0;
   P.reproj_fma = 0;
-  for (int k = 0; k < n; ++k) {
+  if (P.method == 1) {
+    MF_TRY(build_reproj_ops(c, P.geom, &P.ops, st));
+    P.reproj_bytes = P.ops.bytes;
+    P.reproj_fma = P.ops.fma;
+  } else {
     // compulsory traffic: the K neighbour images read once, the re-projection written
-    P.reproj_bytes += 4.0 * (double)bpix * (P.geom[k].nk + 1);
-    if (P.method == 1) {
-      P.ops.emplace_back(new ReprojOp());
-      MF_TRY(build_reproj_op(c, P.geom[k], P.ops.back().get(), st));
-      const ReprojOp& op = *P.ops.back();
-      P.reproj_bytes += (double)op.total_rows * (kOpTileX * 4 + 8);
-      P.reproj_fma += (double)yb * op.total_rows * kOpTileX;
-    }
+    for (int k = 0; k < n; ++k) P.reproj_bytes += 4.0 * (double)bpix * (P.geom[k].nk + 1);
   }
   // FFT plans
   MF_TRY(s->ctx->plan({0, xb, yb, (long long)nz * yb}, &P.rows_fwd_all));
@@ -490,7 +494,7 @@ static int pa_enqueue(mf_series* s) {
   float* scratch = P.scratch.as<float>();
   float* cc = P.ccbuf.as<float>();
   double2* mpart = P.part.as<double2>();
-  float2* ppart = reinterpret_cast<float2*>(mpart + kMomentParts * 2);
+  float2* ppart = reinterpret_cast<float2*>(mpart + moment_parts(yb) * 2);
   float2* stats = P.stats.as<float2>();
   MF_CHECK_CUDA(cudaMemsetAsync(P.d_rowflags.p, 0, sizeof(int) * std::max(1, n * P.ytiles), st));
   // CorrTomoStack::DoIt: resample + bin + R-weight every tilt (CorrStack.cu:353-397)
@@ -511,7 +515,7 @@ static int pa_enqueue(mf_series* s) {
     float* reproj = P.reproj.as<float>();
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k], st));
     if (P.method == 1) {
-      MF_TRY(launch_reproject_apply(c, *P.ops[k], corr, bpix, rowflags, reproj, st));
+      MF_TRY(launch_reproject_apply(c, P.ops.ops[k], corr, bpix, rowflags, reproj, st));
       MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
                                     g.nk, g.fcos, g.fsin, g.ray_len, g.thick, rowflags, reproj,
                                     st));
@@ -523,11 +527,8 @@ static int pa_enqueue(mf_series* s) {
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k + 1], st));
     // MeaAlignProj: PANorm both, FFT, filter, inverse FFT, peak
     const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
-    MF_TRY(norm_mask_pad(c, reproj, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy, (float)pad, (float)yb,
-                         4.0f, cc, mpart, stats, st));
-    MF_TRY(norm_mask_pad(c, corr + (size_t)ip * bpix, xb, 0, xb, yb, pad, 0, 1, 0, mcx, mcy,
-                         (float)pad, (float)yb, 4.0f, cc + ppix, mpart + kMomentParts, stats + 1,
-                         st));
+    MF_TRY(norm_mask_pad(c, reproj, corr + (size_t)ip * bpix, xb, 0, xb, yb, pad, ppix, 2, 0, mcx,
+                         mcy, (float)pad, (float)yb, 4.0f, cc, mpart, stats, st));
     MF_CHECK_CUFFT(cufftExecR2C(P.cc_fwd, cc, (cufftComplex*)cc));
     MF_TRY(xcorr_filter(c, (cufftComplex*)cc, 0, nullptr, (cufftComplex*)(cc + ppix), 0, 1, cmp,
                         yb, 500.0f, 1.0f, st));

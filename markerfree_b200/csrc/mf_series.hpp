@@ -26,7 +26,7 @@ struct ProjAlignState {
   float z0 = 0.0f;
   std::vector<int> order;               // outward processing order of held-out tilts
   std::vector<ReprojGeom> geom;         // per entry of `order`
-  std::vector<std::unique_ptr<ReprojOp>> ops;
+  ReprojOpSet ops;
   DevBuf corr;      // nz x yb x xb corrected (R-weighted) stack
   DevBuf scratch;   // nz x yb x pad rows for the batched R-weight FFT
   DevBuf reproj;    // yb x xb

@@ -13,46 +13,70 @@
 
 namespace mf {
 
-constexpr int kRedBlocks = 64;  // partial-sum blocks per image (fixed: deterministic)
+constexpr int kMomRows = 8;  // image rows per partial-sum block
 
-// Masked moments: part[img][blk] = (sum v, sum v^2) over valid pixels.
-__global__ void k_moments(const float* __restrict__ src, int w, int h, int stride,
-                          size_t img_stride, double2* __restrict__ part) {
-  __shared__ double s1[256], s2[256];
-  const float* p = src + (size_t)blockIdx.y * img_stride;
-  double a = 0.0, b = 0.0;
-  const size_t n = (size_t)w * h;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    int y = (int)(i / w), x = (int)(i % w);
-    float v = p[(size_t)y * stride + x];
-    if (v < -1e10f) continue;
-    a += v;
-    b += (double)__fmul_rn(v, v);
+__device__ __forceinline__ const float* image_ptr(const float* src0, const float* src1,
+                                                  size_t img_stride, int img) {
+  return (img == 1 && src1) ? src1 : src0 + (size_t)img * img_stride;
+}
+
+// Block-wide sum of two doubles over 256 threads in a fixed order.
+__device__ __forceinline__ double2 block_sum2(double a, double b) {
+  __shared__ double s1[8], s2[8];
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
   }
-  s1[threadIdx.x] = a;
-  s2[threadIdx.x] = b;
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    s1[w] = a;
+    s2[w] = b;
+  }
   __syncthreads();
-  for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
-    if (threadIdx.x < hh) {
-      s1[threadIdx.x] += s1[threadIdx.x + hh];
-      s2[threadIdx.x] += s2[threadIdx.x + hh];
+  double2 r = make_double2(0.0, 0.0);
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      r.x += s1[i];
+      r.y += s2[i];
     }
-    __syncthreads();
+  return r;
+}
+
+// Masked moments: part[img][blk] = (sum v, sum v^2) over the valid pixels of
+// kMomRows rows.  Image 1 is read from src1 when it is given.
+__global__ void __launch_bounds__(256) k_moments(const float* __restrict__ src0,
+                                                 const float* __restrict__ src1, int w, int h,
+                                                 int stride, size_t img_stride,
+                                                 double2* __restrict__ part) {
+  const float* p = image_ptr(src0, src1, img_stride, blockIdx.y);
+  double a = 0.0, b = 0.0;
+  const int y0 = blockIdx.x * kMomRows, y1 = min(h, y0 + kMomRows);
+  for (int y = y0; y < y1; ++y) {
+    const float* r = p + (size_t)y * stride;
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
+      float v = __ldg(r + x);
+      if (v < -1e10f) continue;
+      a += v;
+      b += (double)__fmul_rn(v, v);
+    }
   }
-  if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(s1[0], s2[0]);
+  double2 s = block_sum2(a, b);
+  if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
 // stats[img] = (mean, std).  with_std = 0: std = 1 (PANorm); 1: CalcCC::mNormalize.
-__global__ void k_moments_final(const double2* __restrict__ part, int nblk, int w, int h,
-                                int with_std, float2* __restrict__ stats) {
-  if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_moments_final(const double2* __restrict__ part, int nblk,
+                                                       int w, int h, int with_std,
+                                                       float2* __restrict__ stats) {
   const double2* p = part + (size_t)blockIdx.x * nblk;
-  double a = 0.0, b = 0.0;
-  for (int i = 0; i < nblk; ++i) {
-    a += p[i].x;
-    b += p[i].y;
+  double a0 = 0.0, b0 = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    a0 += p[i].x;
+    b0 += p[i].y;
   }
+  double2 s = block_sum2(a0, b0);
+  if (threadIdx.x != 0) return;
+  double a = s.x, b = s.y;
   double n = (double)w * (double)h;
   float mean = (float)(a / n);
   float sd = 1.0f;
@@ -66,10 +90,11 @@ __global__ void k_moments_final(const double2* __restrict__ part, int nblk, int 
 
 // Normalise with stats, apply GRoundEdge, zero the pad columns; reads rows of
 // `src_stride` floats (first w used) and writes rows of `pad` floats.
-__global__ void k_norm_mask(const float* __restrict__ src, int src_stride, size_t src_img_stride,
-                            int w, int h, int pad, size_t dst_img_stride,
-                            const float2* __restrict__ stats, float cx, float cy, float msx,
-                            float msy, float power, float* __restrict__ dst) {
+__global__ void k_norm_mask(const float* __restrict__ src, const float* __restrict__ src1,
+                            int src_stride, size_t src_img_stride, int w, int h, int pad,
+                            size_t dst_img_stride, const float2* __restrict__ stats, float cx,
+                            float cy, float msx, float msy, float power,
+                            float* __restrict__ dst) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y * blockDim.y + threadIdx.y;
   int img = blockIdx.z;
@@ -79,7 +104,7 @@ __global__ void k_norm_mask(const float* __restrict__ src, int src_stride, size_
     *d = 0.0f;
     return;
   }
-  float v = src[(size_t)img * src_img_stride + (size_t)y * src_stride + x];
+  float v = image_ptr(src, src1, src_img_stride, img)[(size_t)y * src_stride + x];
   float2 st = stats[img];
   if (!(v < -1e10f)) v = __fdiv_rn(__fsub_rn(v, st.x), st.y);  // GNormalize
   if (v < -1e10f) {                                             // GRoundEdge
@@ -98,16 +123,18 @@ __global__ void k_norm_mask(const float* __restrict__ src, int src_stride, size_
   *d = __fmul_rn(v, fr);
 }
 
-int norm_mask_pad(Context* c, const float* src, int src_stride, size_t src_img_stride, int w,
-                  int h, int pad, size_t dst_img_stride, int nimg, int with_std, float cx,
-                  float cy, float msx, float msy, float power, float* dst, double2* d_part,
-                  float2* d_stats, cudaStream_t st) {
-  dim3 g1(kRedBlocks, nimg);
-  k_moments<<<g1, 256, 0, st>>>(src, w, h, src_stride, src_img_stride, d_part);
-  k_moments_final<<<nimg, 32, 0, st>>>(d_part, kRedBlocks, w, h, with_std, d_stats);
+int moment_parts(int h) { return (h + kMomRows - 1) / kMomRows; }
+
+int norm_mask_pad(Context* c, const float* src, const float* src1, int src_stride,
+                  size_t src_img_stride, int w, int h, int pad, size_t dst_img_stride, int nimg,
+                  int with_std, float cx, float cy, float msx, float msy, float power, float* dst,
+                  double2* d_part, float2* d_stats, cudaStream_t st) {
+  const int nb = moment_parts(h);
+  k_moments<<<dim3(nb, nimg), 256, 0, st>>>(src, src1, w, h, src_stride, src_img_stride, d_part);
+  k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, with_std, d_stats);
   dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
-  k_norm_mask<<<grd, blk, 0, st>>>(src, src_stride, src_img_stride, w, h, pad, dst_img_stride,
-                                   d_stats, cx, cy, msx, msy, power, dst);
+  k_norm_mask<<<grd, blk, 0, st>>>(src, src1, src_stride, src_img_stride, w, h, pad,
+                                   dst_img_stride, d_stats, cx, cy, msx, msy, power, dst);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -172,22 +199,27 @@ __device__ __forceinline__ bool better(float v, int i, float bv, int bi) {
   return v > bv || (v == bv && i < bi);
 }
 
-__global__ void k_peak_partial(const float* __restrict__ map, size_t map_stride, int stride,
-                               int sx, int ex, int sy, int ey, float2* __restrict__ part) {
+// Each block scans a band of rows of the window (rows split evenly over gridDim.x).
+__global__ void __launch_bounds__(256) k_peak_partial(const float* __restrict__ map,
+                                                      size_t map_stride, int stride, int sx,
+                                                      int ex, int sy, int ey,
+                                                      float2* __restrict__ part) {
   __shared__ float sv[256];
   __shared__ int si[256];
   const float* m = map + (size_t)blockIdx.y * map_stride;
-  const int w = ex - sx;
-  const int n = w * (ey - sy);
+  const int rows = ey - sy;
+  const int r0 = sy + (int)((long long)rows * blockIdx.x / gridDim.x);
+  const int r1 = sy + (int)((long long)rows * (blockIdx.x + 1) / gridDim.x);
   float bv = -INFINITY;
   int bi = INT_MAX;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int y = sy + i / w, x = sx + i % w;
-    int li = y * stride + x;
-    float v = m[li];
-    if (better(v, li, bv, bi)) {
-      bv = v;
-      bi = li;
+  for (int y = r0; y < r1; ++y) {
+    for (int x = sx + threadIdx.x; x < ex; x += blockDim.x) {
+      int li = y * stride + x;
+      float v = __ldg(m + li);
+      if (better(v, li, bv, bi)) {
+        bv = v;
+        bi = li;
+      }
     }
   }
   sv[threadIdx.x] = bv;
@@ -205,15 +237,24 @@ __global__ void k_peak_partial(const float* __restrict__ map, size_t map_stride,
     part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = make_float2(sv[0], __int_as_float(si[0]));
 }
 
+// Called by all 32 lanes of warp 0; every lane gets the winner.
 __device__ void reduce_partials(const float2* p, int n, float* bv, int* bi) {
   float v = -INFINITY;
   int idx = INT_MAX;
-  for (int i = 0; i < n; ++i) {
+  for (int i = threadIdx.x; i < n; i += 32) {
     float pv = p[i].x;
     int pi = __float_as_int(p[i].y);
     if (better(pv, pi, v, idx)) {
       v = pv;
       idx = pi;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    float ov = __shfl_xor_sync(0xffffffffu, v, o);
+    int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (better(ov, oi, v, idx)) {
+      v = ov;
+      idx = oi;
     }
   }
   *bv = v;
@@ -282,10 +323,10 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
                                  float* __restrict__ sy, const float* __restrict__ rot,
                                  const float* __restrict__ z0p, float* __restrict__ err,
                                  float* __restrict__ meas) {
-  if (threadIdx.x != 0) return;
   float bv;
   int bi;
   reduce_partials(part, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
   int px = 0, py = 0;
   pa_window_peak(bi, stride, xb, yb, &px, &py);
   double dx, dy, pk;
@@ -320,7 +361,7 @@ int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, flo
   if (sx < 3) sx = 3;
   if (sy < 3) sy = 3;
   int ex = xb - sx, ey = yb - sy;
-  const int nb = 64;
+  const int nb = kPeakParts;
   k_peak_partial<<<dim3(nb, 1), 256, 0, st>>>(map, 0, stride, sx, ex, sy, ey, d_part);
   k_pa_peak_update<<<1, 32, 0, st>>>(map, stride, xb, yb, d_part, nb, ip, nx, ny, d_angles, d_sx,
                                      d_sy, d_rot, d_z0, d_err, d_meas);
@@ -332,10 +373,10 @@ int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, flo
 // Plain peak (PAFindPeak) returning the binned shift and peak value into out[3].
 __global__ void k_pa_peak_only(const float* __restrict__ map, int stride, int xb, int yb,
                                const float2* __restrict__ part, int nparts, float* out) {
-  if (threadIdx.x != 0) return;
   float bv;
   int bi;
   reduce_partials(part, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
   int px, py;
   pa_window_peak(bi, stride, xb, yb, &px, &py);
   double dx, dy, pk;
@@ -350,7 +391,7 @@ int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float
   int sx = xb / 20, sy = yb / 20;
   if (sx < 3) sx = 3;
   if (sy < 3) sy = 3;
-  const int nb = 64;
+  const int nb = kPeakParts;
   k_peak_partial<<<dim3(nb, 1), 256, 0, st>>>(map, 0, stride, sx, xb - sx, sy, yb - sy, d_part);
   k_pa_peak_only<<<1, 32, 0, st>>>(map, stride, xb, yb, d_part, nb, d_out);
   c->launches += 2;
@@ -363,11 +404,11 @@ int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float
 __global__ void k_cc_peak_final(const float* __restrict__ maps, size_t map_stride, int stride,
                                 int w, int h, const float2* __restrict__ part, int nparts,
                                 float2* __restrict__ shifts) {
-  if (threadIdx.x != 0) return;
   const float* m = maps + (size_t)blockIdx.x * map_stride;
   float bv;
   int bi;
   reduce_partials(part + (size_t)blockIdx.x * nparts, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
   int px = 0, py = 0;
   if (bi != INT_MAX) {
     px = bi % stride;

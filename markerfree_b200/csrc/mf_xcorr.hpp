@@ -5,11 +5,15 @@
 
 namespace mf {
 
-int norm_mask_pad(Context* c, const float* src, int src_stride, size_t src_img_stride, int w,
-                  int h, int pad, size_t dst_img_stride, int nimg, int with_std, float cx,
-                  float cy, float msx, float msy, float power, float* dst, double2* d_part,
-                  float2* d_stats, cudaStream_t st);
-constexpr int kMomentParts = 64;
+// Masked mean (and std) of each image, then normalise + round-edge mask into the
+// padded FFT layout.  Image i is read from src + i*src_img_stride, except image 1
+// which is read from src1 when src1 is not null.  d_part needs
+// moment_parts(h) * nimg entries.
+int norm_mask_pad(Context* c, const float* src, const float* src1, int src_stride,
+                  size_t src_img_stride, int w, int h, int pad, size_t dst_img_stride, int nimg,
+                  int with_std, float cx, float cy, float msx, float msy, float power, float* dst,
+                  double2* d_part, float2* d_stats, cudaStream_t st);
+int moment_parts(int h);
 
 int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,
                  cufftComplex* img, size_t img_stride, int npairs, int cmp, int ny, float bfactor,
@@ -22,7 +26,7 @@ int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float
                  float* d_out, cudaStream_t st);
 int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w, int h, int nmaps,
              float2* d_part, float2* d_shifts, cudaStream_t st);
-constexpr int kPeakParts = 64;
+constexpr int kPeakParts = 256;  // partial blocks of the single-map peak search
 int fit_z0(Context* c, int nz, int zt, const float* d_angles, float* d_sx, float* d_sy,
            const float* d_rot, float* d_z0, cudaStream_t st);
 int max_err(Context* c, const float* d_err, const int* d_order, int n, float* d_out,
@@ -38,7 +42,8 @@ int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
 // Common-line tilt-axis search over all tilts (Rotate.cu).  Scores (num floats)
 // are returned to the host; the caller applies the arg-max rule.
 struct AxisPlanCache;
-int tilt_axis_scores(Context* c, const float* stack, int nx, int ny, int nz, const float* angles,
+int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, int ny, int nz,
+                     const float* angles,
                      const float* sx, const float* sy, int zt, const float* rot_cand, int num,
                      int line_len, std::vector<float>* scores, cudaStream_t st);
 
