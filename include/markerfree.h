@@ -67,11 +67,16 @@ typedef struct {
   int gpu;           /* G: CUDA device ordinal                                  */
   int nproj;         /* -p: neighbours back-projected per held-out tilt         */
   int save_mode;     /* -s: 0 = .txt, 1 = .xf                                   */
+  int precision;     /* mf_precision of the re-projection operands (not in the
+                        reference; 0 = FP32, which is the reference's arithmetic) */
 } mf_options;
 
 /* Precision of the re-projection operands (the corrected stack rows and the
  * back-projection operator).  Accumulation is always FP32; peak fitting, shift
- * accumulation and the rotation-centre normal equation are FP64. */
+ * accumulation and the rotation-centre normal equation are FP64.  FP16/BF16 run
+ * the re-projection on the tensor cores; 128-row tiles whose neighbour rows hold
+ * a -1e30 sentinel (or, for FP16, a value beyond its range) are recomputed with
+ * the exact FP32 gather. */
 typedef enum { MF_PREC_FP32 = 0, MF_PREC_BF16 = 1, MF_PREC_FP16 = 2 } mf_precision;
 
 typedef struct mf_context mf_context;
@@ -102,6 +107,8 @@ MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw_stack, in
                                    int nz, const float* file_angles, mf_series** out);
 /* Destroy every series of a context before the context itself. */
 MF_API void mf_series_destroy(mf_series* s);
+/* Takes effect at the next mf_projalign_setup (a set-up pass of another
+ * precision is discarded; mf_proj_align sets up by itself). */
 MF_API int mf_series_set_precision(mf_series* s, mf_precision p);
 /* Copies the pre-processed stack (nz*ny*nx floats) to host memory. */
 MF_API int mf_series_get_stack(mf_series* s, float* host_out);
@@ -165,6 +172,10 @@ MF_API int mf_context_stage_times(mf_context* ctx, double* out6);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work or timing events after the library's. */
 MF_API void* mf_context_stream(mf_context* ctx);
+/* Image rows per tensor-core tile of the FP16/BF16 re-projection (64, 128 or
+ * 256; 0 = chosen from the image shape and the SM count).  Read when a pass is
+ * set up (mf_projalign_setup) or a single re-projection is queued. */
+MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
 
 /* ---- single kernels on caller-owned device memory (same stream semantics:
  * the call is ordered on the context stream and returns after queuing). ------ */
@@ -179,7 +190,9 @@ MF_API int mf_find_proj_range(const float* angles, int nz, const unsigned char* 
 /* CalcReprojFBP::DoIt (CalcReproj.cu:255-311): back-project tilts [istart, iend] of
  * the corrected stack d_corr (nz x yb x xb) into a 2*xb x thickness slab per row
  * and re-project it at angles[iproj] into d_out (yb x xb).  method 0 = exact
- * per-sample gather, 1 = banded operator (the production path). */
+ * per-sample gather, 1 = banded operator in FP32 (the FP32 production path),
+ * 2 / 3 = the same operator applied on the tensor cores with FP16 / BF16 operands
+ * and FP32 accumulation (the mixed-precision production path). */
 MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb, int nz,
                             const float* angles, int iproj, int istart, int iend, int thickness,
                             int method, float* d_out);

@@ -48,7 +48,8 @@ class OptionsC(ctypes.Structure):
     _fields_ = [("offset", ctypes.c_float), ("pitch_angle", ctypes.c_float),
                 ("zshift", ctypes.c_float), ("thickness", ctypes.c_int),
                 ("align_z", ctypes.c_int), ("out_bin", ctypes.c_int), ("gpu", ctypes.c_int),
-                ("nproj", ctypes.c_int), ("save_mode", ctypes.c_int)]
+                ("nproj", ctypes.c_int), ("save_mode", ctypes.c_int),
+                ("precision", ctypes.c_int)]
 
 
 # (name, restype, argtypes) of every entry point in include/markerfree.h
@@ -93,6 +94,7 @@ SIGNATURES = [
     ("mf_context_stage_times", ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_double)]),
     ("mf_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("mf_context_set_tc_rows", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -188,6 +190,10 @@ class Context:
         keys = ("reproj_ms", "reproj_launches", "xcorr_ms", "passes", "reproj_bytes",
                 "reproj_fma")
         return dict(zip(keys, out))
+
+    def set_tc_rows(self, rows: int):
+        """Image rows per tensor-core tile (64, 128, 256; 0 = automatic)."""
+        _check(lib().mf_context_set_tc_rows(self.h, int(rows)))
 
     def stream_ptr(self) -> int:
         return int(lib().mf_context_stream(self.h) or 0)
@@ -305,13 +311,13 @@ class Series:
 
 
 def align(ctx: Context, raw_stack, file_angles, offset=0.0, pitch_angle=0.0, zshift=0.0,
-          align_z=600, out_bin=1, nproj=10, want_stack=True):
+          align_z=600, out_bin=1, nproj=10, want_stack=True, precision=PREC_FP32):
     """Process::DoIt minus file I/O.  Returns (Param, aligned stack or None, passes)."""
     raw = _f32(raw_stack)
     nz, ny, nx = raw.shape
     p = Param(nz)
     c = p.c()
-    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
     out = None
     ptr = None
     if want_stack:
@@ -326,12 +332,13 @@ def align(ctx: Context, raw_stack, file_angles, offset=0.0, pitch_angle=0.0, zsh
 
 
 def align_device(ctx: Context, d_raw, nx, ny, nz, file_angles, d_out, offset=0.0,
-                 pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10):
+                 pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10,
+                 precision=PREC_FP32):
     """mf_align_device: raw stack and aligned output in device memory (torch tensors or
     addresses).  Returns (Param, passes)."""
     p = Param(nz)
     c = p.c()
-    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
     n = ctypes.c_int()
     _check(lib().mf_align_device(ctx.h, _ptr(d_raw), nx, ny, nz, _f32(file_angles)[:nz],
                                  ctypes.byref(o), ctypes.byref(c), _ptr(d_out), ctypes.byref(n)))
@@ -340,11 +347,12 @@ def align_device(ctx: Context, d_raw, nx, ny, nz, file_angles, d_out, offset=0.0
 
 
 def align_host_ptr(ctx: Context, raw_ptr: int, nx, ny, nz, file_angles, out_ptr: int,
-                   offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10):
+                   offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10,
+                   precision=PREC_FP32):
     """mf_align on caller-owned host buffers given by address (e.g. pinned memory)."""
     p = Param(nz)
     c = p.c()
-    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0)
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
     n = ctypes.c_int()
     f = lib().mf_align
     raw_arr = np.ctypeslib.as_array(ctypes.cast(raw_ptr, _c_float_p), (nz * ny * nx,))

@@ -97,6 +97,14 @@ MF_API int mf_context_stage_times(mf_context* ctx, double* out6) {
 
 MF_API void* mf_context_stream(mf_context* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
 
+MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows) {
+  if (!ctx) return set_error(MF_ERR_ARG, "null context");
+  if (rows != 0 && rows != 64 && rows != 128 && rows != 256)
+    return set_error(MF_ERR_ARG, "tensor-core tile rows must be 0, 64, 128 or 256 (got %d)", rows);
+  ctx->c.tc_rows = rows;
+  return MF_OK;
+}
+
 // ---------------------------------------------------------------------------
 static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_device, int nx,
                                 int ny, int nz, const float* file_angles, mf_series** out) {
@@ -158,6 +166,12 @@ MF_API int mf_series_set_precision(mf_series* s, mf_precision p) {
   if (!s) return set_error(MF_ERR_ARG, "null series");
   if (p != MF_PREC_FP32 && p != MF_PREC_BF16 && p != MF_PREC_FP16)
     return set_error(MF_ERR_ARG, "unknown precision %d", (int)p);
+  if (s->precision != p && s->pa.ready) {
+    // the operators and buffers of the set-up pass belong to the old precision
+    if (s->pa.graph) cudaGraphExecDestroy(s->pa.graph);
+    s->pa.graph = nullptr;
+    s->pa.ready = false;
+  }
   s->precision = p;
   return MF_OK;
 }
@@ -296,8 +310,12 @@ static int align_common(mf_context* ctx, const float* raw, bool on_device, int n
   if (!opt || !param) return set_error(MF_ERR_ARG, "null options or parameters");
   if (opt->nproj <= 0) return set_error(MF_ERR_ARG, "nProj must be > 0.");
   if (opt->out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
+  if (opt->precision != MF_PREC_FP32 && opt->precision != MF_PREC_BF16 &&
+      opt->precision != MF_PREC_FP16)
+    return set_error(MF_ERR_ARG, "unknown precision %d", opt->precision);
   mf_series* s = nullptr;
   MF_TRY(series_create_common(ctx, raw, on_device, nx, ny, nz, file_angles, &s));
+  s->precision = (mf_precision)opt->precision;
   int rc = MF_OK;
   int np = 0;
   if (opt->align_z != 0) {
@@ -392,6 +410,34 @@ MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb
   if (method == 0) {
     MF_TRY(launch_reproject_exact(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0, g.nk,
                                   g.fcos, g.fsin, g.ray_len, g.thick, nullptr, d_out, st));
+  } else if (method == 2 || method == 3) {
+    // tensor-core apply on a 16-bit copy of the neighbour tilts
+    const int prec = method == 2 ? MF_PREC_FP16 : MF_PREC_BF16;
+    const int xpitch = (xb + 7) / 8 * 8;
+    const int ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
+    TcOpSet set;
+    std::vector<ReprojGeom> gs(1, g);
+    MF_TRY(build_reproj_tc_ops(&ctx->c, gs, prec, &set, st));
+    MF_TRY(S->c.alloc((size_t)2 * xpitch * yb * nz));
+    MF_TRY(S->d.alloc(sizeof(int) * ((size_t)nz * ytiles + 1)));
+    int* tflags = S->d.as<int>();
+    int* err = tflags + (size_t)nz * ytiles;
+    MF_CHECK_CUDA(cudaMemsetAsync(S->d.p, 0, sizeof(int) * ((size_t)nz * ytiles + 1), st));
+    MF_TRY(launch_to_half(&ctx->c, d_corr, xb, yb, nullptr, istart, iend - istart + 1, prec,
+                          S->c.p, xpitch, tflags, st));
+    TmaDesc imgmap;
+    const int nb = tc_pick_rows(&ctx->c, xb, yb);
+    MF_TRY(tc_prepare(&ctx->c, nb));
+    MF_TRY(tc_image_map(S->c.p, prec, xb, xpitch, yb, nz, nb, &imgmap));
+    MF_TRY(launch_reproject_tc(&ctx->c, set, set.ops[0], imgmap, nb, err, d_out, st));
+    MF_TRY(launch_reproject_exact_flagged(&ctx->c, d_corr, xb, yb, pix, S->b.as<float>(), g.i0,
+                                          g.nk, g.fcos, g.fsin, g.ray_len, g.thick, tflags, d_out,
+                                          st));
+    int herr = 0;
+    MF_CHECK_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (herr != 0)
+      return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", herr);
   } else {
     ReprojOpSet set;
     std::vector<ReprojGeom> gs(1, g);

@@ -31,6 +31,7 @@ struct Options {
   std::string method;
   int iteration = 0;
   float gamma = 0;
+  int precision = MF_PREC_FP32;  // --precision (not in the reference)
 };
 
 void usage() {
@@ -44,6 +45,8 @@ void usage() {
             << "    RP\n"
             << "[-p NPROJ]\n    Number of neighbor projections\n"
             << "[-s SAVE_MODE]\n    SaveParameter (0 or 1)\n"
+            << "[--precision fp32|fp16|bf16]\n"
+            << "    Re-projection operands (fp32 is the reference's arithmetic)\n"
             << "[-h]\n    Help\n";
 }
 
@@ -76,6 +79,7 @@ int get_opts(int argc, char** argv, Options* o) {
                                      {"mode", required_argument, nullptr, 'm'},
                                      {"savemode", required_argument, nullptr, 's'},
                                      {"nproj", required_argument, nullptr, 'p'},
+                                     {"precision", required_argument, nullptr, 1000},
                                      {nullptr, 0, nullptr, 0}};
   int ch;
   while ((ch = getopt_long(argc, argv, "hi:o:n:a:g:m:s:p:", longopts, nullptr)) != -1) {
@@ -91,6 +95,19 @@ int get_opts(int argc, char** argv, Options* o) {
       case 'h':
         usage();
         return 0;
+      case 1000:
+        if (strcmp(optarg, "fp32") == 0) {
+          o->precision = MF_PREC_FP32;
+        } else if (strcmp(optarg, "fp16") == 0) {
+          o->precision = MF_PREC_FP16;
+        } else if (strcmp(optarg, "bf16") == 0) {
+          o->precision = MF_PREC_BF16;
+        } else {
+          printf("precision must be fp32, fp16 or bf16.");
+          fflush(stdout);
+          return -1;
+        }
+        break;
       case 'i':
         std::istringstream(optarg) >> o->input;
         break;
@@ -207,6 +224,7 @@ void run(const Options& o) {
   mo.gpu = o.gpu;
   mo.nproj = o.nproj;
   mo.save_mode = o.save_mode;
+  mo.precision = o.precision;
   std::vector<float> sx(nz), sy(nz), rot(nz);
   mf_align_param p{sx.data(), sy.data(), rot.data(), 0.0f};
   int xo, yo;

@@ -87,6 +87,7 @@ struct Context {
   int64_t launches = 0;  // library kernel launches queued (for reporting)
   int sm_count = 148;
   bool profiling = false;
+  int tc_rows = 0;  // tensor-core tile rows (64/128/256); 0 = chosen per shape
   double stage[6] = {0, 0, 0, 0, 0, 0};  // see mf_context_stage_times
 };
 
@@ -119,6 +120,52 @@ struct ReprojOpSet {
   std::vector<ReprojOpView> ops;
   double bytes = 0;  // compulsory bytes of one apply of every operator
   double fma = 0;    // multiply-adds of one apply of every operator
+};
+
+// ---- tensor-core (tcgen05) form of the same operator ------------------------
+// Used by the FP16/BF16 precision modes: operator coefficients and neighbour rows
+// in 16 bits, products accumulated in FP32 in tensor memory.  Output columns are
+// grouped in x-tiles of kTcM = 128 (the MMA's M).  For x-tile t and neighbour k
+// the touched bins [lo, hi] become a segment starting at b0 = lo rounded down to
+// a multiple of 8 (a TMA box must start on a 16-byte boundary) and covering
+// nch chunks of kTcK = 64 bins (one 128-byte swizzle row of 16-bit values).
+// Chunk c of the operator is a 128 x 64 block stored K-major: the 64
+// coefficients of output column m are contiguous, at op16 + (c*128 + m)*64.
+// Coefficients are stored multiplied by kTcScale (a power of two that keeps them
+// inside the FP16 normal range); the epilogue divides it out exactly.
+constexpr int kTcM = 128;
+constexpr int kTcK = 64;
+constexpr float kTcScale = 64.0f;
+struct TcSeg {
+  int tilt;    // absolute tilt index of the neighbour
+  int b0;      // first bin of the segment (multiple of 8)
+  int nch;     // chunks of kTcK bins
+  int chunk0;  // first chunk of the segment in the operator
+};
+struct TcXTile {
+  int seg0;  // first segment of this x-tile in the segment table
+  int nseg;
+  int nch;   // chunks over all segments
+  int pad;
+};
+// Opaque storage for a CUtensorMap (the driver type is 64-byte aligned, 128 B).
+struct alignas(64) TmaDesc {
+  unsigned char b[128];
+};
+struct TcOpView {
+  int ip = -1, i0 = 0, nk = 0, xb = 0, yb = 0, ntx = 0, nchunks = 0;
+  const TcXTile* xt = nullptr;  // [ntx] (segment indices are global)
+  const TcSeg* segs = nullptr;  // the set's whole segment table
+  const int* colvalid = nullptr;
+};
+struct TcOpSet {
+  DevBuf op16, xt, segs, colvalid;
+  std::vector<TcOpView> ops;
+  int total_chunks = 0;
+  int half_kind = 0;  // MF_PREC_BF16 or MF_PREC_FP16
+  TmaDesc opmap;      // 2-D tensor map over op16, box 64 x 128
+  double bytes = 0;   // compulsory bytes of one apply of every operator
+  double fma = 0;     // multiply-adds issued to the tensor cores
 };
 
 // ---- kernels (launch wrappers; all ordered on `st`) -------------------------
@@ -159,6 +206,39 @@ void reproj_geometry(const float* angles, int ip, int i0, int i1, int xb, int yb
 // Builds the operators of all geometries (same xb, yb) with two launches.
 int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
                      cudaStream_t st);
+
+// Tensor-core operators of all geometries (same xb, yb) in `half_kind` precision.
+int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
+                        TcOpSet* set, cudaStream_t st);
+// Encodes set->opmap over set->op16 (called by build_reproj_tc_ops).
+int tc_op_map(TcOpSet* set);
+// 3-D tensor map over a 16-bit copy of the corrected stack (nz x yb rows of xb
+// values with row pitch `xpitch` elements), box 64 bins x nb rows.
+int tc_image_map(const void* base, int half_kind, int xb, int xpitch, int yb, int nz, int nb,
+                 TmaDesc* out);
+// Rows per tensor-core tile (the MMA's N) for an image shape: the context's
+// override if set, else the widest of 256/128/64 that still gives most SMs a tile.
+int tc_pick_rows(const Context* c, int xb, int yb);
+// Sets the kernel attributes of the tile-rows variant `nb` on the current device
+// (done outside any stream capture).
+int tc_prepare(Context* c, int nb);
+// out (yb x xb) = tensor-core apply of one operator to the 16-bit stack behind
+// `imgmap`; columns without a valid ray get -1e30.  *d_err becomes non-zero if a
+// pipeline wait gave up (the kernel then returns without finishing).
+int launch_reproject_tc(Context* c, const TcOpSet& set, const TcOpView& op, const TmaDesc& imgmap,
+                        int nb, int* d_err, float* out, cudaStream_t st);
+// FP32 corrected images -> 16-bit copy (row pitch xpitch) for tilts d_tilts[0..n)
+// (or tilts tilt0..tilt0+n-1 when d_tilts is null).  tflags[tilt * ytiles + t]
+// is set when 128-row tile t of the tilt holds a value the 16-bit path cannot
+// carry (a -1e30 sentinel, a NaN, or a magnitude beyond the FP16 range).
+int launch_to_half(Context* c, const float* src, int xb, int yb, const int* d_tilts, int tilt0,
+                   int n, int half_kind, void* dst, int xpitch, int* tflags, cudaStream_t st);
+// Exact re-projection of the 128-row tiles of `out` whose neighbour tilts
+// [i0, i0+nk) have a tflags entry set (the fallback after the tensor-core apply).
+int launch_reproject_exact_flagged(Context* c, const float* corr, int xb, int yb, size_t pix,
+                                   const float* d_bp, int i0, int nk, float fcos, float fsin,
+                                   int ray_len, int thick, const int* tflags, float* out,
+                                   cudaStream_t st);
 
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
                      int nproj, int* range);

@@ -20,6 +20,10 @@
 //    the K neighbour rows to the output row, the same for every row: a banded
 //    matrix.  It is built once per series (the angles do not change while
 //    projection matching runs) and applied to all Yb rows as a dense-tiled GEMM.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 
@@ -99,8 +103,15 @@ __device__ __forceinline__ int cell_bin(int ix, int iz, int W, int T, float c, f
 __global__ void k_reproject_exact(const float* __restrict__ corr, int xb, int yb, size_t pix,
                                   const float* __restrict__ bp, int i0, int nk, float fcos,
                                   float fsin, int L, int T, const int* __restrict__ rowflags,
-                                  int rows_per_block, float* __restrict__ out) {
+                                  const int* __restrict__ tflags, int rows_per_block,
+                                  float* __restrict__ out) {
   if (rowflags && rowflags[blockIdx.y] == 0) return;
+  if (tflags) {
+    // per-tilt flags of the 16-bit copy: recompute the tile if any neighbour's is set
+    int any = 0;
+    for (int k = 0; k < nk; ++k) any |= tflags[(size_t)(i0 + k) * gridDim.y + blockIdx.y];
+    if (!any) return;
+  }
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
   if (bx >= xb) return;
   const int W = 2 * xb;
@@ -141,7 +152,19 @@ int launch_reproject_exact(Context* c, const float* corr, int xb, int yb, size_t
   const int rpb = d_rowflags ? kApplyTileY : 1;
   dim3 blk(128, 1), grd((xb + 127) / 128, (yb + rpb - 1) / rpb);
   k_reproject_exact<<<grd, blk, 0, st>>>(corr, xb, yb, pix, d_bp, i0, nk, fcos, fsin, ray_len,
-                                         thick, d_rowflags, rpb, out);
+                                         thick, d_rowflags, nullptr, rpb, out);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int launch_reproject_exact_flagged(Context* c, const float* corr, int xb, int yb, size_t pix,
+                                   const float* d_bp, int i0, int nk, float fcos, float fsin,
+                                   int ray_len, int thick, const int* tflags, float* out,
+                                   cudaStream_t st) {
+  dim3 blk(128, 1), grd((xb + 127) / 128, (yb + kApplyTileY - 1) / kApplyTileY);
+  k_reproject_exact<<<grd, blk, 0, st>>>(corr, xb, yb, pix, d_bp, i0, nk, fcos, fsin, ray_len,
+                                         thick, nullptr, tflags, kApplyTileY, out);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -369,6 +392,271 @@ int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpS
     v.tiles = set->tiles.as<OpTile>() + (size_t)i * ntiles;
     v.colvalid = set->colvalid.as<int>() + (size_t)i * xb;
   }
+  // the temporaries are freed when this returns; wait for the kernels using them
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core operator build.  The band of every (x-tile, neighbour) comes from
+// the same scan as above; the coefficients are accumulated in FP32 into a
+// staging buffer laid out like the final operator (chunk-major, K-major inside a
+// chunk), then rounded once to 16 bits.  Held-out tilts are processed in groups
+// so that the FP32 staging buffer stays small.
+struct TcFillGeom {
+  int nk, ray_len, T, bp_off;
+  float fcos, fsin;
+  int cnt_off;     // int offset of this tilt's per-column valid-sample counts
+  int segidx_off;  // int offset of this tilt's (x-tile, neighbour) -> segment table
+  int chunk_base;  // first chunk of the staging buffer's window
+  int cv_off;      // int offset of this tilt's colvalid entries
+};
+
+__global__ void k_optc_fill(int xb, const TcFillGeom* __restrict__ geoms,
+                            const float* __restrict__ bps, const int* __restrict__ cnt,
+                            const int* __restrict__ segidx, const TcSeg* __restrict__ segs,
+                            float* __restrict__ stage, int* __restrict__ colvalid) {
+  const TcFillGeom g = geoms[blockIdx.z];
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (bx >= xb || k >= g.nk) return;
+  const float* bp = bps + g.bp_off;
+  const int nk = g.nk, T = g.T, L = g.ray_len;
+  const int n = cnt[g.cnt_off + bx];
+  const bool valid = !((float)n < __fmul_rn(0.8f, (float)L));
+  if (k == 0) colvalid[g.cv_off + bx] = valid ? 1 : 0;
+  if (!valid) return;
+  const int t = bx / kTcM, m = bx % kTcM;
+  const int si = segidx[g.segidx_off + t * nk + k];
+  if (si < 0) return;
+  const TcSeg sg = segs[si];
+  const int W = 2 * xb;
+  const float cent = __fmul_rn((float)xb, 0.5f);
+  const float inv_n = 1.0f / (float)n;
+  const float ck = bp[3 * k + 1], sk = bp[3 * k + 2], wk = bp[3 * k];
+  float* base = stage + ((size_t)(sg.chunk0 - g.chunk_base) * kTcM + m) * kTcK;
+  RayStart r = ray_start(bx, xb, W, T, g.fcos, g.fsin, L);
+  int cur = -1;
+  float acc = 0.0f;
+  auto flush = [&]() {
+    const int d = cur - sg.b0;
+    base[(size_t)(d / kTcK) * kTcM * kTcK + (d % kTcK)] += acc;
+  };
+  for (int j = 0; j < L; ++j) {
+    int ix, iz;
+    if (!ray_cell(r, j, W, T, g.fcos, g.fsin, &ix, &iz)) continue;
+    int bk = cell_bin(ix, iz, W, T, ck, sk, cent, xb);
+    if (bk < 0) continue;
+    float fcount = 0.0f;
+    for (int q = 0; q < nk; ++q) {
+      int b = cell_bin(ix, iz, W, T, bp[3 * q + 1], bp[3 * q + 2], cent, xb);
+      if (b >= 0) fcount = __fadd_rn(fcount, bp[3 * q]);
+    }
+    if (fcount < 0.001f) continue;
+    if (bk != cur) {
+      if (cur >= 0) flush();
+      cur = bk;
+      acc = 0.0f;
+    }
+    acc += ck * wk / fcount * inv_n;
+  }
+  if (cur >= 0) flush();
+}
+
+__global__ void k_op_to_fp16(const float* __restrict__ src, size_t n, float scale,
+                             __half* __restrict__ dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = __float2half_rn(src[i] * scale);
+}
+__global__ void k_op_to_bf16(const float* __restrict__ src, size_t n, float scale,
+                             __nv_bfloat16* __restrict__ dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = __float2bfloat16_rn(src[i] * scale);
+}
+
+int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
+                        TcOpSet* set, cudaStream_t st) {
+  const int n = (int)geoms.size();
+  set->ops.clear();
+  set->bytes = 0;
+  set->fma = 0;
+  set->total_chunks = 0;
+  set->half_kind = half_kind;
+  if (half_kind != MF_PREC_BF16 && half_kind != MF_PREC_FP16)
+    return set_error(MF_ERR_ARG, "tensor-core operators need FP16 or BF16 (got %d)", half_kind);
+  if (n == 0) return MF_OK;
+  const int xb = geoms[0].xb, yb = geoms[0].yb;
+  const int ntx = (xb + kTcM - 1) / kTcM;
+  // pass 1: per column valid-sample count and per neighbour bin range
+  std::vector<OpGeomDev> gd(n);
+  std::vector<float> bps;
+  int lohi = 0;
+  for (int i = 0; i < n; ++i) {
+    const ReprojGeom& g = geoms[i];
+    gd[i].nk = g.nk;
+    gd[i].ray_len = g.ray_len;
+    gd[i].T = g.thick;
+    gd[i].bp_off = (int)bps.size();
+    gd[i].fcos = g.fcos;
+    gd[i].fsin = g.fsin;
+    gd[i].lohi_off = lohi;
+    gd[i].tile_off = 0;
+    gd[i].seg_off = 0;
+    bps.insert(bps.end(), g.bp.begin(), g.bp.end());
+    lohi += xb * g.nk;
+  }
+  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi;
+  MF_TRY(d_geom.alloc(sizeof(OpGeomDev) * n));
+  MF_TRY(d_bp.alloc(sizeof(float) * bps.size()));
+  MF_TRY(d_cnt.alloc(sizeof(int) * (size_t)n * xb));
+  MF_TRY(d_lo.alloc(sizeof(int) * (size_t)lohi));
+  MF_TRY(d_hi.alloc(sizeof(int) * (size_t)lohi));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
+                                cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_bp.p, bps.data(), sizeof(float) * bps.size(),
+                                cudaMemcpyHostToDevice, st));
+  k_op_scan<<<dim3((xb + 127) / 128, n), 128, 0, st>>>(xb, d_geom.as<OpGeomDev>(),
+                                                       d_bp.as<float>(), d_cnt.as<int>(),
+                                                       d_lo.as<int>(), d_hi.as<int>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  std::vector<int> lo(lohi), hi(lohi);
+  MF_CHECK_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  // segments: per tilt, per x-tile, per neighbour with a non-empty band
+  std::vector<TcSeg> segs;
+  std::vector<TcXTile> xts((size_t)n * ntx);
+  std::vector<int> segidx;  // [tilt][x-tile][neighbour]
+  std::vector<int> segidx_off(n), chunk_first(n + 1);
+  int chunks = 0;
+  for (int i = 0; i < n; ++i) {
+    const ReprojGeom& g = geoms[i];
+    const int nk = g.nk;
+    segidx_off[i] = (int)segidx.size();
+    segidx.resize(segidx.size() + (size_t)ntx * nk, -1);
+    chunk_first[i] = chunks;
+    const int* lo_t = lo.data() + gd[i].lohi_off;
+    const int* hi_t = hi.data() + gd[i].lohi_off;
+    for (int t = 0; t < ntx; ++t) {
+      const int x0 = t * kTcM, x1 = std::min(xb, x0 + kTcM);
+      TcXTile& X = xts[(size_t)i * ntx + t];
+      X.seg0 = (int)segs.size();
+      X.nseg = 0;
+      X.nch = 0;
+      X.pad = 0;
+      for (int k = 0; k < nk; ++k) {
+        int l = INT_MAX, h = -1;
+        for (int x = x0; x < x1; ++x) {
+          l = std::min(l, lo_t[(size_t)x * nk + k]);
+          h = std::max(h, hi_t[(size_t)x * nk + k]);
+        }
+        if (h < 0) continue;
+        TcSeg sg;
+        sg.tilt = g.i0 + k;
+        sg.b0 = l & ~7;
+        sg.nch = (h - sg.b0 + kTcK) / kTcK;
+        sg.chunk0 = chunks;
+        chunks += sg.nch;
+        segidx[segidx_off[i] + t * nk + k] = (int)segs.size();
+        segs.push_back(sg);
+        X.nseg++;
+        X.nch += sg.nch;
+      }
+    }
+    TcOpView v;
+    v.ip = g.ip;
+    v.i0 = g.i0;
+    v.nk = nk;
+    v.xb = xb;
+    v.yb = yb;
+    v.ntx = ntx;
+    v.nchunks = chunks - chunk_first[i];
+    set->ops.push_back(v);
+    // compulsory traffic: 16-bit neighbour images, FP32 output, the operator itself
+    set->bytes += 2.0 * xb * yb * nk + 4.0 * xb * yb + (double)v.nchunks * kTcM * kTcK * 2;
+    set->fma += (double)v.nchunks * kTcM * kTcK * yb;
+  }
+  chunk_first[n] = chunks;
+  set->total_chunks = chunks;
+  const size_t chunk_elems = (size_t)kTcM * kTcK;
+  MF_TRY(set->op16.alloc(2 * chunk_elems * std::max(chunks, 1)));
+  MF_TRY(set->xt.alloc(sizeof(TcXTile) * xts.size()));
+  MF_TRY(set->segs.alloc(sizeof(TcSeg) * std::max<size_t>(segs.size(), 1)));
+  MF_TRY(set->colvalid.alloc(sizeof(int) * (size_t)n * xb));
+  DevBuf d_segidx;
+  MF_TRY(d_segidx.alloc(sizeof(int) * segidx.size()));
+  MF_CHECK_CUDA(cudaMemcpyAsync(set->xt.p, xts.data(), sizeof(TcXTile) * xts.size(),
+                                cudaMemcpyHostToDevice, st));
+  if (!segs.empty())
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->segs.p, segs.data(), sizeof(TcSeg) * segs.size(),
+                                  cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_segidx.p, segidx.data(), sizeof(int) * segidx.size(),
+                                cudaMemcpyHostToDevice, st));
+  // pass 2 in groups of tilts whose FP32 staging fits in a bounded buffer
+  const size_t stage_cap = (size_t)64 << 20;  // floats (256 MB)
+  size_t max_one = 0;
+  for (int i = 0; i < n; ++i)
+    max_one = std::max(max_one, (size_t)(chunk_first[i + 1] - chunk_first[i]) * chunk_elems);
+  DevBuf stagebuf, d_fg;
+  MF_TRY(stagebuf.alloc(sizeof(float) * std::max(std::min(stage_cap, (size_t)chunks * chunk_elems),
+                                                  std::max<size_t>(max_one, 1))));
+  MF_TRY(d_fg.alloc(sizeof(TcFillGeom) * n));
+  std::vector<TcFillGeom> fg(n);
+  int nkmax = 0;
+  for (int i = 0; i < n; ++i) {
+    fg[i].nk = geoms[i].nk;
+    fg[i].ray_len = geoms[i].ray_len;
+    fg[i].T = geoms[i].thick;
+    fg[i].bp_off = gd[i].bp_off;
+    fg[i].fcos = geoms[i].fcos;
+    fg[i].fsin = geoms[i].fsin;
+    fg[i].cnt_off = i * xb;
+    fg[i].segidx_off = segidx_off[i];
+    fg[i].cv_off = i * xb;
+    fg[i].chunk_base = 0;
+    nkmax = std::max(nkmax, geoms[i].nk);
+  }
+  const size_t cap_elems = stagebuf.bytes / sizeof(float);
+  int g0 = 0;
+  while (g0 < n) {
+    int g1 = g0 + 1;
+    while (g1 < n && (size_t)(chunk_first[g1 + 1] - chunk_first[g0]) * chunk_elems <= cap_elems)
+      ++g1;
+    const size_t elems = (size_t)(chunk_first[g1] - chunk_first[g0]) * chunk_elems;
+    for (int i = g0; i < g1; ++i) fg[i].chunk_base = chunk_first[g0];
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_fg.as<TcFillGeom>() + g0, fg.data() + g0,
+                                  sizeof(TcFillGeom) * (g1 - g0), cudaMemcpyHostToDevice, st));
+    if (elems > 0) MF_CHECK_CUDA(cudaMemsetAsync(stagebuf.p, 0, sizeof(float) * elems, st));
+    k_optc_fill<<<dim3((xb + 127) / 128, nkmax, g1 - g0), 128, 0, st>>>(
+        xb, d_fg.as<TcFillGeom>() + g0, d_bp.as<float>(), d_cnt.as<int>(), d_segidx.as<int>(),
+        set->segs.as<TcSeg>(), stagebuf.as<float>(), set->colvalid.as<int>());
+    c->launches++;
+    MF_CHECK_CUDA(cudaGetLastError());
+    if (elems > 0) {
+      const int blocks = (int)std::min<size_t>((elems + 255) / 256, (size_t)c->sm_count * 16);
+      if (half_kind == MF_PREC_FP16)
+        k_op_to_fp16<<<blocks, 256, 0, st>>>(
+            stagebuf.as<float>(), elems, kTcScale,
+            set->op16.as<__half>() + (size_t)chunk_first[g0] * chunk_elems);
+      else
+        k_op_to_bf16<<<blocks, 256, 0, st>>>(
+            stagebuf.as<float>(), elems, kTcScale,
+            set->op16.as<__nv_bfloat16>() + (size_t)chunk_first[g0] * chunk_elems);
+      c->launches++;
+      MF_CHECK_CUDA(cudaGetLastError());
+    }
+    g0 = g1;
+  }
+  for (int i = 0; i < n; ++i) {
+    TcOpView& v = set->ops[i];
+    v.xt = set->xt.as<TcXTile>() + (size_t)i * ntx;
+    v.segs = set->segs.as<TcSeg>();
+    v.colvalid = set->colvalid.as<int>() + (size_t)i * xb;
+  }
+  MF_TRY(tc_op_map(set));
   // the temporaries are freed when this returns; wait for the kernels using them
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;

@@ -462,7 +462,20 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_CHECK_CUDA(cudaMemcpyAsync(P.d_z0.p, &P.z0, sizeof(float), cudaMemcpyHostToDevice, st));
   P.reproj_bytes = 0;
   P.reproj_fma = 0;
-  if (P.method == 1) {
+  P.prec = s->precision;
+  if (P.prec != MF_PREC_FP32) {
+    P.xpitch = (xb + 7) / 8 * 8;
+    MF_TRY(P.corr16.alloc((size_t)2 * P.xpitch * yb * nz));
+    MF_TRY(P.tflags.alloc(sizeof(int) * (size_t)nz * P.ytiles));
+    MF_TRY(P.d_tcerr.alloc(sizeof(int)));
+    MF_CHECK_CUDA(cudaMemsetAsync(P.d_tcerr.p, 0, sizeof(int), st));
+    P.tc_nb = tc_pick_rows(c, xb, yb);
+    MF_TRY(tc_prepare(c, P.tc_nb));
+    MF_TRY(tc_image_map(P.corr16.p, P.prec, xb, P.xpitch, yb, nz, P.tc_nb, &P.imgmap));
+    MF_TRY(build_reproj_tc_ops(c, P.geom, P.prec, &P.tcops, st));
+    P.reproj_bytes = P.tcops.bytes;
+    P.reproj_fma = P.tcops.fma;
+  } else if (P.method == 1) {
     MF_TRY(build_reproj_ops(c, P.geom, &P.ops, st));
     P.reproj_bytes = P.ops.bytes;
     P.reproj_fma = P.ops.fma;
@@ -504,6 +517,10 @@ static int pa_enqueue(mf_series* s) {
   MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_all, scratch, (cufftComplex*)scratch));
   MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, nz * yb, st));
   MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_all, (cufftComplex*)scratch, corr));
+  const bool tc = P.prec != MF_PREC_FP32;
+  if (tc)
+    MF_TRY(launch_to_half(c, corr, xb, yb, nullptr, 0, nz, P.prec, P.corr16.p, P.xpitch,
+                          P.tflags.as<int>(), st));
   // FitRotCenterZ + RemoveOffsetZ(-1)
   MF_TRY(fit_z0(c, nz, P.zt, s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
                 s->d_rot.as<float>(), P.d_z0.as<float>(), st));
@@ -514,7 +531,13 @@ static int pa_enqueue(mf_series* s) {
     int* rowflags = P.d_rowflags.as<int>() + (size_t)k * P.ytiles;
     float* reproj = P.reproj.as<float>();
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k], st));
-    if (P.method == 1) {
+    if (tc) {
+      MF_TRY(launch_reproject_tc(c, P.tcops, P.tcops.ops[k], P.imgmap, P.tc_nb,
+                                 P.d_tcerr.as<int>(), reproj, st));
+      MF_TRY(launch_reproject_exact_flagged(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k],
+                                            g.i0, g.nk, g.fcos, g.fsin, g.ray_len, g.thick,
+                                            P.tflags.as<int>(), reproj, st));
+    } else if (P.method == 1) {
       MF_TRY(launch_reproject_apply(c, P.ops.ops[k], corr, bpix, rowflags, reproj, st));
       MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
                                     g.nk, g.fcos, g.fsin, g.ray_len, g.thick, rowflags, reproj,
@@ -544,6 +567,9 @@ static int pa_enqueue(mf_series* s) {
     MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_one, scratch, (cufftComplex*)scratch));
     MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, yb, st));
     MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_one, (cufftComplex*)scratch, corr + (size_t)ip * bpix));
+    if (tc)
+      MF_TRY(launch_to_half(c, corr, xb, yb, P.d_order.as<int>() + k, 0, 1, P.prec, P.corr16.p,
+                            P.xpitch, P.tflags.as<int>(), st));
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k + 2], st));
   }
   MF_TRY(max_err(c, P.d_err.as<float>(), P.d_order.as<int>(), n, P.d_maxerr.as<float>(), st));
@@ -596,9 +622,14 @@ int projalign_doit(mf_series* s, float* max_err_out) {
     MF_TRY(pa_enqueue(s));
   }
   float res[2];
+  int tcerr = 0;
   MF_CHECK_CUDA(cudaMemcpyAsync(&res[0], P.d_maxerr.p, sizeof(float), cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(&res[1], P.d_z0.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (P.prec != MF_PREC_FP32)
+    MF_CHECK_CUDA(cudaMemcpyAsync(&tcerr, P.d_tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   MF_TRY(s->download_shifts());
+  if (tcerr != 0)
+    return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", tcerr);
   P.z0 = res[1];
   if (c->profiling && (int)P.events.size() >= 3 * n) {
     for (int k = 0; k < n; ++k) {

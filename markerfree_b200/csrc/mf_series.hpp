@@ -44,6 +44,15 @@ struct ProjAlignState {
   std::vector<cudaEvent_t> events;  // 3 per held-out tilt when profiling
   bool use_graph = true;
   int method = 1;  // 1: banded operator with exact fallback; 0: exact gather only
+  // FP16/BF16 modes: tensor-core apply of the operator to a 16-bit copy of the
+  // corrected stack, exact FP32 fallback for row tiles the copy flags.
+  int prec = MF_PREC_FP32;
+  TcOpSet tcops;
+  DevBuf corr16;    // nz x yb x xpitch 16-bit values
+  DevBuf tflags;    // nz x ytiles
+  DevBuf d_tcerr;   // pipeline error word of the tensor-core kernel
+  TmaDesc imgmap;
+  int tc_nb = 256, xpitch = 0;
   ~ProjAlignState();
 };
 
