@@ -33,6 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+PRECISIONS = {"fp32": 0, "bf16": 1, "fp16": 2}
 
 
 def peaks():
@@ -209,7 +210,9 @@ def run_ours(args):
     d_raw = torch.from_numpy(s.stack).to(f"cuda:{dev}")
     d_out = torch.empty((nz, yo, xo), dtype=torch.float32, device=f"cuda:{dev}")
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
-    kw = dict(offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=s.thickness, out_bin=1, nproj=10)
+    prec = PRECISIONS[args.precision]
+    kw = dict(offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=s.thickness, out_bin=1, nproj=10,
+              precision=prec)
 
     def barrier():
         if pg is not None:
@@ -275,7 +278,9 @@ def run_ours(args):
     t_launch = st["reproj_ms"] / launches_rep / 1e3
     bytes_launch = st["reproj_bytes"] / launches_rep
     achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
-    roof = {"kernel": "k_op_apply (+ sentinel fallback check), one launch per held-out tilt",
+    kname = ("k_op_apply (FP32 banded operator, sentinel fallback check)" if prec == 0 else
+             "k_reproject_tc (tcgen05, 16-bit operands, FP32 accumulation in TMEM)")
+    roof = {"kernel": kname + ", one launch per held-out tilt",
             "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "peak_source": src,
             "traffic": None,
@@ -291,7 +296,8 @@ def run_ours(args):
         roof["traffic"] = tr.get("bytes_per_launch_full_scale")
     line = {"metric": "series/min (2k^2, 61 tilts)", "value": value, "unit": "series/min",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == 0 else f"{args.precision} operands, f32 accumulation",
             "data": "synthetic (seeded phantom series, BASELINE shapes)",
             "config": workload_config(s, args.scale),
             "e2e": {"value": e2e_value, "unit": "series/min",
@@ -330,7 +336,8 @@ def run_kernel_case(args):
     out = torch.empty((ny, nx), device="cuda", dtype=torch.float32)
     for _ in range(args.steps):
         if args.kernel_case == "reproject":
-            mf.dev_reproject(ctx, corr, nx, ny, nz, ang, ip, i0, i1, s.thickness, 1, out)
+            mf.dev_reproject(ctx, corr, nx, ny, nz, ang, ip, i0, i1, s.thickness,
+                             args.kernel_method, out)
         else:
             mf.dev_measure_shift(ctx, out, corr[ip], nx, ny)
     ctx.sync()
@@ -348,6 +355,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests only)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--precision", default="fp32", choices=list(PRECISIONS),
+                    help="re-projection operands (fp32 = the reference's arithmetic)")
+    ap.add_argument("--kernel-method", type=int, default=1,
+                    help="re-projection method of --kernel-case reproject (1 FP32, 2 FP16, 3 BF16)")
     args = ap.parse_args()
     if args.kernel_case:
         return run_kernel_case(args)

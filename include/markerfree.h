@@ -119,22 +119,22 @@ MF_API int mf_series_set_param(mf_series* s, const mf_align_param* p);
 MF_API int mf_series_get_param(mf_series* s, mf_align_param* p);
 
 /* ---- stages --------------------------------------------------------------- */
-/* Transform::Setup + DoIt (Markerfree/src/method/Transform.cpp:55-128): stretch
+/* Transform::Setup + DoIt (Markerfree/src/method/Transform.cpp:24-157): stretch
  * cross-correlation of every tilt against its neighbour nearer zero tilt, shifts
  * accumulated outward.  The series keeps the Transform state between calls. */
 MF_API int mf_transform_doit(mf_series* s, float* max_err);
-/* CalcTIltAxis::DoIt (Markerfree/src/method/Rotate.cu:333-378): common-line search
+/* CalcTIltAxis::DoIt (Markerfree/src/method/Rotate.cu:292-337): common-line search
  * over `num` candidate axes spanning `range` degrees; sets rotate[] for all tilts. */
 MF_API int mf_tilt_axis(mf_series* s, float range, int num, float* axis_out);
 /* FindOffset::DoIt (Markerfree/src/method/FindOffset.cu:85-96): adds the best of
  * 31 one-degree tilt-angle offsets to param.angle_offset. */
 MF_API int mf_find_offset(mf_series* s, float* offset_out);
-/* ProjAlign::Setup (Markerfree/src/method/ProjAlign.cpp:126-203). */
+/* ProjAlign::Setup (Markerfree/src/method/ProjAlign.cpp:48-125). */
 MF_API int mf_projalign_setup(mf_series* s, float zshift, int align_z, int nproj);
-/* ProjAlign::DoIt (Markerfree/src/method/ProjAlign.cpp:205-257): one projection-
+/* ProjAlign::DoIt (Markerfree/src/method/ProjAlign.cpp:127-179): one projection-
  * matching pass over all tilts; returns the largest measured shift (px). */
 MF_API int mf_projalign_doit(mf_series* s, float* max_err);
-/* Rotation-centre z of the last pass (ProjAlign.cpp:537-564). */
+/* Rotation-centre z of the last pass (ProjAlign.cpp:459-486). */
 MF_API int mf_projalign_z0(mf_series* s, float* z0);
 /* Process::mCoarseAlign (Markerfree/src/main/Process.cpp:238-270); applies the
  * offset to the series' angles as the reference does. */
@@ -184,10 +184,10 @@ MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
 MF_API int mf_dev_correct_proj(mf_context* ctx, const float* d_proj, int nx, int ny,
                                float shift_x, float shift_y, float tilt_axis, int only_shift,
                                int bin, int random_fill, int rweight, float* d_out);
-/* CalcReprojFBP::FindProjRange (Markerfree/src/method/CalcReproj.cu:281-334). */
+/* CalcReprojFBP::FindProjRange (Markerfree/src/method/CalcReproj.cu:206-259). */
 MF_API int mf_find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
                               int nproj, int* range2);
-/* CalcReprojFBP::DoIt (CalcReproj.cu:255-311): back-project tilts [istart, iend] of
+/* CalcReprojFBP::DoIt (CalcReproj.cu:180-311): back-project tilts [istart, iend] of
  * the corrected stack d_corr (nz x yb x xb) into a 2*xb x thickness slab per row
  * and re-project it at angles[iproj] into d_out (yb x xb).  method 0 = exact
  * per-sample gather, 1 = banded operator in FP32 (the FP32 production path),

@@ -86,7 +86,7 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   lines[((size_t)z * num + b) * (L + 2) + y] = (cnt == 0) ? kSentinel : __fdiv_rn(sum, (float)cnt);
 }
 
-// GCalcMean + GRemoveMean (Rotate.cu:138-198) for one line per block.
+// GCalcMean + GRemoveMean (Rotate.cu:97-157) for one line per block.
 __global__ void k_line_prep(float* __restrict__ lines, int L) {
   __shared__ double s_sum[256];
   __shared__ int s_cnt[256];
@@ -141,7 +141,7 @@ __global__ void k_axis_sum(const cufftComplex* __restrict__ spec, int nz, int nu
   sum[(size_t)b * cmp + k] = make_cuComplex(re, im);
 }
 
-// GConv (1-D, B = 10) + GSum (Rotate.cu:220-292) for (candidate b, tilt z).
+// GConv (1-D, B = 10) + GSum (Rotate.cu:179-251) for (candidate b, tilt z).
 __global__ void k_axis_cc(const cufftComplex* __restrict__ spec,
                           const cufftComplex* __restrict__ sum, int nz, int num, int cmp,
                           float* __restrict__ cc_out) {

@@ -775,7 +775,7 @@ int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr
 }
 
 // ---------------------------------------------------------------------------
-// CalcReproj.cu:281-334
+// CalcReproj.cu:206-259
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
                      int nproj, int* range) {
   const float ref_range = 20.5f, ref_stretch = 1.2f;

@@ -125,7 +125,7 @@ int mf_series::download_shifts() {
 namespace mf {
 
 // ---------------------------------------------------------------------------
-// Transform::DoIt (Transform.cpp:91-188), all tilt pairs batched.
+// Transform::DoIt + Measure (Transform.cpp:60-97), all tilt pairs batched.
 int transform_doit(mf_series* s, float* max_err_out) {
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
@@ -215,7 +215,7 @@ int transform_doit(mf_series* s, float* max_err_out) {
       if (e > maxerr) maxerr = e;
     }
   }
-  // UpdateShift (Transform.cpp:130-188)
+  // UpdateShift + UnStretch (Transform.cpp:99-157)
   int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
   for (int i = 0; i < nz; ++i) {
     T.pshx[i] -= T.pshx[zt];
@@ -254,7 +254,7 @@ int transform_doit(mf_series* s, float* max_err_out) {
 }
 
 // ---------------------------------------------------------------------------
-// CalcTIltAxis::DoIt (Rotate.cu:333-415, 509-528)
+// CalcTIltAxis::DoIt + CLsetup (Rotate.cu:292-374)
 int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
   if (num < 2) return set_error(MF_ERR_ARG, "tilt axis: need at least 2 candidates");
   Context* c = &s->ctx->c;
@@ -353,7 +353,7 @@ int find_offset(mf_series* s, float* offset_out) {
       float f[6];
       for (int k = 0; k < 6; ++k) f[k] = (float)mom[(size_t)6 * p + k];
       for (int k = 0; k < 5; ++k) f[k] /= f[5];
-      // the reference subtracts the mean itself, not its square (FindOffset.cu:214-215)
+      // the reference subtracts the mean itself, not its square (FindOffset.cu:222-223)
       double s1 = f[2] - f[0], s2 = f[3] - f[1];
       double cc = f[4] - f[0] * f[1];
       if (s1 < 0) s1 = 0;
@@ -380,7 +380,7 @@ int find_offset(mf_series* s, float* offset_out) {
 }
 
 // ---------------------------------------------------------------------------
-// ProjAlign::Setup / Setsize (ProjAlign.cpp:126-203) plus the precomputation
+// ProjAlign::Setup / Setsize (ProjAlign.cpp:48-125) plus the precomputation
 // that the reference repeats for every pass: processing order, neighbour
 // ranges and the re-projection operators.
 int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
@@ -412,7 +412,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_TRY(P.ccbuf.alloc(sizeof(float) * ppix * 2));
   MF_TRY(P.part.alloc(sizeof(double2) * moment_parts(yb) * 2 + sizeof(float2) * kPeakParts));
   MF_TRY(P.stats.alloc(sizeof(float2) * 2));
-  // outward order (ProjAlign.cpp:229-254) and neighbour ranges
+  // outward order (ProjAlign.cpp:151-176) and neighbour ranges
   P.zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
   std::vector<unsigned char> skip(nz, 1);
   skip[P.zt] = 0;
@@ -495,7 +495,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   return MF_OK;
 }
 
-// Queue one projection-matching pass (ProjAlign::DoItBin, ProjAlign.cpp:211-257).
+// Queue one projection-matching pass (ProjAlign::DoItBin, ProjAlign.cpp:133-179).
 static int pa_enqueue(mf_series* s) {
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;

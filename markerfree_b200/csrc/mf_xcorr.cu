@@ -276,7 +276,7 @@ __device__ __forceinline__ void pa_window_peak(int bi, int stride, int xb, int y
   *py = bi / stride;
 }
 
-// ProjAlign.cpp:427-453: parabolic sub-pixel fit (FP64) around the integer peak.
+// ProjAlign.cpp:350-372: parabolic sub-pixel fit (FP64) around the integer peak.
 __device__ void pa_fit(const float* m, int stride, int px, int py, double* dx, double* dy,
                        double* peak) {
   int ic = py * stride + px;
@@ -305,7 +305,7 @@ __device__ __forceinline__ void rot_shift(float in0, float in1, float angle_deg,
   *o1 = sy;
 }
 
-// ProjAlign.cpp:631-639
+// CalcZInducedShift (ProjAlign.cpp:553-561)
 __device__ __forceinline__ void z_induced(float z0, float angle, float rot, float* s0,
                                           float* s1) {
   *s0 = 0.0f;
@@ -316,7 +316,7 @@ __device__ __forceinline__ void z_induced(float z0, float angle, float rot, floa
   rot_shift(a, 0.0f, rot, s0, s1);
 }
 
-// Final peak + ClacAlignProj update (ProjAlign.cpp:259-319) for held-out tilt ip.
+// Final peak + ClacAlignProj update (ProjAlign.cpp:181-241) for held-out tilt ip.
 __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int xb, int yb,
                                  const float2* __restrict__ part, int nparts, int ip, int nx,
                                  int ny, const float* __restrict__ angles, float* __restrict__ sx,
@@ -449,7 +449,7 @@ int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w
 }
 
 // ---------------------------------------------------------------------------
-// FitRotCenterZ + RemoveOffsetZ(-1) (ProjAlign.cpp:537-579, 641-657); the
+// FitRotCenterZ + RemoveOffsetZ(-1) (ProjAlign.cpp:459-501, 553-579); the
 // reference's uninitialised accumulator dA is taken as 0.
 __global__ void k_fit_z0(int nz, int zt, const float* __restrict__ angles, float* sx, float* sy,
                          const float* __restrict__ rot, float* z0p) {

@@ -181,7 +181,7 @@ void correct_proj(const float* proj, int nx, int ny, float shift_x, float shift_
 }
 
 // ---------------------------------------------------------------------------
-// CalcReproj.cu:281-334 (FindProjRange)
+// CalcReproj.cu:206-259 (FindProjRange)
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj, int nproj,
                      int* range) {
   const float ref_range = 20.5f, ref_stretch = 1.2f;
@@ -379,7 +379,7 @@ std::vector<cd> fwd2d(const float* img, int nx, int ny, int stride, bool norm) {
 }
 
 // CalcCC.cu:95-135 (GConv, GWiener, GCenterOrigin) then the C2R of
-// ProjAlign.cpp:392-401 / CalcCC.cu:366-379.  Returns the real map (ny x nx).
+// ProjAlign.cpp:314-323 / CalcCC.cu:366-379.  Returns the real map (ny x nx).
 std::vector<float> xcorr_map(const std::vector<cd>& ref, std::vector<cd> img, int nx, int ny,
                              float bfactor) {
   int cx = nx / 2 + 1;
@@ -414,7 +414,7 @@ std::vector<float> xcorr_map(const std::vector<cd>& ref, std::vector<cd> img, in
   return out;
 }
 
-// ProjAlign.cpp:403-453 (PAFindPeak); map is dense ny x nx.
+// ProjAlign.cpp:325-375 (PAFindPeak); map is dense ny x nx.
 float pa_find_peak(const std::vector<float>& m, int nx, int ny, float* shift) {
   float fpeak = (float)-1e20;
   int px = 0, py = 0;
@@ -445,7 +445,7 @@ float pa_find_peak(const std::vector<float>& m, int nx, int ny, float* shift) {
   return (float)(a * dx * dx + b * dx + c * dy * dy + d * dy + m[ic]);
 }
 
-// ProjAlign.cpp:321-390 (MeaAlignProj with PANorm / GetCentral)
+// ProjAlign.cpp:243-312 (MeaAlignProj with PANorm / GetCentral)
 float measure_shift(const float* reproj, const float* proj, int xb, int yb, float* shift) {
   int pad = (xb / 2 + 1) * 2;
   auto panorm = [&](const float* img) {
@@ -465,7 +465,7 @@ float measure_shift(const float* reproj, const float* proj, int xb, int yb, floa
   return pa_find_peak(map, xb, yb, shift);
 }
 
-// ProjAlign.cpp:526-535
+// RotShift (ProjAlign.cpp:448-457)
 void rot_shift(const float* in, float angle, float* out) {
   float c = (float)cos(angle * D2R), s = (float)sin(angle * D2R);
   float sx = in[0] * c - in[1] * s;
@@ -560,7 +560,7 @@ void oc_preprocess(const float* raw, int nx, int ny, int nz, const float* angles
 }
 
 // ---------------------------------------------------------------------------
-// ProjAlign (ProjAlign.cpp:126-657), one instance per mProjAlign call.
+// ProjAlign (ProjAlign.cpp:48-579), one instance per mProjAlign call.
 struct oc_projalign {
   const float* stack;
   int nx, ny, nz;
@@ -581,7 +581,7 @@ static void pa_correct(oc_projalign* pa, int i) {
                pa->corr.data() + (size_t)i * pa->xb * pa->yb);
 }
 
-// ProjAlign.cpp:631-639
+// CalcZInducedShift (ProjAlign.cpp:553-561)
 static void z_induced(oc_projalign* pa, int f, float* s) {
   s[0] = s[1] = 0.0f;
   if (pa->z0 == 0) return;
@@ -621,11 +621,11 @@ void oc_projalign_measured(const oc_projalign* pa, float* xy) {
 int oc_projalign_bin(const oc_projalign* pa) { return pa->bin; }
 void oc_projalign_destroy(oc_projalign* pa) { delete pa; }
 
-// ProjAlign.cpp:211-257 (DoItBin) + 259-319 (ClacAlignProj) + 537-579.
+// ProjAlign.cpp:133-179 (DoItBin) + 181-241 (ClacAlignProj) + 459-501.
 float oc_projalign_doit(oc_projalign* pa) {
   int nz = pa->nz;
   for (int i = 0; i < nz; ++i) pa_correct(pa, i);
-  // FitRotCenterZ (ProjAlign.cpp:537-564; the uninitialised dA is taken as 0)
+  // FitRotCenterZ (ProjAlign.cpp:459-486; the uninitialised dA is taken as 0)
   {
     int zt = frame_idx_from_tilt(nz, pa->angles.data(), 0.0f);
     float s0[2] = {pa->param->shift_x[zt], pa->param->shift_y[zt]};
@@ -641,7 +641,7 @@ float oc_projalign_doit(oc_projalign* pa) {
     }
     pa->z0 = (float)(dA / (dB + 1e-30));
   }
-  // RemoveOffsetZ(-1) (ProjAlign.cpp:566-579)
+  // RemoveOffsetZ(-1) (ProjAlign.cpp:488-501)
   int zt = frame_idx_from_tilt(nz, pa->angles.data(), 0.0f);
   if (pa->z0 != 0) {
     for (int i = 0; i < nz; ++i) {
@@ -695,7 +695,7 @@ float oc_projalign_doit(oc_projalign* pa) {
 }
 
 // ---------------------------------------------------------------------------
-// Rotate.cu:333-613 (CalcTIltAxis::DoIt)
+// Rotate.cu:292-572 (CalcTIltAxis::DoIt)
 float oc_tilt_axis_scores(const float* stack, int nx, int ny, int nz, const float* angles,
                           oc_param* param, float range, int num, float* scores_out) {
   int zt = frame_idx_from_tilt(nz, angles, 0.0f);
@@ -926,7 +926,7 @@ static void stretch(const float* in, int gw, int h, int stride, const float* m, 
     }
 }
 
-// Transform (Transform.cpp:55-188)
+// Transform (Transform.cpp:24-157)
 struct oc_transform {
   const float* stack;
   int nx, ny, nz, bin, xb, yb;
@@ -1061,7 +1061,7 @@ float oc_transform_doit(oc_transform* t) {
     float e = (float)sqrt(t->pshx[z] * t->pshx[z] + t->pshy[z] * t->pshy[z]);
     if (e > maxerr) maxerr = e;
   }
-  // UpdateShift (Transform.cpp:130-162)
+  // UpdateShift (Transform.cpp:99-131)
   int zt = frame_idx_from_tilt(nz, t->angles.data(), 0.0f);
   for (int i = 0; i < nz; ++i) {
     // subtracts the live zero-tilt entry, which is itself zeroed at i == zt
@@ -1133,7 +1133,7 @@ float oc_find_offset(const float* stack, int nx, int ny, int nz, const float* an
       float f[6];
       for (int k = 0; k < 6; ++k) f[k] = (float)v[k];
       for (int k = 0; k < 5; ++k) f[k] /= f[5];
-      // the reference subtracts the mean, not its square (FindOffset.cu:214-215)
+      // the reference subtracts the mean, not its square (FindOffset.cu:222-223)
       double s1 = f[2] - f[0], s2 = f[3] - f[1];
       double cc = f[4] - f[0] * f[1];
       if (s1 < 0) s1 = 0;

@@ -47,7 +47,7 @@ void oc_find_proj_range(const float* angles, int nz, const unsigned char* skip, 
 void oc_reproject(const float* corr, int xb, int yb, int nz, const float* angles, int iproj,
                   int istart, int iend, int thickness, float* out);
 
-// ---- CC measurement (Markerfree/src/method/ProjAlign.cpp:321-453) ----
+// ---- CC measurement (Markerfree/src/method/ProjAlign.cpp:243-375) ----
 // Returns the shift (binned px) of proj against reproj; peak value in *peak.
 void oc_measure_shift(const float* reproj, const float* proj, int xb, int yb, float* shift2,
                       float* peak);
@@ -64,7 +64,7 @@ void oc_projalign_measured(const oc_projalign* pa, float* xy);
 int oc_projalign_bin(const oc_projalign* pa);
 void oc_projalign_destroy(oc_projalign* pa);
 
-// ---- tilt axis (Markerfree/src/method/Rotate.cu:333-613) ----
+// ---- tilt axis (Markerfree/src/method/Rotate.cu:292-572) ----
 float oc_tilt_axis(const float* stack, int nx, int ny, int nz, const float* angles,
                    oc_param* param, float range, int num);
 // Same, also returning the `num` candidate scores.
