@@ -62,7 +62,7 @@ def neighbours(ang, iproj, nproj=10):
 
 @pytest.mark.parametrize("rows", [64, 128, 256])
 @pytest.mark.parametrize("method", [2, 3])
-@pytest.mark.parametrize("iproj,thick", [(10, 30), (2, 40), (13, 8)])
+@pytest.mark.parametrize("iproj,thick", [(10, 30), (2, 40), (13, 12)])
 def test_tc_reproject_matches_oracle(ctx, mflib, tall, method, rows, iproj, thick):
     import torch
     s, corr = tall
