@@ -196,7 +196,23 @@ MF_API int mf_find_proj_range(const float* angles, int nz, const unsigned char* 
 MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb, int nz,
                             const float* angles, int iproj, int istart, int iend, int thickness,
                             int method, float* d_out);
-/* ProjAlign::MeaAlignProj + PAFindPeak (ProjAlign.cpp:321-453): shift (binned px)
+/* The exact re-projection of mf_dev_reproject (method 0) for callers that cannot
+ * allocate device memory.  It has no counterpart in the reference.  Hosts such as
+ * acquisition programs that reserve the GPU's memory for their own buffers, or
+ * real-time loops in which a cudaMalloc/cudaFree could synchronise the device,
+ * cannot let the library grow scratch buffers; this entry point allocates
+ * nothing.  Its per-neighbour table lives in a static device array of at most
+ * 256 neighbour tilts (3 KB, held by every GPU that loads the library until the
+ * process exits); more neighbours are rejected with MF_ERR_ARG.  The first call
+ * on a device looks the array's address up, so make that first call before any
+ * stream capture on the device.  All calls share the array: calls whose kernels
+ * overlap on the GPU (e.g. on two streams) race.  `stream` is a cudaStream_t
+ * (NULL = the legacy default stream) of the current device; the call returns
+ * after queuing the work. */
+MF_API int mf_dev_reproject_noalloc(void* stream, const float* d_corr, int xb, int yb, int nz,
+                                    const float* angles, int iproj, int istart, int iend,
+                                    int thickness, float* d_out);
+/* ProjAlign::MeaAlignProj + PAFindPeak (ProjAlign.cpp:243-375): shift (binned px)
  * of d_proj against d_reproj, both yb x xb. */
 MF_API int mf_dev_measure_shift(mf_context* ctx, const float* d_reproj, const float* d_proj,
                                 int xb, int yb, float* shift2, float* peak);

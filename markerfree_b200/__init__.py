@@ -105,6 +105,10 @@ SIGNATURES = [
                                         ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p]),
+    ("mf_dev_reproject_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_void_p]),
     ("mf_dev_measure_shift", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int, ctypes.c_int, _f32p, _c_float_p]),
     ("mf_mrc_info", ctypes.c_int, [ctypes.c_char_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
