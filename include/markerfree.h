@@ -177,6 +177,34 @@ MF_API void* mf_context_stream(mf_context* ctx);
  * set up (mf_projalign_setup) or a single re-projection is queued. */
 MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
 
+/* ---- groups: many series in lockstep ---------------------------------------
+ * Not in the reference, which aligns one series per process.  A group runs the
+ * projection-matching pass (ProjAlign::DoIt, Markerfree/src/method/ProjAlign.cpp:
+ * 127-179) of up to 32 series of one context, shape and precision together: each
+ * stage of the pass is one launch over all of them, and a pass is one CUDA graph.
+ * Per-series results equal those of aligning each series alone.  Destroy a group
+ * before its series. */
+typedef struct mf_group mf_group;
+/* ProjAlign::Setup for every series (their current angles and parameters). */
+MF_API int mf_group_create(mf_series* const* series, int n, float zshift, int align_z, int nproj,
+                           mf_group** out);
+MF_API void mf_group_destroy(mf_group* g);
+/* One pass over the series with active[i] != 0; max_err[i] gets the largest
+ * measured shift of each active series (the reference's DoIt return value). */
+MF_API int mf_group_doit(mf_group* g, const int* active, float* max_err);
+/* Process::mProjAlign + ProjAlignOnce (Markerfree/src/main/Process.cpp:272-319) for
+ * every series: shifts reset, then the reference's schedule with each series'
+ * own break rule; passes[i] (optional) gets each series' pass count. */
+MF_API int mf_group_proj_align(mf_group* g, int* passes);
+/* Rotation-centre z of every series after the last pass. */
+MF_API int mf_group_z0(mf_group* g, float* z0);
+/* mf_align_device for n series of one shape (raw stacks and outputs in device
+ * memory): coarse alignment per series, projection matching in groups.
+ * params[i] must hold nz-entry arrays; d_out may be NULL (no output stack). */
+MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_raw, int nx, int ny,
+                                int nz, const float* const* file_angles, const mf_options* opt,
+                                mf_align_param* params, float* const* d_out, int* passes);
+
 /* ---- single kernels on caller-owned device memory (same stream semantics:
  * the call is ordered on the context stream and returns after queuing). ------ */
 /* CorrTomoStack::mCorrectProj (Markerfree/src/method/CorrStack.cu:370-397) for one

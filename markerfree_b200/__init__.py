@@ -95,6 +95,20 @@ SIGNATURES = [
                                               ctypes.POINTER(ctypes.c_double)]),
     ("mf_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("mf_context_set_tc_rows", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("mf_group_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                       ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_group_destroy", None, [ctypes.c_void_p]),
+    ("mf_group_doit", ctypes.c_int, [ctypes.c_void_p, _i32p, _f32p]),
+    ("mf_group_proj_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("mf_group_z0", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_align_many_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p),
+                                            ctypes.POINTER(OptionsC),
+                                            ctypes.POINTER(AlignParamC),
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -364,6 +378,66 @@ def align_host_ptr(ctx: Context, raw_ptr: int, nx, ny, nz, file_angles, out_ptr:
              ctypes.byref(c), ctypes.c_void_p(out_ptr), ctypes.byref(n)))
     p.angle_offset = c.angle_offset
     return p, n.value
+
+
+class Group:
+    """Projection matching of up to 32 series of one shape in lockstep."""
+
+    def __init__(self, series, zshift=0.0, align_z=600, nproj=10):
+        arr = (ctypes.c_void_p * len(series))(*[s.h.value for s in series])
+        h = ctypes.c_void_p()
+        _check(lib().mf_group_create(arr, len(series), zshift, align_z, nproj, ctypes.byref(h)))
+        self.h = h
+        self.series = list(series)
+
+    def doit(self, active=None) -> np.ndarray:
+        n = len(self.series)
+        act = np.ones(n, np.int32) if active is None else np.ascontiguousarray(active, np.int32)
+        err = np.zeros(n, np.float32)
+        _check(lib().mf_group_doit(self.h, act, err))
+        return err
+
+    def proj_align(self) -> np.ndarray:
+        passes = np.zeros(len(self.series), np.int32)
+        _check(lib().mf_group_proj_align(self.h, passes.ctypes.data_as(ctypes.c_void_p)))
+        return passes
+
+    @property
+    def z0(self) -> np.ndarray:
+        z = np.zeros(len(self.series), np.float32)
+        _check(lib().mf_group_z0(self.h, z))
+        return z
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.mf_group_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def align_many_device(ctx: Context, d_raws, nx, ny, nz, file_angles, d_outs=None, offset=0.0,
+                      pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10,
+                      precision=PREC_FP32):
+    """mf_align_many_device: n raw stacks (device tensors or addresses) of one shape.
+    Returns (list of Param, passes array)."""
+    n = len(d_raws)
+    raws = (ctypes.c_void_p * n)(*[_ptr(d).value for d in d_raws])
+    angs = [_f32(a)[:nz] for a in file_angles]
+    angp = (ctypes.c_void_p * n)(*[a.ctypes.data for a in angs])
+    params = [Param(nz) for _ in range(n)]
+    cs = (AlignParamC * n)(*[p.c() for p in params])
+    outs = None
+    if d_outs is not None:
+        outs = (ctypes.c_void_p * n)(*[_ptr(d).value for d in d_outs])
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
+    passes = np.zeros(n, np.int32)
+    _check(lib().mf_align_many_device(ctx.h, n, raws, nx, ny, nz, angp, ctypes.byref(o), cs, outs,
+                                      passes.ctypes.data_as(ctypes.c_void_p)))
+    for p, c in zip(params, cs):
+        p.angle_offset = c.angle_offset
+    return params, passes
 
 
 def find_proj_range(angles, skip, iproj, nproj):

@@ -419,10 +419,11 @@ MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb
     std::vector<ReprojGeom> gs(1, g);
     MF_TRY(build_reproj_tc_ops(&ctx->c, gs, prec, &set, st));
     MF_TRY(S->c.alloc((size_t)2 * xpitch * yb * nz));
-    MF_TRY(S->d.alloc(sizeof(int) * ((size_t)nz * ytiles + 1)));
+    const size_t nflags = (size_t)nz * ytiles * kFlagParts;
+    MF_TRY(S->d.alloc(sizeof(int) * (nflags + 1)));
     int* tflags = S->d.as<int>();
-    int* err = tflags + (size_t)nz * ytiles;
-    MF_CHECK_CUDA(cudaMemsetAsync(S->d.p, 0, sizeof(int) * ((size_t)nz * ytiles + 1), st));
+    int* err = tflags + nflags;
+    MF_CHECK_CUDA(cudaMemsetAsync(S->d.p, 0, sizeof(int) * (nflags + 1), st));
     MF_TRY(launch_to_half(&ctx->c, d_corr, xb, yb, nullptr, istart, iend - istart + 1, prec,
                           S->c.p, xpitch, tflags, st));
     TmaDesc imgmap;

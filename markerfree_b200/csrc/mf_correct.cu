@@ -104,6 +104,49 @@ __global__ void k_correct_bin(CorrArgs a) {
   a.out[(size_t)j * a.out_tilt_stride + (size_t)by * a.out_row_stride + bx] = res;
 }
 
+// k_correct_bin for a group of series: job j is tilt (j % nz) of series j / nz,
+// or, with a step table, the held-out tilt of series j at that step.
+__global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int binx, int biny) {
+  __shared__ float s_cs, s_sn, s_sx, s_sy;
+  const int j = blockIdx.z;
+  const int b = g.steps ? j : j / g.nz;
+  if (g.active && g.active[b] == 0) return;
+  const GroupSeriesDev& S = g.ser[b];
+  const int z = g.steps ? g.steps[b].ip : j % g.nz;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const float axis = (float)((double)S.rot[z] * kD2R);  // CorrStack.cu:376-378
+    s_cs = (float)cos((double)axis);
+    s_sn = (float)sin((double)axis);
+    s_sx = S.sx[z];
+    s_sy = S.sy[z];
+  }
+  __syncthreads();
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= xb || by >= yb) return;
+  const float* img = S.stack + (size_t)z * g.nx * g.ny;
+  float res;
+  if (g.bin == 1) {
+    res = corr_pixel(img, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
+  } else {
+    float sum = 0.0f;
+    bool bad = false;
+    for (int iy = 0; iy < biny && !bad; ++iy) {
+      for (int ix = 0; ix < binx; ++ix) {
+        float v = corr_pixel(img, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx, s_sy,
+                             s_cs, s_sn, g.random_fill);
+        if (v < -1e10f) {
+          bad = true;
+          break;
+        }
+        sum = __fadd_rn(sum, v);
+      }
+    }
+    res = bad ? kSentinel : sum;
+  }
+  g.out[(size_t)j * g.out_tilt_stride + (size_t)by * g.out_row_stride + bx] = res;
+}
+
 static void fill_sizes(CorrArgs* a, int nx, int ny, int bin) {
   int pad_x = (nx / 2 + 1) * 2;
   a->out_x = (pad_x / 2 - 1) * 2;  // CorrStack.cu:204
@@ -135,6 +178,16 @@ int launch_correct_bin(Context* c, const float* stack, int nx, int ny, const int
   a.out_tilt_stride = out_tilt_stride;
   dim3 blk(32, 8), grd((a.xb + 31) / 32, (a.yb + 7) / 8, ntilts);
   k_correct_bin<<<grd, blk, 0, st>>>(a);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int launch_correct_group(Context* c, const GroupCorrArgs& g, int njobs, cudaStream_t st) {
+  CorrArgs a{};
+  fill_sizes(&a, g.nx, g.ny, g.bin);
+  dim3 blk(64, 4), grd((a.xb + 63) / 64, (a.yb + 3) / 4, njobs);
+  k_correct_group<<<grd, blk, 0, st>>>(g, a.out_x, a.xb, a.yb, a.binx, a.biny);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

@@ -240,6 +240,71 @@ int launch_reproject_exact_flagged(Context* c, const float* corr, int xb, int yb
                                    int ray_len, int thick, const int* tflags, float* out,
                                    cudaStream_t st);
 
+// ---- multi-series (group) execution ------------------------------------------
+// A group runs the projection-matching pass of up to kMaxGroup series of one
+// shape in lockstep: every stage is one launch over all series of the group
+// (the i-th held-out tilt of every series together).  Per-series state lives in
+// device tables; a per-series `active` flag lets the captured pass skip series
+// that have already left the current ProjAlignOnce loop.
+constexpr int kMaxGroup = 32;
+constexpr int kFlagParts = 8;  // column parts of a 16-bit copy's per-tile flags
+
+struct GroupSeriesDev {
+  const float* stack;  // pre-processed stack (nz x ny x nx)
+  float* sx;
+  float* sy;
+  const float* rot;
+  const float* angles;
+  float* z0;
+  float* err;    // nz: |shift| of the last measurement per tilt
+  float* meas;   // 2 * nz: binned shift of the last measurement per tilt
+  float* corr;   // corrected stack of this series (nz x yb x xb)
+  const int* order;  // outward processing order (nz - 1 entries)
+  int zt, pad0;
+};
+struct GroupStepDev {  // the held-out tilt of one series at one step of the pass
+  int ip, i0, nk, ray_len, thick, bp_off;  // bp_off: float offset in the bp table
+  float fcos, fsin;
+};
+struct GroupCorrArgs {
+  const GroupSeriesDev* ser;
+  const GroupStepDev* steps;  // null: all tilts of every series (job = b * nz + tilt)
+  const int* active;          // null: all series
+  int nx, ny, nz, bin, random_fill;
+  float* out;
+  int out_row_stride;
+  size_t out_tilt_stride;
+};
+// resample + bin (k_correct_bin) for a group; one output image per job
+int launch_correct_group(Context* c, const GroupCorrArgs& a, int njobs, cudaStream_t st);
+// exact re-projection of the flagged 128-row tiles of every active series at one
+// step; flags: tflags of the 16-bit copies ([b*nz + tilt][ytiles][kFlagParts])
+// when tc, else the FP32 apply's rowflags ([b][ytiles])
+int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                                 const int* active, int nseries, int nz, int xb, int yb,
+                                 const float* d_bp, const int* tflags, const int* rowflags,
+                                 float* out, cudaStream_t st);
+struct ApplyJob {  // one series of a group for the FP32 apply
+  const OpTile* tiles;
+  const int* colvalid;
+  const float* corr;
+  float* out;
+  int* rowflags;
+};
+int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
+                                 const int* active, int njobs, int xb, int yb, int ntiles,
+                                 cudaStream_t st);
+struct TcJob {
+  const TcXTile* xt;
+  const int* colvalid;
+  float* out;
+  int zoff;  // first tilt of this series in the group's 16-bit stack
+  int pad;
+};
+int launch_reproject_tc_group(Context* c, const TcOpSet& set, const TcJob* jobs, int njobs,
+                              const int* active, int xb, int yb, const TmaDesc& imgmap, int nb,
+                              int* d_err, cudaStream_t st);
+
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,
                      int nproj, int* range);
 int frame_idx_from_tilt(int nz, const float* a, float tilt);

@@ -96,6 +96,10 @@ __device__ __forceinline__ int cell_bin(int ix, int iz, int W, int T, float c, f
   return (int)v;
 }
 
+__device__ void exact_rows(const float* __restrict__ corr, int xb, size_t pix,
+                           const float* __restrict__ bp, int i0, int nk, float fcos, float fsin,
+                           int L, int T, int bx, int ya, int yz, float* __restrict__ out);
+
 // ---------------------------------------------------------------------------
 // Exact path: one thread per detector column; a block covers `rows_per_block`
 // image rows.  With row flags (the fallback after the banded apply) a block
@@ -109,15 +113,24 @@ __global__ void k_reproject_exact(const float* __restrict__ corr, int xb, int yb
   if (tflags) {
     // per-tilt flags of the 16-bit copy: recompute the tile if any neighbour's is set
     int any = 0;
-    for (int k = 0; k < nk; ++k) any |= tflags[(size_t)(i0 + k) * gridDim.y + blockIdx.y];
+    for (int k = 0; k < nk; ++k)
+      for (int q = 0; q < kFlagParts; ++q)
+        any |= tflags[((size_t)(i0 + k) * gridDim.y + blockIdx.y) * kFlagParts + q];
     if (!any) return;
   }
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
   if (bx >= xb) return;
+  const int ya = blockIdx.y * rows_per_block, yz = min(yb, ya + rows_per_block);
+  exact_rows(corr, xb, pix, bp, i0, nk, fcos, fsin, L, T, bx, ya, yz, out);
+}
+
+// Rows [ya, yz) of column bx with the reference's per-sample arithmetic.
+__device__ void exact_rows(const float* __restrict__ corr, int xb, size_t pix,
+                           const float* __restrict__ bp, int i0, int nk, float fcos, float fsin,
+                           int L, int T, int bx, int ya, int yz, float* __restrict__ out) {
   const int W = 2 * xb;
   const float cent = __fmul_rn((float)xb, 0.5f);
   const RayStart r = ray_start(bx, xb, W, T, fcos, fsin, L);
-  const int ya = blockIdx.y * rows_per_block, yz = min(yb, ya + rows_per_block);
   for (int y = ya; y < yz; ++y) {
     float sum = 0.0f;
     int cnt = 0;
@@ -153,6 +166,47 @@ int launch_reproject_exact(Context* c, const float* corr, int xb, int yb, size_t
   dim3 blk(128, 1), grd((xb + 127) / 128, (yb + rpb - 1) / rpb);
   k_reproject_exact<<<grd, blk, 0, st>>>(corr, xb, yb, pix, d_bp, i0, nk, fcos, fsin, ray_len,
                                          thick, d_rowflags, nullptr, rpb, out);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Group form: blockIdx.z = series.  A row tile is recomputed when its flags say so
+// (any neighbour's 16-bit tile flag, or the FP32 apply's row flag).
+__global__ void k_reproject_exact_group(const GroupSeriesDev* __restrict__ ser,
+                                        const GroupStepDev* __restrict__ steps,
+                                        const int* __restrict__ active, int nz, int xb, int yb,
+                                        const float* __restrict__ bps,
+                                        const int* __restrict__ tflags,
+                                        const int* __restrict__ rowflags,
+                                        float* __restrict__ out) {
+  const int b = blockIdx.z;
+  if (active && active[b] == 0) return;
+  const GroupStepDev S = steps[b];
+  const int ytiles = gridDim.y;
+  if (tflags) {
+    int any = 0;
+    for (int k = 0; k < S.nk; ++k)
+      for (int q = 0; q < kFlagParts; ++q)
+        any |= tflags[((size_t)(b * nz + S.i0 + k) * ytiles + blockIdx.y) * kFlagParts + q];
+    if (!any) return;
+  } else if (rowflags[b * ytiles + blockIdx.y] == 0) {
+    return;
+  }
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bx >= xb) return;
+  const int ya = blockIdx.y * kApplyTileY, yz = min(yb, ya + kApplyTileY);
+  exact_rows(ser[b].corr, xb, (size_t)xb * yb, bps + S.bp_off, S.i0, S.nk, S.fcos, S.fsin,
+             S.ray_len, S.thick, bx, ya, yz, out + (size_t)b * xb * yb);
+}
+
+int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                                 const int* active, int nseries, int nz, int xb, int yb,
+                                 const float* d_bp, const int* tflags, const int* rowflags,
+                                 float* out, cudaStream_t st) {
+  dim3 blk(128, 1), grd((xb + 127) / 128, (yb + kApplyTileY - 1) / kApplyTileY, nseries);
+  k_reproject_exact_group<<<grd, blk, 0, st>>>(ser, steps, active, nz, xb, yb, d_bp, tflags,
+                                               rowflags, out);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -677,7 +731,18 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
     k_op_apply(const float* __restrict__ corr, int xb, int yb, size_t pix,
                const float* __restrict__ coef, const int2* __restrict__ rowmap,
                const OpTile* __restrict__ tiles, const int* __restrict__ colvalid,
-               int* __restrict__ rowflags, float* __restrict__ out) {
+               int* __restrict__ rowflags, float* __restrict__ out,
+               const ApplyJob* __restrict__ jobs, const int* __restrict__ active) {
+  if (jobs) {
+    // group form: blockIdx.z selects the series
+    if (active && active[blockIdx.z] == 0) return;
+    const ApplyJob J = jobs[blockIdx.z];
+    corr = J.corr;
+    tiles = J.tiles;
+    colvalid = J.colvalid;
+    rowflags = J.rowflags;
+    out = J.out;
+  }
   __shared__ __align__(16) float As[2][kOpChunk][kApplyTileY];
   __shared__ __align__(16) float Bs[2][kOpChunk][kOpTileX];
   __shared__ int s_flag;
@@ -768,7 +833,19 @@ int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr
                            int* d_rowflags, float* out, cudaStream_t st) {
   dim3 grd(op.ntiles, (op.yb + kApplyTileY - 1) / kApplyTileY);
   k_op_apply<<<grd, 256, 0, st>>>(corr, op.xb, op.yb, pix, op.coef, op.rowmap, op.tiles,
-                                  op.colvalid, d_rowflags, out);
+                                  op.colvalid, d_rowflags, out, nullptr, nullptr);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
+                                 const int* active, int njobs, int xb, int yb, int ntiles,
+                                 cudaStream_t st) {
+  dim3 grd(ntiles, (yb + kApplyTileY - 1) / kApplyTileY, njobs);
+  k_op_apply<<<grd, 256, 0, st>>>(nullptr, xb, yb, (size_t)xb * yb, set.coef.as<float>(),
+                                  set.rowmap.as<int2>(), nullptr, nullptr, nullptr, nullptr,
+                                  d_jobs, active);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

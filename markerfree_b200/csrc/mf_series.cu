@@ -47,6 +47,11 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   } else if (kind == 4) {
     // 1-D R2C in place with the default padded layout (tilt-axis lines)
     r = cufftPlan1d(&h, nx, CUFFT_R2C, batch);
+  } else if (kind == 5) {
+    // 2-D C2R in place over `batch` maps spaced two padded images apart (the second
+    // image of each (reference, image) pair of a group's cross-correlation buffer)
+    int n[2] = {ny, nx}, inem[2] = {ny, cmp}, onem[2] = {ny, pad};
+    r = cufftPlanMany(&h, 2, n, inem, 1, 2 * ny * cmp, onem, 1, 2 * ny * pad, CUFFT_C2R, batch);
   } else if (kind == 2) {
     int n[2] = {ny, nx}, inem[2] = {ny, pad}, onem[2] = {ny, cmp};
     r = cufftPlanMany(&h, 2, n, inem, 1, ny * pad, onem, 1, ny * cmp, CUFFT_R2C, batch);
@@ -466,7 +471,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   if (P.prec != MF_PREC_FP32) {
     P.xpitch = (xb + 7) / 8 * 8;
     MF_TRY(P.corr16.alloc((size_t)2 * P.xpitch * yb * nz));
-    MF_TRY(P.tflags.alloc(sizeof(int) * (size_t)nz * P.ytiles));
+    MF_TRY(P.tflags.alloc(sizeof(int) * (size_t)nz * P.ytiles * kFlagParts));
     MF_TRY(P.d_tcerr.alloc(sizeof(int)));
     MF_CHECK_CUDA(cudaMemsetAsync(P.d_tcerr.p, 0, sizeof(int), st));
     P.tc_nb = tc_pick_rows(c, xb, yb);

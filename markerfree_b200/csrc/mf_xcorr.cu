@@ -3,9 +3,9 @@
 //
 // Reference: Markerfree/src/method/CalcCC.cu (GSum2D/GSum1D :48-92, GConv,
 // GWiener, GCenterOrigin :95-135, GNormalize :137-147, GStretchRandom :149-171,
-// GRoundEdge :173-195, FindPeak :381-435) and ProjAlign.cpp (PANorm :373-390,
-// PAFindPeak :403-453, ClacAlignProj :259-319, FitRotCenterZ/RemoveOffsetZ
-// :537-579).  The reference copies every cross-correlation map to the host and
+// GRoundEdge :173-195, FindPeak :381-435) and ProjAlign.cpp (PANorm :295-312,
+// PAFindPeak :325-375, ClacAlignProj :181-241, FitRotCenterZ/RemoveOffsetZ
+// :459-501).  The reference copies every cross-correlation map to the host and
 // scans it on one CPU thread; here the arg-max, the parabolic fit and the
 // parameter update run on the GPU and nothing leaves the device.
 #include "mf_internal.hpp"
@@ -18,6 +18,20 @@ constexpr int kMomRows = 8;  // image rows per partial-sum block
 __device__ __forceinline__ const float* image_ptr(const float* src0, const float* src1,
                                                   size_t img_stride, int img) {
   return (img == 1 && src1) ? src1 : src0 + (size_t)img * img_stride;
+}
+
+// Source images of a group step: image 2b is series b's re-projection, image
+// 2b+1 its held-out projection; series with active[b] == 0 are skipped.
+struct ImgTable {
+  const float* const* ptrs;  // null: image_ptr() addressing
+  const int* active;
+};
+__device__ __forceinline__ const float* table_ptr(const ImgTable& t, const float* src0,
+                                                  const float* src1, size_t img_stride, int img) {
+  return t.ptrs ? t.ptrs[img] : image_ptr(src0, src1, img_stride, img);
+}
+__device__ __forceinline__ bool table_skip(const ImgTable& t, int img) {
+  return t.active != nullptr && t.active[img >> 1] == 0;
 }
 
 // Block-wide sum of two doubles over 256 threads in a fixed order.
@@ -47,8 +61,9 @@ __device__ __forceinline__ double2 block_sum2(double a, double b) {
 __global__ void __launch_bounds__(256) k_moments(const float* __restrict__ src0,
                                                  const float* __restrict__ src1, int w, int h,
                                                  int stride, size_t img_stride,
-                                                 double2* __restrict__ part) {
-  const float* p = image_ptr(src0, src1, img_stride, blockIdx.y);
+                                                 double2* __restrict__ part, ImgTable tab) {
+  if (table_skip(tab, blockIdx.y)) return;
+  const float* p = table_ptr(tab, src0, src1, img_stride, blockIdx.y);
   double a = 0.0, b = 0.0;
   const int y0 = blockIdx.x * kMomRows, y1 = min(h, y0 + kMomRows);
   for (int y = y0; y < y1; ++y) {
@@ -94,17 +109,17 @@ __global__ void k_norm_mask(const float* __restrict__ src, const float* __restri
                             int src_stride, size_t src_img_stride, int w, int h, int pad,
                             size_t dst_img_stride, const float2* __restrict__ stats, float cx,
                             float cy, float msx, float msy, float power,
-                            float* __restrict__ dst) {
+                            float* __restrict__ dst, ImgTable tab) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y * blockDim.y + threadIdx.y;
   int img = blockIdx.z;
-  if (x >= pad || y >= h) return;
+  if (x >= pad || y >= h || table_skip(tab, img)) return;
   float* d = dst + (size_t)img * dst_img_stride + (size_t)y * pad + x;
   if (x >= w) {
     *d = 0.0f;
     return;
   }
-  float v = image_ptr(src, src1, src_img_stride, img)[(size_t)y * src_stride + x];
+  float v = table_ptr(tab, src, src1, src_img_stride, img)[(size_t)y * src_stride + x];
   float2 st = stats[img];
   if (!(v < -1e10f)) v = __fdiv_rn(__fsub_rn(v, st.x), st.y);  // GNormalize
   if (v < -1e10f) {                                             // GRoundEdge
@@ -130,11 +145,29 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
                   int with_std, float cx, float cy, float msx, float msy, float power, float* dst,
                   double2* d_part, float2* d_stats, cudaStream_t st) {
   const int nb = moment_parts(h);
-  k_moments<<<dim3(nb, nimg), 256, 0, st>>>(src, src1, w, h, src_stride, src_img_stride, d_part);
+  const ImgTable tab{nullptr, nullptr};
+  k_moments<<<dim3(nb, nimg), 256, 0, st>>>(src, src1, w, h, src_stride, src_img_stride, d_part,
+                                            tab);
   k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, with_std, d_stats);
   dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
   k_norm_mask<<<grd, blk, 0, st>>>(src, src1, src_stride, src_img_stride, w, h, pad,
-                                   dst_img_stride, d_stats, cx, cy, msx, msy, power, dst);
+                                   dst_img_stride, d_stats, cx, cy, msx, msy, power, dst, tab);
+  c->launches += 3;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int norm_mask_pad_group(Context* c, const float* const* d_ptrs, const int* active, int nimg,
+                        int w, int h, int pad, size_t dst_img_stride, float cx, float cy,
+                        float msx, float msy, float power, float* dst, double2* d_part,
+                        float2* d_stats, cudaStream_t st) {
+  const int nb = moment_parts(h);
+  const ImgTable tab{d_ptrs, active};
+  k_moments<<<dim3(nb, nimg), 256, 0, st>>>(nullptr, nullptr, w, h, w, 0, d_part, tab);
+  k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, 0, d_stats);
+  dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
+  k_norm_mask<<<grd, blk, 0, st>>>(nullptr, nullptr, w, 0, w, h, pad, dst_img_stride, d_stats,
+                                   cx, cy, msx, msy, power, dst, tab);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -353,6 +386,64 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
   }
 }
 
+// Group form: blockIdx.x = series b, map b at maps + b * map_stride, partials
+// part + b * nparts.
+__global__ void k_pa_peak_update_group(const float* __restrict__ maps, size_t map_stride,
+                                       int stride, int xb, int yb,
+                                       const float2* __restrict__ part, int nparts,
+                                       const GroupSeriesDev* __restrict__ ser,
+                                       const GroupStepDev* __restrict__ steps,
+                                       const int* __restrict__ active, int nx, int ny) {
+  const int b = blockIdx.x;
+  if (active && active[b] == 0) return;
+  const float* map = maps + (size_t)b * map_stride;
+  float bv;
+  int bi;
+  reduce_partials(part + (size_t)b * nparts, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const int ip = steps[b].ip;
+  int px = 0, py = 0;
+  pa_window_peak(bi, stride, xb, yb, &px, &py);
+  double dx, dy, pk;
+  pa_fit(map, stride, px, py, &dx, &dy, &pk);
+  float pkx = (float)(px + dx), pky = (float)(py + dy);
+  float shx = __fsub_rn(pkx, (float)(xb / 2));
+  float shy = __fsub_rn(pky, (float)(yb / 2));
+  float binx = __fdiv_rn((float)nx, (float)xb), biny = __fdiv_rn((float)ny, (float)yb);
+  float a0 = __fmul_rn(shx, binx), a1 = __fmul_rn(shy, biny);
+  float fs = __fadd_rn(__fmul_rn(a0, a0), __fmul_rn(a1, a1));
+  fs = sqrtf(fs);
+  float r = S.rot[ip];
+  rot_shift(a0, a1, r, &a0, &a1);
+  float i0, i1;
+  z_induced(*S.z0, S.angles[ip], r, &i0, &i1);
+  a0 = __fadd_rn(a0, i0);
+  a1 = __fadd_rn(a1, i1);
+  S.sx[ip] = __fadd_rn(S.sx[ip], a0);
+  S.sy[ip] = __fadd_rn(S.sy[ip], a1);
+  S.err[ip] = fs;
+  S.meas[2 * ip] = shx;
+  S.meas[2 * ip + 1] = shy;
+}
+
+int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,
+                         int yb, float2* d_part, const GroupSeriesDev* ser,
+                         const GroupStepDev* steps, const int* active, int nseries, int nx,
+                         int ny, cudaStream_t st) {
+  int sx = xb / 20, sy = yb / 20;
+  if (sx < 3) sx = 3;
+  if (sy < 3) sy = 3;
+  const int nb = kPeakParts;
+  k_peak_partial<<<dim3(nb, nseries), 256, 0, st>>>(maps, map_stride, stride, sx, xb - sx, sy,
+                                                    yb - sy, d_part);
+  k_pa_peak_update_group<<<nseries, 32, 0, st>>>(maps, map_stride, stride, xb, yb, d_part, nb,
+                                                 ser, steps, active, nx, ny);
+  c->launches += 2;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
                    int ip, int nx, int ny, const float* d_angles, float* d_sx, float* d_sy,
                    const float* d_rot, const float* d_z0, float* d_err, float* d_meas,
@@ -451,9 +542,54 @@ int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w
 // ---------------------------------------------------------------------------
 // FitRotCenterZ + RemoveOffsetZ(-1) (ProjAlign.cpp:459-501, 553-579); the
 // reference's uninitialised accumulator dA is taken as 0.
+__device__ void fit_z0_one(int nz, int zt, const float* __restrict__ angles, float* sx,
+                           float* sy, const float* __restrict__ rot, float* z0p);
+
 __global__ void k_fit_z0(int nz, int zt, const float* __restrict__ angles, float* sx, float* sy,
                          const float* __restrict__ rot, float* z0p) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  fit_z0_one(nz, zt, angles, sx, sy, rot, z0p);
+}
+
+__global__ void k_fit_z0_group(const GroupSeriesDev* __restrict__ ser,
+                               const int* __restrict__ active, int nz) {
+  const int b = blockIdx.x;
+  if (threadIdx.x != 0 || (active && active[b] == 0)) return;
+  const GroupSeriesDev& S = ser[b];
+  fit_z0_one(nz, S.zt, S.angles, S.sx, S.sy, S.rot, S.z0);
+}
+
+// max over err[order[i]] (the DoIt return value), initial -1e20, per series
+__global__ void k_max_err_group(const GroupSeriesDev* __restrict__ ser,
+                                const int* __restrict__ active, int n, float* out) {
+  const int b = blockIdx.x;
+  if (threadIdx.x != 0 || (active && active[b] == 0)) return;
+  float m = -1e20f;
+  for (int i = 0; i < n; ++i) {
+    float e = ser[b].err[ser[b].order[i]];
+    if (e > m) m = e;
+  }
+  out[b] = m;
+}
+
+int fit_z0_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int nz,
+                 cudaStream_t st) {
+  k_fit_z0_group<<<nseries, 32, 0, st>>>(ser, active, nz);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int n,
+                  float* d_out, cudaStream_t st) {
+  k_max_err_group<<<nseries, 32, 0, st>>>(ser, active, n, d_out);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+__device__ void fit_z0_one(int nz, int zt, const float* __restrict__ angles, float* sx,
+                           float* sy, const float* __restrict__ rot, float* z0p) {
   float s0x, s0y;
   rot_shift(sx[zt], sy[zt], -rot[zt], &s0x, &s0y);
   float cent0 = (float)((double)s0x / cos((double)angles[zt] * kD2R));

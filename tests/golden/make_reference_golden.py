@@ -16,11 +16,19 @@ leaves undefined and which may hang a GPU, so every case passes a non-zero offse
 (-g O,... with O = 1e-4 degrees) and the search is never run.
 
 usage: python tests/golden/make_reference_golden.py OUTDIR [case ...]
+       python tests/golden/make_reference_golden.py --fixtures OUTDIR [case ...]
+
+The second form turns the run outputs in OUTDIR into the committed fixtures
+tests/golden/ref_<case>.json (generator arguments, flags, the events the
+reference printed, its final parameters and per-slice sums of its aligned
+stack), ref_<case>.txt (its parameter file) and ref_<case>_crop.npy (a 64 x 64
+crop of the middle aligned slice).
 """
 from __future__ import annotations
 
 import json
 import os
+import re
 import subprocess
 import sys
 import time
@@ -112,7 +120,72 @@ def run_case(outdir, name):
     return rc
 
 
+# The reference's stdout lines kept as events (printf formats of Transform.cpp:67,92,
+# Rotate.cu:328, ProjAlign.cpp:203,485 and Process.cpp:297,305).
+_EVENT_PATTERNS = [
+    ("img", re.compile(r"^Image\s+(\d+) shift:\s+(\S+),\s+(\S+) px")),
+    ("maxerr", re.compile(r"^maxerr:\s+(\S+)")),
+    ("axis", re.compile(r"^New tilt axis:\s+(\S+)")),
+    ("z0", re.compile(r"^Rot center Z:\s+\S+\s+(\S+)\s+\S+")),
+    ("err", re.compile(r"^f(?:Last)?Err\S*:\s+(\S+)")),
+    ("meas", re.compile(r"^\s+(-?\d+\.\d\d)\s+(-?\d+\.\d\d)\s+(-?\d+\.\d\d)\s*$")),
+]
+
+
+def parse_log(text):
+    events = []
+    for line in text.splitlines():
+        for kind, pat in _EVENT_PATTERNS:
+            m = pat.match(line)
+            if not m:
+                continue
+            vals = [float(v) for v in m.groups()]
+            if kind == "img":
+                vals[0] = int(vals[0])
+            events.append([kind] + vals)
+            break
+    return events
+
+
+def parse_txt(path):
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("#"):
+                continue
+            parts = line.split()
+            if len(parts) == 5:
+                rows.append([float(v) for v in parts])
+    return rows
+
+
+def write_fixtures(outdir, name):
+    d = os.path.join(outdir, name)
+    with open(os.path.join(d, "case.json")) as fh:
+        case = json.load(fh)
+    with open(os.path.join(d, "ref.log"), errors="replace") as fh:
+        events = parse_log(fh.read())
+    al = np.load(os.path.join(d, "aligned.npz"))
+    fx = {"case": name, "generator": case["generator"], "thickness": case["thickness"],
+          "nproj": case["nproj"], "cmd": case["cmd"], "events": events,
+          "params": parse_txt(os.path.join(d, "ref.txt")),
+          "aligned_slice_sum": al["slice_sum"].tolist(),
+          "aligned_slice_sq": al["slice_sq"].tolist()}
+    with open(os.path.join(HERE, f"ref_{name}.json"), "w") as fh:
+        json.dump(fx, fh)
+    with open(os.path.join(d, "ref.txt")) as src, open(os.path.join(HERE, f"ref_{name}.txt"),
+                                                       "w") as dst:
+        dst.write(src.read())
+    np.save(os.path.join(HERE, f"ref_{name}_crop.npy"), al["crop"])
+    print(name, len(events), "events", flush=True)
+
+
 def main():
+    if sys.argv[1] == "--fixtures":
+        outdir = sys.argv[2]
+        for n in sys.argv[3:] or list(CASES):
+            write_fixtures(outdir, n)
+        return 0
     outdir = sys.argv[1]
     names = sys.argv[2:] or list(CASES)
     rc = 0
