@@ -1,16 +1,22 @@
 """Series/min of the B200 alignment path on the realistic single-series workload.
 
-Workload: one 2048 x 2048 x 61-tilt series (+-60 deg in 2 deg steps, tilt axis 84.7,
+Workload: 2048 x 2048 x 61-tilt series (+-60 deg in 2 deg steps, tilt axis 84.7,
 shifts N(0, 8 px) + 0.3 px/tilt drift, Poisson + Gaussian noise at SNR 0.05), run as
 `-g 0,0,0,0,300,1,0 -p 10`: pre-processing, coarse alignment (3 x stretch cross-
 correlation + tilt-axis search, tilt-angle offset search), the full projection-
-matching schedule, and the aligned output stack.  One step aligns one series.
-Seeded synthetic data stands in for the reference's simulated phantoms.
+matching schedule, and the aligned output stack.  Seeded synthetic data stands in
+for the reference's simulated phantoms.
 
-  value  series/min with the raw stack already in HBM and the aligned stack written to
-         HBM (mf_align_device), summed over ranks (independent series per GPU)
-  e2e    the same through the host API (mf_align) with pinned host buffers: the raw
-         stack upload and the aligned stack download are inside the timed region
+  value   series/min of the batched mixed-precision form: one step aligns --batch
+          series (default 8) with FP16 re-projection operands, projection matching
+          in one lockstep group (mf_align_many_device), raw stacks already in HBM and
+          aligned stacks written to HBM; summed over ranks (independent series)
+  e2e     the same through the C ABI with host buffers: uploads of the raw stacks
+          from pinned memory and downloads of the aligned stacks inside the timed
+          region
+  plain   one series at a time with FP32 operands (the reference's arithmetic)
+  served  the serving loop (mf_server_*) on a Poisson stream of mixed-size requests
+          at 80% of the measured batched capacity: series/min and p50/p99 latency
 
 `--impl reference` times the reference algorithm on the host cores: the reference
 program has no CPU implementation (every stage is CUDA), so the CPU restatement in
@@ -111,8 +117,8 @@ def make_workload(scale: float):
 
 def workload_config(s, scale):
     nz, ny, nx = s.stack.shape
-    return {"workload": f"single series {nx}x{ny}x{nz} tilts (+-60 deg, 2 deg), T=300, -p 10, "
-                        "coarse + projection matching + aligned stack",
+    return {"workload": f"{nx}x{ny}x{nz}-tilt series (+-60 deg, 2 deg), T=300, -p 10: "
+                        "pre-processing, coarse alignment, projection matching, aligned stack",
             "nx": nx, "ny": ny, "tilts": nz, "thickness": s.thickness, "nproj": 10,
             "scale": scale, "l2": "inputs (1 GiB raw stack) larger than L2 (126 MB)",
             "parallelism": "independent series per GPU"}
@@ -195,6 +201,67 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def _time_steps(stream, fn, steps):
+    """CUDA-event time (ms) of `steps` calls of fn on the library's stream."""
+    import torch
+    evs = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def served_run(mf, s, dev, n_req, capacity_spm, seed=5):
+    """The serving loop on a Poisson arrival stream (the served-request workload:
+    sizes 50% 2048^2, 30% 1024^2, 20% 4096^2, mean rate 80% of the measured batched
+    capacity).  The 1024^2 and 4096^2 series are derived from the 2048^2 series by
+    2 x 2 binning and 2 x pixel replication, so one phantom serves all sizes.
+    Requests return their parameters; inputs come from pinned host memory."""
+    import torch
+    nz = s.stack.shape[0]
+    st2 = s.stack
+    st1 = st2.reshape(nz, st2.shape[1] // 2, 2, st2.shape[2] // 2, 2).mean(axis=(2, 4))
+    st4 = np.repeat(np.repeat(st2, 2, axis=1), 2, axis=2)
+    pinned = {}
+    for key, arr, az in (("2048", st2, s.thickness), ("1024", st1, max(8, s.thickness // 2)),
+                         ("4096", st4, s.thickness)):
+        t = torch.from_numpy(np.ascontiguousarray(arr, np.float32)).pin_memory()
+        pinned[key] = (t, arr.shape, az)
+    del st4
+    rng = np.random.default_rng(seed)
+    n4 = max(1, round(0.2 * n_req))
+    n1 = max(1, round(0.3 * n_req))
+    kinds = ["4096"] * n4 + ["1024"] * n1 + ["2048"] * (n_req - n4 - n1)
+    rng.shuffle(kinds)
+    rate_per_s = 0.8 * capacity_spm / 60.0
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_per_s, n_req))
+    srv = mf.Server(gpu=dev, hbm_budget=0, max_group=8, workers=3, group_wait_ms=40.0)
+    ids = []
+    t0 = time.perf_counter()
+    for k, ta in zip(kinds, arrivals):
+        wait = ta - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        t, shape, az = pinned[k]
+        ids.append(srv.submit(None, s.angles, raw_ptr=t.data_ptr(), shape=shape, align_z=az,
+                              nproj=10, precision=PRECISIONS["fp16"]))
+    lats = [srv.wait(j, timeout_s=1800.0)[2] for j in ids]
+    st = srv.stats()
+    srv.close()
+    return {"requests": n_req, "mix": {"2048": kinds.count("2048"), "1024": kinds.count("1024"),
+                                       "4096": kinds.count("4096")},
+            "arrival_rate_per_min": rate_per_s * 60.0,
+            "series_per_min": st["series_per_min"], "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+            "mean_latency_s": float(np.mean(lats)), "groups": int(st["groups"]),
+            "mean_group_size": st["mean_group"], "peak_admitted_gb": st["peak_bytes"] / 1e9,
+            "precision": "fp16 operands, f32 accumulation",
+            "returns": "per-tilt parameters (aligned stacks not copied back)"}
+
+
 def run_ours(args):
     import torch
     import markerfree_b200 as mf
@@ -213,106 +280,125 @@ def run_ours(args):
     nz, ny, nx = s.stack.shape
     xo, yo = mf.binned_size(nx, ny, 1)
     ctx = mf.Context(dev)
-    d_raw = torch.from_numpy(s.stack).to(f"cuda:{dev}")
-    d_out = torch.empty((nz, yo, xo), dtype=torch.float32, device=f"cuda:{dev}")
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+    B = args.batch
     prec = PRECISIONS[args.precision]
     kw = dict(offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=s.thickness, out_bin=1, nproj=10,
               precision=prec)
+    d_raw = torch.from_numpy(s.stack).to(f"cuda:{dev}")
+    d_outs = [torch.empty((nz, yo, xo), dtype=torch.float32, device=f"cuda:{dev}")
+              for _ in range(B)]
+    angs = [s.angles] * B
 
     def barrier():
         if pg is not None:
             pg.barrier()
         torch.cuda.synchronize()
 
-    passes = 0
+    last = {}
+
+    def step():
+        ps, passes = mf.align_many_device(ctx, [d_raw] * B, nx, ny, nz, angs, d_outs, **kw)
+        last["passes"] = int(passes[0])
+        last["axis"] = float(ps[0].rotate[0])
+
     for _ in range(args.warmup):
-        p, passes = mf.align_device(ctx, d_raw, nx, ny, nz, s.angles, d_out, **kw)
-    l0 = ctx.kernel_launches()
+        step()
     barrier()
-    evs = []
+    l0 = ctx.kernel_launches()
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            p, passes = mf.align_device(ctx, d_raw, nx, ny, nz, s.angles, d_out, **kw)
-            b.record(stream)
-            evs.append((a, b))
+        ms = _time_steps(stream, step, args.steps)
         barrier()
         launches = ctx.kernel_launches() - l0
-        ms = sum(a.elapsed_time(b) for a, b in evs)
-        # Same steps again with per-stage CUDA events on the library's stream.  Timed
-        # passes then launch kernels one by one instead of replaying the captured
-        # graph (graph-recorded events cannot be timed); the kernels are identical.
+        # one more step with per-stage CUDA events on the library's stream (passes then
+        # launch kernels one by one instead of replaying the graph; same kernels)
         ctx.set_profiling(True)
         ctx.stage_times()
-        p_evs = []
-        for _ in range(args.steps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            mf.align_device(ctx, d_raw, nx, ny, nz, s.angles, d_out, **kw)
-            b.record(stream)
-            p_evs.append((a, b))
-        barrier()
+        p_ms = _time_steps(stream, step, 1)
         st = ctx.stage_times()
         ctx.set_profiling(False)
-    p_ms = sum(a.elapsed_time(b) for a, b in p_evs)
-    # e2e through the host API with pinned buffers
+    # e2e through the C ABI with host buffers: per step B uploads from pinned memory,
+    # the group alignment, B downloads of the aligned stacks
     h_raw = torch.from_numpy(s.stack).pin_memory()
     h_out = torch.empty((nz, yo, xo), dtype=torch.float32).pin_memory()
-    mf.align_host_ptr(ctx, h_raw.data_ptr(), nx, ny, nz, s.angles, h_out.data_ptr(), **kw)
+    d_ins = [torch.empty_like(d_raw) for _ in range(B)]
+
+    def step_e2e():
+        with torch.cuda.stream(stream):
+            for d in d_ins:
+                d.copy_(h_raw, non_blocking=True)
+        mf.align_many_device(ctx, d_ins, nx, ny, nz, angs, d_outs, **kw)
+        with torch.cuda.stream(stream):
+            for d in d_outs:
+                h_out.copy_(d, non_blocking=True)
+
+    step_e2e()
     barrier()
-    e_evs = []
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        mf.align_host_ptr(ctx, h_raw.data_ptr(), nx, ny, nz, s.angles, h_out.data_ptr(), **kw)
-        b.record(stream)
-        e_evs.append((a, b))
+    e_ms = _time_steps(stream, step_e2e, args.steps)
+    del d_ins
+    # the plain path: one series at a time, FP32 (the reference's arithmetic)
+    kw32 = dict(kw, precision=PRECISIONS["fp32"])
+    d_one = d_outs[0]
+
+    def step_plain():
+        mf.align_device(ctx, d_raw, nx, ny, nz, s.angles, d_one, **kw32)
+
+    for _ in range(2):
+        step_plain()
     barrier()
-    e_ms = sum(a.elapsed_time(b) for a, b in e_evs)
-    t = torch.tensor([ms, e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    pl_ms = _time_steps(stream, step_plain, args.steps)
+    t = torch.tensor([ms, e_ms, pl_ms], dtype=torch.float64, device=f"cuda:{dev}")
     if pg is not None:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    ms, e_ms = float(t[0]), float(t[1])
+    ms, e_ms, pl_ms = (float(v) for v in t)
     ms_step = ms / args.steps
-    value = 60000.0 / ms_step * world
-    e2e_value = 60000.0 / (e_ms / args.steps) * world
+    value = 60000.0 * B / ms_step * world
+    e2e_value = 60000.0 * B / (e_ms / args.steps) * world
+    plain_value = 60000.0 / (pl_ms / args.steps) * world
     pk, src = peaks()
-    # dominant kernel: the banded re-projection (measured per held-out tilt)
+    # dominant kernel: the re-projection, one launch per step of a pass for the group
     launches_rep = max(st["reproj_launches"], 1)
     t_launch = st["reproj_ms"] / launches_rep / 1e3
     bytes_launch = st["reproj_bytes"] / launches_rep
     achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
-    kname = ("k_op_apply (FP32 banded operator, sentinel fallback check)" if prec == 0 else
+    tensor_tflops = 2.0 * st["reproj_fma"] / launches_rep / t_launch / 1e12 if t_launch else 0.0
+    kname = ("k_op_apply (FP32 banded operator)" if prec == 0 else
              "k_reproject_tc (tcgen05, 16-bit operands, FP32 accumulation in TMEM)")
-    roof = {"kernel": kname + ", one launch per held-out tilt",
+    roof = {"kernel": kname + f", one launch per held-out tilt step for a group of {B}",
             "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "peak_source": src,
-            "traffic": None,
+            "frac": achieved / pk["hbm_gbs"], "peak_source": src, "traffic": None,
             "avg_launch_ms": t_launch * 1e3, "bytes_per_launch": bytes_launch,
+            "tensor_tflops": tensor_tflops,
+            "tensor_frac_of_bf16_peak": tensor_tflops / (pk.get("bf16_tflops", 1590.0)),
             "share_of_step": st["reproj_ms"] / max(p_ms, 1e-9),
-            "xcorr_and_recorrect_share_of_step": st["xcorr_ms"] / max(p_ms, 1e-9),
-            "fma_per_launch": st["reproj_fma"] / launches_rep,
-            "profiled_ms_per_step": p_ms / args.steps}
+            "rest_of_pass_share_of_step": st["xcorr_ms"] / max(p_ms, 1e-9),
+            "profiled_ms_per_step": p_ms}
     prof = os.path.join(ROOT, "profiles", "traffic_reproject.json")
     if os.path.exists(prof):
         with open(prof) as f:
             tr = json.load(f)
-        roof["traffic"] = tr.get("bytes_per_launch_full_scale")
+        roof["traffic"] = tr.get("bytes_per_launch")
+    cfg = workload_config(s, args.scale)
+    cfg.update({"series_per_step": B, "grouping": f"{B} series per group (lockstep passes)"})
     line = {"metric": "series/min (2k^2, 61 tilts)", "value": value, "unit": "series/min",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if prec == 0 else f"{args.precision} operands, f32 accumulation",
             "data": "synthetic (seeded phantom series, BASELINE shapes)",
-            "config": workload_config(s, args.scale),
+            "config": cfg,
             "e2e": {"value": e2e_value, "unit": "series/min",
-                    "h2d_bytes_per_step": int(s.stack.nbytes),
-                    "d2h_bytes_per_step": int(h_out.numel() * 4 + 3 * nz * 4)},
-            "gpu_launches": int(launches), "passes_per_series": passes,
+                    "h2d_bytes_per_step": int(s.stack.nbytes) * B,
+                    "d2h_bytes_per_step": int(h_out.numel() * 4 + 3 * nz * 4) * B},
+            "plain": {"value": plain_value, "unit": "series/min",
+                      "what": "one series at a time, FP32 operands (mf_align_device)"},
+            "batched_over_plain": value / plain_value,
+            "gpu_launches": int(launches), "passes_per_series": last.get("passes"),
             "roofline": roof, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["served"] = served_run(mf, s, dev, args.serve_requests, value / world)
+        line["served_over_plain"] = line["served"]["series_per_min"] / plain_value
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(s, passes=max(passes, 1))
+        line["cpu_baseline"] = cpu_sample(s, passes=max(last.get("passes", 1), 1))
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -325,7 +411,8 @@ def run_ours(args):
 def run_kernel_case(args):
     """One stage of the workload on its own, for profilers (ncu -k ...): `reproject`
     re-projects one held-out tilt (full size, 10 neighbours) with the banded
-    operator; `xcorr` measures one cross-correlation shift."""
+    operator; `xcorr` measures one cross-correlation shift; `axis` runs one
+    tilt-axis search (100 candidates over 20 degrees)."""
     import torch
     import markerfree_b200 as mf
     s = make_workload(args.scale)
@@ -340,6 +427,13 @@ def run_kernel_case(args):
     g = torch.Generator(device="cuda").manual_seed(7)
     corr = torch.randn((nz, ny, nx), generator=g, device="cuda", dtype=torch.float32)
     out = torch.empty((ny, nx), device="cuda", dtype=torch.float32)
+    if args.kernel_case == "axis":
+        ser = mf.Series(ctx, s.stack, ang)
+        for _ in range(args.steps):
+            ser.tilt_axis(20.0)
+        ctx.sync()
+        print(json.dumps({"kernel_case": "axis", "tilts": nz}))
+        return 0
     for _ in range(args.steps):
         if args.kernel_case == "reproject":
             mf.dev_reproject(ctx, corr, nx, ny, nz, ang, ip, i0, i1, s.thickness,
@@ -353,7 +447,7 @@ def run_kernel_case(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr"],
+    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr", "axis"],
                     help="run one stage alone (profiling)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -361,8 +455,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests only)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--precision", default="fp32", choices=list(PRECISIONS),
-                    help="re-projection operands (fp32 = the reference's arithmetic)")
+    ap.add_argument("--precision", default="fp16", choices=list(PRECISIONS),
+                    help="re-projection operands of the batched path (fp32 = the reference's "
+                         "arithmetic; the plain line is always fp32)")
+    ap.add_argument("--batch", type=int, default=8, help="series per group (one step)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
+    ap.add_argument("--serve-requests", type=int, default=20)
     ap.add_argument("--kernel-method", type=int, default=1,
                     help="re-projection method of --kernel-case reproject (1 FP32, 2 FP16, 3 BF16)")
     args = ap.parse_args()

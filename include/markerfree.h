@@ -205,6 +205,35 @@ MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_ra
                                 int nz, const float* const* file_angles, const mf_options* opt,
                                 mf_align_param* params, float* const* d_out, int* passes);
 
+/* ---- serving: continuous batching of requests ------------------------------
+ * Not in the reference.  A server keeps `workers` streams busy with requests
+ * (tilt series) that arrive at any time: a request is admitted when its
+ * estimated device memory fits in `hbm_budget` bytes (0 = 90% of the free
+ * memory), prepared on its own (upload, pre-processing, coarse alignment), then
+ * projection-matched in a group with other prepared requests of its shape (up to
+ * `max_group`; a request waits at most `group_wait_ms` for companions while more
+ * of its shape are on their way).  A request's result equals the one it gets
+ * when aligned alone. */
+typedef struct mf_server mf_server;
+MF_API int mf_server_create(int gpu, size_t hbm_budget, int max_group, int workers,
+                            double group_wait_ms, mf_server** out);
+/* Queue a request.  raw (nz x ny x nx, file order) and aligned_out (optional,
+ * the mf_correct_stack layout) are caller-owned host memory that must stay valid
+ * until mf_server_wait has returned for the job. */
+MF_API int mf_server_submit(mf_server* s, const float* raw, int nx, int ny, int nz,
+                            const float* file_angles, const mf_options* opt, float* aligned_out,
+                            int64_t* job_id);
+/* Block until the job is done (or timeout_s passes: MF_ERR_STATE).  param arrays
+ * (nz entries), passes and latency_s (submit to done) are optional. */
+MF_API int mf_server_wait(mf_server* s, int64_t job_id, double timeout_s, mf_align_param* param,
+                          int* passes, double* latency_s);
+/* out8: [0] jobs done, [1] series/min from the first submit to the last
+ * completion, [2] p50 and [3] p99 latency (s), [4] peak admitted bytes, [5]
+ * groups run, [6] mean group size, [7] seconds from first submit to last done. */
+MF_API int mf_server_stats(mf_server* s, double* out8);
+/* Finishes every submitted request, then releases the workers. */
+MF_API void mf_server_destroy(mf_server* s);
+
 /* ---- single kernels on caller-owned device memory (same stream semantics:
  * the call is ordered on the context stream and returns after queuing). ------ */
 /* CorrTomoStack::mCorrectProj (Markerfree/src/method/CorrStack.cu:370-397) for one

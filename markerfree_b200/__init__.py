@@ -109,6 +109,17 @@ SIGNATURES = [
                                             ctypes.POINTER(OptionsC),
                                             ctypes.POINTER(AlignParamC),
                                             ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    ("mf_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, _f32p,
+                                        ctypes.POINTER(OptionsC), ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_int64)]),
+    ("mf_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                      ctypes.POINTER(AlignParamC), _c_int_p,
+                                      ctypes.POINTER(ctypes.c_double)]),
+    ("mf_server_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("mf_server_destroy", None, [ctypes.c_void_p]),
     ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -438,6 +449,67 @@ def align_many_device(ctx: Context, d_raws, nx, ny, nz, file_angles, d_outs=None
     for p, c in zip(params, cs):
         p.angle_offset = c.angle_offset
     return params, passes
+
+
+class Server:
+    """Continuous-batching request loop (mf_server_*).  Submitted host arrays are
+    kept referenced until their job has been waited for."""
+
+    def __init__(self, gpu=0, hbm_budget=0, max_group=8, workers=2, group_wait_ms=50.0):
+        h = ctypes.c_void_p()
+        _check(lib().mf_server_create(gpu, hbm_budget, max_group, workers, group_wait_ms,
+                                      ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, raw, file_angles, out=None, offset=0.0, pitch_angle=0.0, zshift=0.0,
+               align_z=600, out_bin=1, nproj=10, precision=PREC_FP32, raw_ptr=None,
+               shape=None) -> int:
+        """raw: float32 (nz, ny, nx) array, or raw_ptr (host address) with shape."""
+        if raw_ptr is None:
+            raw = _f32(raw)
+            nz, ny, nx = raw.shape
+            ptr = raw.ctypes.data
+        else:
+            nz, ny, nx = shape
+            ptr = raw_ptr
+        ang = _f32(file_angles)[:nz].copy()
+        o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
+        jid = ctypes.c_int64()
+        outp = None if out is None else ctypes.c_void_p(out.ctypes.data)
+        _check(lib().mf_server_submit(self.h, ctypes.c_void_p(ptr), nx, ny, nz, ang,
+                                      ctypes.byref(o), outp, ctypes.byref(jid)))
+        self._keep[jid.value] = (raw, ang, out, nz)
+        return jid.value
+
+    def wait(self, job_id: int, timeout_s: float = 600.0):
+        """Returns (Param, passes, latency seconds)."""
+        nz = self._keep[job_id][3]
+        p = Param(nz)
+        c = p.c()
+        n = ctypes.c_int()
+        lat = ctypes.c_double()
+        rc = lib().mf_server_wait(self.h, job_id, timeout_s, ctypes.byref(c), ctypes.byref(n),
+                                  ctypes.byref(lat))
+        self._keep.pop(job_id, None)
+        _check(rc)
+        p.angle_offset = c.angle_offset
+        return p, n.value, lat.value
+
+    def stats(self) -> dict:
+        out = (ctypes.c_double * 8)()
+        _check(lib().mf_server_stats(self.h, out))
+        keys = ("jobs", "series_per_min", "p50_s", "p99_s", "peak_bytes", "groups",
+                "mean_group", "span_s")
+        return dict(zip(keys, out))
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.mf_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def find_proj_range(angles, skip, iproj, nproj):

@@ -23,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + os.path.join(ROOT, "include")] + ARCH
 LIB_SOURCES = ["mf_common.cpp", "mf_io.cpp", "mf_capi.cpp", "mf_correct.cu", "mf_reproj.cu",
-               "mf_reproj_tc.cu", "mf_xcorr.cu", "mf_axis.cu", "mf_series.cu", "mf_batch.cu", "mf_noalloc.cu"]
+               "mf_reproj_tc.cu", "mf_xcorr.cu", "mf_axis.cu", "mf_series.cu", "mf_batch.cu", "mf_serve.cpp",
+               "mf_noalloc.cu"]
 HEADERS = ["mf_internal.hpp", "mf_xcorr.hpp", "mf_series.hpp"]
 
 

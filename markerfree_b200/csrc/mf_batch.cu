@@ -46,8 +46,11 @@ struct mf_group {
   cudaGraphExec_t graph = nullptr;
   int64_t graph_kernels = 0;
   bool use_graph = true;
+  std::vector<cudaEvent_t> events;  // 3 per step when the context profiles
+  double op_bytes = 0, op_fma = 0;  // mean compulsory bytes / MACs of one operator apply
   ~mf_group() {
     if (graph) cudaGraphExecDestroy(graph);
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
   }
 };
 
@@ -232,14 +235,22 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     MF_CHECK_CUDA(cudaMemcpyAsync(g->d_applyjobs.p, jobs.data(), sizeof(ApplyJob) * jobs.size(),
                                   cudaMemcpyHostToDevice, st));
   }
+  const double nops = (double)B * n;
+  g->op_bytes = (g->prec != MF_PREC_FP32 ? g->tcops.bytes : g->ops.bytes) / nops;
+  g->op_fma = (g->prec != MF_PREC_FP32 ? g->tcops.fma : g->ops.fma) / nops;
   // FFT plans (cached per context)
   mf_context* ctx = g->ctx;
-  MF_TRY(ctx->plan({0, xb, yb, (long long)B * nz * yb}, &g->rows_fwd_all));
-  MF_TRY(ctx->plan({1, xb, yb, (long long)B * nz * yb}, &g->rows_inv_all));
-  MF_TRY(ctx->plan({0, xb, yb, (long long)B * yb}, &g->rows_fwd_one));
-  MF_TRY(ctx->plan({1, xb, yb, (long long)B * yb}, &g->rows_inv_one));
-  MF_TRY(ctx->plan({2, xb, yb, 2LL * B}, &g->cc_fwd));
-  MF_TRY(ctx->plan({5, xb, yb, (long long)B}, &g->cc_inv));
+  // The same plan shapes as a single series' pass, executed once per series: a
+  // plan batched over the group may round differently, and a different rounding
+  // can flip a near-tied decision later (tilt-axis candidates, nearest-neighbour
+  // re-correction), so per-series execution keeps each result identical to the
+  // series aligned alone.
+  MF_TRY(ctx->plan({0, xb, yb, (long long)nz * yb}, &g->rows_fwd_all));
+  MF_TRY(ctx->plan({1, xb, yb, (long long)nz * yb}, &g->rows_inv_all));
+  MF_TRY(ctx->plan({0, xb, yb, (long long)yb}, &g->rows_fwd_one));
+  MF_TRY(ctx->plan({1, xb, yb, (long long)yb}, &g->rows_inv_one));
+  MF_TRY(ctx->plan({2, xb, yb, 2}, &g->cc_fwd));
+  MF_TRY(ctx->plan({3, xb, yb, 1}, &g->cc_inv));
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;
 }
@@ -262,16 +273,23 @@ static int group_enqueue(mf_group* g) {
   // CorrTomoStack::DoIt for every tilt of every active series
   GroupCorrArgs ca{ser, nullptr, active, g->nx, g->ny, nz, g->bin, 1, scratch, pad, ppix};
   MF_TRY(launch_correct_group(c, ca, B * nz, st));
-  MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_all, scratch, (cufftComplex*)scratch));
+  for (int b = 0; b < B; ++b) {
+    float* sb = scratch + (size_t)b * nz * ppix;
+    MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_all, sb, (cufftComplex*)sb));
+  }
   MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, B * nz * yb, st));
-  MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_all, (cufftComplex*)scratch, corr));
+  for (int b = 0; b < B; ++b)
+    MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_all, (cufftComplex*)(scratch + (size_t)b * nz * ppix),
+                                corr + (size_t)b * nz * bpix));
   if (tc)
     MF_TRY(launch_to_half(c, corr, xb, yb, nullptr, 0, B * nz, g->prec, g->corr16.p, g->xpitch,
                           g->tflags.as<int>(), st));
   MF_TRY(fit_z0_group(c, ser, active, B, nz, st));
   const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
+  const bool prof = c->profiling && (int)g->events.size() >= 3 * n;
   for (int k = 0; k < n; ++k) {
     const GroupStepDev* sk = steps + (size_t)k * B;
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k], st));
     if (tc) {
       MF_TRY(launch_reproject_tc_group(c, g->tcops, g->tcjobs.data() + (size_t)k * B, B, active,
                                        xb, yb, g->imgmap, g->tc_nb, g->d_tcerr.as<int>(), st));
@@ -286,31 +304,43 @@ static int group_enqueue(mf_group* g) {
                                           nullptr, g->rowflags.as<int>(), g->reproj.as<float>(),
                                           st));
     }
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 1], st));
     // MeaAlignProj for every series: PANorm both images, FFT, filter, inverse, peak
     MF_TRY(norm_mask_pad_group(c, g->d_normptr.as<const float*>() + (size_t)k * 2 * B, active,
                                2 * B, xb, yb, pad, ppix, mcx, mcy, (float)pad, (float)yb, 4.0f,
                                cc, g->mpart.as<double2>(), g->stats.as<float2>(), st));
-    MF_CHECK_CUFFT(cufftExecR2C(g->cc_fwd, cc, (cufftComplex*)cc));
+    for (int b = 0; b < B; ++b) {
+      float* cb = cc + (size_t)b * 2 * ppix;
+      MF_CHECK_CUFFT(cufftExecR2C(g->cc_fwd, cb, (cufftComplex*)cb));
+    }
     MF_TRY(xcorr_filter(c, (cufftComplex*)cc, ppix, nullptr, (cufftComplex*)(cc + ppix), ppix, B,
                         cmp, yb, 500.0f, 1.0f, st));
-    MF_CHECK_CUFFT(cufftExecC2R(g->cc_inv, (cufftComplex*)(cc + ppix), cc + ppix));
+    for (int b = 0; b < B; ++b) {
+      float* mb = cc + (size_t)(2 * b + 1) * ppix;
+      MF_CHECK_CUFFT(cufftExecC2R(g->cc_inv, (cufftComplex*)mb, mb));
+    }
     MF_TRY(pa_peak_update_group(c, cc + ppix, 2 * ppix, pad, xb, yb, g->ppart.as<float2>(), ser,
                                 sk, active, B, g->nx, g->ny, st));
     // re-correct the aligned tilt of every series (mCorrectProj)
     GroupCorrArgs rc{ser, sk, active, g->nx, g->ny, nz, g->bin, 1, g->recorr.as<float>(), pad,
                      ppix};
     MF_TRY(launch_correct_group(c, rc, B, st));
-    MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_one, g->recorr.as<float>(),
-                                (cufftComplex*)g->recorr.as<float>()));
+    for (int b = 0; b < B; ++b) {
+      float* rb = g->recorr.as<float>() + (size_t)b * ppix;
+      MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_one, rb, (cufftComplex*)rb));
+    }
     MF_TRY(launch_rweight(c, (cufftComplex*)g->recorr.as<float>(), cmp, B * yb, st));
-    MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_one, (cufftComplex*)g->recorr.as<float>(),
-                                g->recorr_out.as<float>()));
+    for (int b = 0; b < B; ++b)
+      MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_one,
+                                  (cufftComplex*)(g->recorr.as<float>() + (size_t)b * ppix),
+                                  g->recorr_out.as<float>() + (size_t)b * bpix));
     k_group_scatter<<<dim3(64, B), 256, 0, st>>>(g->recorr_out.as<float>(), ser, sk, active, bpix);
     c->launches++;
     MF_CHECK_CUDA(cudaGetLastError());
     if (tc)
       MF_TRY(launch_to_half(c, corr, xb, yb, g->d_tiltidx.as<int>() + (size_t)k * B, 0, B, g->prec,
                             g->corr16.p, g->xpitch, g->tflags.as<int>(), st));
+    if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 2], st));
   }
   MF_TRY(max_err_group(c, ser, active, B, n, g->d_maxerr.as<float>(), st));
   return MF_OK;
@@ -326,7 +356,13 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   for (int b = 0; b < B; ++b) MF_TRY(g->ser[b]->upload_params());
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_active.p, g->active.data(), sizeof(int) * B,
                                 cudaMemcpyHostToDevice, st));
-  if (g->use_graph && !g->graph) {
+  // Profiled passes run eagerly: events recorded by graph nodes cannot be timed.
+  while (c->profiling && (int)g->events.size() < 3 * g->n) {
+    cudaEvent_t e;
+    MF_CHECK_CUDA(cudaEventCreate(&e));
+    g->events.push_back(e);
+  }
+  if (g->use_graph && !g->graph && !c->profiling) {
     int64_t l0 = c->launches;
     cudaGraph_t gr = nullptr;
     MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -348,7 +384,7 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
       }
     }
   }
-  if (g->graph) {
+  if (g->graph && !c->profiling) {
     MF_CHECK_CUDA(cudaGraphLaunch(g->graph, st));
     c->launches += g->graph_kernels;
   } else {
@@ -372,18 +408,35 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   if (tcerr != 0)
     return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", tcerr);
+  int nact = 0;
   for (int b = 0; b < B; ++b)
     if (active[b]) {
       max_err[b] = me[b];
       g->ser[b]->pa.z0 = g->z0[b];
+      nact++;
     }
+  if (c->profiling && (int)g->events.size() >= 3 * g->n) {
+    // stage times of this pass: [0] re-projection launches (one per step for the
+    // whole group), [2] the rest of each step; bytes and MACs of the active series
+    for (int k = 0; k < g->n; ++k) {
+      float a = 0.0f, b2 = 0.0f;
+      MF_CHECK_CUDA(cudaEventElapsedTime(&a, g->events[3 * k], g->events[3 * k + 1]));
+      MF_CHECK_CUDA(cudaEventElapsedTime(&b2, g->events[3 * k + 1], g->events[3 * k + 2]));
+      c->stage[0] += a;
+      c->stage[2] += b2;
+    }
+    c->stage[1] += g->n;
+    c->stage[3] += 1;
+    c->stage[4] += g->op_bytes * g->n * nact;
+    c->stage[5] += g->op_fma * g->n * nact;
+  }
   return MF_OK;
 }
 
 // Process::mProjAlign + ProjAlignOnce (Process.cpp:272-319) for every series of
 // the group.  Each series follows its own break rule; a pass runs the series that
 // are still inside the current ProjAlignOnce loop.
-static int group_proj_align(mf_group* g, int* passes) {
+int group_proj_align(mf_group* g, int* passes) {
   const int B = g->B;
   std::vector<int> np(B, 0);
   // ResetShift (Process.cpp:321-327); the axis found by the coarse stage is kept
@@ -427,8 +480,8 @@ static int group_proj_align(mf_group* g, int* passes) {
   return MF_OK;
 }
 
-static int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift,
-                        int align_z, int nproj, mf_group** out) {
+int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift, int align_z,
+                 int nproj, mf_group** out) {
   if (!out) return set_error(MF_ERR_ARG, "null output pointer");
   *out = nullptr;
   if (!ctx || !series || nser < 1 || nser > kMaxGroup)
@@ -437,6 +490,7 @@ static int group_create(mf_context* ctx, mf_series* const* series, int nser, flo
     const mf_series* s = series[b];
     if (!s) return set_error(MF_ERR_ARG, "null series %d", b);
     if (s->ctx != ctx) return set_error(MF_ERR_ARG, "series %d belongs to another context", b);
+    if (s->gpu != ctx->c.gpu) return set_error(MF_ERR_ARG, "series %d is on another GPU", b);
     if (s->nx != series[0]->nx || s->ny != series[0]->ny || s->nz != series[0]->nz ||
         s->precision != series[0]->precision)
       return set_error(MF_ERR_ARG,

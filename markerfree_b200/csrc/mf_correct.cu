@@ -6,6 +6,8 @@
 // R-weights it with batched 1-D cuFFTs and un-pads it with one cudaMemcpy per
 // row.  Here resampling and binning are one kernel that writes straight into the
 // row layout the FFT wants, and the inverse FFT writes the dense corrected stack.
+#include <algorithm>
+
 #include "mf_internal.hpp"
 
 namespace mf {
@@ -219,25 +221,29 @@ int launch_correct_one(Context* c, const float* img, int nx, int ny, float sx, f
 }
 
 // CorrStack.cu:431-446: spectrum / N times 2r (0.55 + 0.45 cos 2 pi r), r = k / N.
+// Rows are visited with a grid-stride loop, so any number of rows (a whole group
+// of stacks) fits in one launch.
 __global__ void k_rweight(cufftComplex* spec, int cmp, int rows) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int row = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= cmp || row >= rows) return;
-  size_t i = (size_t)row * cmp + x;
+  if (x >= cmp) return;
   float fN = 2 * ((float)cmp - 1.0f);
-  cufftComplex v = spec[i];
-  v.x = __fdiv_rn(v.x, fN);
-  v.y = __fdiv_rn(v.y, fN);
   float r = __fdiv_rn((float)x, fN);
   float cw = (float)cos((double)__fmul_rn(6.2831852f, r));
   r = __fmul_rn(__fmul_rn(2.0f, r), __fadd_rn(0.55f, __fmul_rn(0.45f, cw)));
-  v.x = __fmul_rn(v.x, r);
-  v.y = __fmul_rn(v.y, r);
-  spec[i] = v;
+  for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < rows;
+       row += gridDim.y * blockDim.y) {
+    size_t i = (size_t)row * cmp + x;
+    cufftComplex v = spec[i];
+    v.x = __fdiv_rn(v.x, fN);
+    v.y = __fdiv_rn(v.y, fN);
+    v.x = __fmul_rn(v.x, r);
+    v.y = __fmul_rn(v.y, r);
+    spec[i] = v;
+  }
 }
 
 int launch_rweight(Context* c, cufftComplex* spec, int cmp, int rows, cudaStream_t st) {
-  dim3 blk(128, 2), grd((cmp + 127) / 128, (rows + 1) / 2);
+  dim3 blk(128, 2), grd((cmp + 127) / 128, std::min((rows + 1) / 2, 16384));
   k_rweight<<<grd, blk, 0, st>>>(spec, cmp, rows);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());

@@ -43,6 +43,9 @@ from markerfree_b200 import synth  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "Markerfree")
 
+# A case name ending in "_p<k>" runs the base case with its stack multiplied by
+# 1 + 1e-6 * U(-1, 1) (seed k): the spread of the reference's own results over
+# such perturbations bounds how closely any other implementation can follow it.
 CASES = {
     # name: (generator kwargs, thickness, nproj, timeout s)
     "c1s256": (dict(nx=256, ny=256, vol_z=64, n_blobs=80, seed=1101, snr=0.5,
@@ -52,7 +55,22 @@ CASES = {
                 40, 6, 600),
     "cfg1": (dict(nx=512, ny=512, vol_z=128, n_blobs=200, seed=1001, snr=0.1,
                   shift_sd=4.0), 100, 10, 1200),
+    # a well-conditioned series: high SNR, the alignment settles in few passes
+    "hi384": (dict(nx=384, ny=384, vol_z=96, n_blobs=160, seed=1201, snr=4.0, shift_sd=3.0,
+                   axis=87.0), 80, 10, 1200),
 }
+
+
+def case_spec(name):
+    """(generator kwargs, thickness, nproj, timeout, perturbation seed or None)."""
+    base, _, tag = name.partition("_p")
+    kw, thick, nproj, tmo = CASES[base]
+    return kw, thick, nproj, tmo, (int(tag) if tag else None)
+
+
+def perturbed(stack, seed):
+    rng = np.random.default_rng(seed)
+    return (stack * (1.0 + 1e-6 * rng.uniform(-1.0, 1.0, stack.shape))).astype(np.float32)
 
 
 def write_mrc(path, stack, mode=2):
@@ -85,13 +103,13 @@ def read_mrc_float(path):
 
 
 def run_case(outdir, name):
-    kw, thick, nproj, tmo = CASES[name]
+    kw, thick, nproj, tmo, pert = case_spec(name)
     s = synth.make_series(thickness=thick, nproj=nproj, **kw)
     d = os.path.join(outdir, name)
     os.makedirs(d, exist_ok=True)
     mrc = os.path.join(d, "in.mrc")
     tlt = os.path.join(d, "in.rawtlt")
-    write_mrc(mrc, s.stack)
+    write_mrc(mrc, s.stack if pert is None else perturbed(s.stack, pert))
     with open(tlt, "w") as fh:
         for a in s.angles:
             fh.write(f"{a:.2f}\n")
@@ -115,7 +133,7 @@ def run_case(outdir, name):
     os.remove(mrc)
     with open(os.path.join(d, "case.json"), "w") as fh:
         json.dump({"generator": kw, "thickness": thick, "nproj": nproj, "cmd": cmd[1:],
-                   "rc": rc, "wall_s": wall}, fh, indent=1)
+                   "rc": rc, "wall_s": wall, "perturbation_seed": pert}, fh, indent=1)
     print(name, "rc", rc, "wall", round(wall, 2), flush=True)
     return rc
 
@@ -167,7 +185,9 @@ def write_fixtures(outdir, name):
         events = parse_log(fh.read())
     al = np.load(os.path.join(d, "aligned.npz"))
     fx = {"case": name, "generator": case["generator"], "thickness": case["thickness"],
-          "nproj": case["nproj"], "cmd": case["cmd"], "events": events,
+          "nproj": case["nproj"], "cmd": case["cmd"],
+          "perturbation_seed": case.get("perturbation_seed"), "wall_s": case.get("wall_s"),
+          "events": events,
           "params": parse_txt(os.path.join(d, "ref.txt")),
           "aligned_slice_sum": al["slice_sum"].tolist(),
           "aligned_slice_sq": al["slice_sq"].tolist()}
@@ -188,6 +208,8 @@ def main():
         return 0
     outdir = sys.argv[1]
     names = sys.argv[2:] or list(CASES)
+    for n in names:
+        case_spec(n)  # unknown names fail before any run
     rc = 0
     for n in names:
         rc |= run_case(outdir, n)
