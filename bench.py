@@ -302,9 +302,12 @@ def run_ours(args):
         last["passes"] = int(passes[0])
         last["axis"] = float(ps[0].rotate[0])
 
+    log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
+    log(f"workload ready {nx}x{ny}x{nz}, batch {B}")
     for _ in range(args.warmup):
         step()
     barrier()
+    log("warm-up done")
     l0 = ctx.kernel_launches()
     with ClockSampler(dev) as clk:
         ms = _time_steps(stream, step, args.steps)
@@ -332,10 +335,17 @@ def run_ours(args):
             for d in d_outs:
                 h_out.copy_(d, non_blocking=True)
 
+    log("batched timing done")
     step_e2e()
     barrier()
     e_ms = _time_steps(stream, step_e2e, args.steps)
-    del d_ins
+    log("e2e timing done")
+    h2d_bytes = int(s.stack.nbytes) * B
+    d2h_bytes = int(h_out.numel() * 4 + 3 * nz * 4) * B
+    # the pinned buffers recorded their copies on the library's stream: release them
+    # while that stream exists
+    del d_ins, h_raw, h_out, step_e2e
+    torch.cuda.synchronize()
     # the plain path: one series at a time, FP32 (the reference's arithmetic)
     kw32 = dict(kw, precision=PRECISIONS["fp32"])
     d_one = d_outs[0]
@@ -347,6 +357,7 @@ def run_ours(args):
         step_plain()
     barrier()
     pl_ms = _time_steps(stream, step_plain, args.steps)
+    log("plain timing done")
     t = torch.tensor([ms, e_ms, pl_ms], dtype=torch.float64, device=f"cuda:{dev}")
     if pg is not None:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -387,20 +398,23 @@ def run_ours(args):
             "data": "synthetic (seeded phantom series, BASELINE shapes)",
             "config": cfg,
             "e2e": {"value": e2e_value, "unit": "series/min",
-                    "h2d_bytes_per_step": int(s.stack.nbytes) * B,
-                    "d2h_bytes_per_step": int(h_out.numel() * 4 + 3 * nz * 4) * B},
+                    "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
             "plain": {"value": plain_value, "unit": "series/min",
                       "what": "one series at a time, FP32 operands (mf_align_device)"},
             "batched_over_plain": value / plain_value,
             "gpu_launches": int(launches), "passes_per_series": last.get("passes"),
             "roofline": roof, "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_serve:
+        log("serving run")
         line["served"] = served_run(mf, s, dev, args.serve_requests, value / world)
+        log("serving run done")
         line["served_over_plain"] = line["served"]["series_per_min"] / plain_value
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(s, passes=max(last.get("passes", 1), 1))
     if rank == 0:
         print(json.dumps(line), flush=True)
+    del d_outs, d_one, d_raw
+    torch.cuda.synchronize()
     ctx.close()
     if pg is not None:
         pg.barrier()
@@ -429,6 +443,9 @@ def run_kernel_case(args):
     out = torch.empty((ny, nx), device="cuda", dtype=torch.float32)
     if args.kernel_case == "axis":
         ser = mf.Series(ctx, s.stack, ang)
+        p = ser.get_param()
+        p.rotate[:] = s.axis  # candidates around the true axis, as in the refinements
+        ser.set_param(p)
         for _ in range(args.steps):
             ser.tilt_axis(20.0)
         ctx.sync()

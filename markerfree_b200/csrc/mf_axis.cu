@@ -13,6 +13,24 @@
 
 namespace mf {
 
+// Arithmetic of the reference's device code.  nvcc contracts a*b + c into one
+// fused multiply-add (its default), taking the first product of a sum of two
+// products as the fused one: x*c - y*s + o becomes fma(x, c, -(y*s)) + o.  The
+// candidate angles' sine and cosine are CUDA's sinf/cosf of the same float
+// argument, as in the reference.  Emulating both keeps the sampled pixels and
+// the line values those of the reference binary.
+__device__ __forceinline__ float lin2(float x, float c, float yprod, float o) {
+  return __fadd_rn(__fmaf_rn(x, c, yprod), o);
+}
+
+// cs[b] = (cosf(a), sinf(a)), a = rot[b] * 3.1415926f / 180.0f (Rotate.cu:16-18, 50-52)
+__global__ void k_axis_cs(const float* __restrict__ rot, int num, float2* __restrict__ cs) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= num) return;
+  const float a = __fdiv_rn(__fmul_rn(rot[b], 3.1415926f), 180.0f);
+  cs[b] = make_float2(cosf(a), sinf(a));
+}
+
 // GCalcCommonRegion (Rotate.cu:9-40); entries whose first step already leaves
 // the image stay 0 here (the reference leaves them unset).
 __global__ void k_common_region(int width, int height, int L, const float2* __restrict__ cs,
@@ -22,20 +40,21 @@ __global__ void k_common_region(int width, int height, int L, const float2* __re
   int i = blockIdx.x * L + y;
   float fsin = cs[blockIdx.x].y, fcos = cs[blockIdx.x].x;
   int half = L / 2;
-  float ox = __fadd_rn(__fmul_rn((float)width, 0.5f), shift_x);
-  float oy = __fadd_rn(__fmul_rn((float)height, 0.5f), shift_y);
-  float fy = __fsub_rn((float)y, __fmul_rn((float)L, 0.5f));
+  float ox = __fmaf_rn((float)width, 0.5f, shift_x);
+  float oy = __fmaf_rn((float)height, 0.5f, shift_y);
+  float fy = __fmaf_rn(-(float)L, 0.5f, (float)y);
+  const float ys = -__fmul_rn(fy, fsin), yc = __fmul_rn(fy, fcos);
   int left = 0, right = 0;
   for (int x = 1; x < half; ++x) {
-    float X = __fadd_rn(__fsub_rn(__fmul_rn((float)(-x), fcos), __fmul_rn(fy, fsin)), ox);
-    float Y = __fadd_rn(__fadd_rn(__fmul_rn((float)(-x), fsin), __fmul_rn(fy, fcos)), oy);
+    float X = lin2((float)(-x), fcos, ys, ox);
+    float Y = lin2((float)(-x), fsin, yc, oy);
     if (X < 0 || X >= width) break;
     if (Y < 0 || Y >= height) break;
     left = -x;
   }
   for (int x = 1; x < half; ++x) {
-    float X = __fadd_rn(__fsub_rn(__fmul_rn((float)x, fcos), __fmul_rn(fy, fsin)), ox);
-    float Y = __fadd_rn(__fadd_rn(__fmul_rn((float)x, fsin), __fmul_rn(fy, fcos)), oy);
+    float X = lin2((float)x, fcos, ys, ox);
+    float Y = lin2((float)x, fsin, yc, oy);
     if (X < 0 || X >= width) break;
     if (Y < 0 || Y >= height) break;
     right = x;
@@ -44,7 +63,49 @@ __global__ void k_common_region(int width, int height, int L, const float2* __re
   region[2 * i + 1] = right;
 }
 
-// GRadon (Rotate.cu:42-95) for every tilt z = blockIdx.z.
+// Sample coordinates of GRadon (Rotate.cu:62-63, 76-77): X = x cos - y sin + ox,
+// Y = x sin + y cos + oy, contracted as the reference's device code is.
+struct RadonLine {
+  float c, s, ys, yc, ox, oy;  // ys = -(y sin), yc = y cos
+  __device__ __forceinline__ float X(float fx) const { return lin2(fx, c, ys, ox); }
+  __device__ __forceinline__ float Y(float fx) const { return lin2(fx, s, yc, oy); }
+};
+
+// Smallest x in [a, b) with pred(x), for a predicate that is false then true
+// along x; b when it is never true.
+template <class P>
+__device__ __forceinline__ int first_true(int a, int b, P pred) {
+  while (a < b) {
+    const int m = a + ((b - a) >> 1);
+    if (pred(m))
+      b = m;
+    else
+      a = m + 1;
+  }
+  return a;
+}
+
+// Sub-interval of [a, b) on which 0 <= f(x) < lim, for f = rounded (x k + consts):
+// f is monotone in x (non-decreasing for k >= 0, non-increasing for k < 0) because
+// every step (the fused x k + c, then + o) is a correctly rounded monotone
+// operation, so the set is an interval.
+template <class F>
+__device__ __forceinline__ void in_range(int* a, int* b, float k, float lim, F f) {
+  if (*a >= *b) return;
+  if (k >= 0.0f) {
+    *a = first_true(*a, *b, [&](int x) { return f((float)x) >= 0.0f; });
+    *b = first_true(*a, *b, [&](int x) { return !(f((float)x) < lim); });
+  } else {
+    *a = first_true(*a, *b, [&](int x) { return f((float)x) < lim; });
+    *b = first_true(*a, *b, [&](int x) { return !(f((float)x) >= 0.0f); });
+  }
+}
+
+// GRadon (Rotate.cu:42-95) for every tilt z = blockIdx.z.  The samples that fall
+// inside the image form one interval of x (the coordinates are monotone in x), so
+// it is found once per line by bisection on the same rounded expressions and the
+// loop then runs without bounds tests; the samples taken and their order (left
+// to right, as the reference's two loops) are unchanged.
 __global__ void k_radon(const float* __restrict__ stack, int width, int height, int L, int num,
                         const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
                         const float* __restrict__ sxs, const float* __restrict__ sys,
@@ -54,31 +115,32 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   int z = blockIdx.z;
   if (y >= L) return;
   const float* proj = stack + (size_t)z * width * height;
-  float fsr = cs[b].y, fcr = cs[b].x;
-  float fy = __fsub_rn((float)y, __fmul_rn((float)L, 0.5f));
-  float ox = __fadd_rn(__fmul_rn((float)width, 0.5f), sxs[z]);
-  float oy = __fadd_rn(__fmul_rn((float)height, 0.5f), sys[z]);
-  float fc = tilt_cos[z];
-  int i = b * L + y;
+  RadonLine ln;
+  ln.s = cs[b].y;
+  ln.c = cs[b].x;
+  const float fy = __fmaf_rn(-(float)L, 0.5f, (float)y);
+  ln.ox = __fmaf_rn((float)width, 0.5f, sxs[z]);
+  ln.oy = __fmaf_rn((float)height, 0.5f, sys[z]);
+  ln.ys = -__fmul_rn(fy, ln.s);
+  ln.yc = __fmul_rn(fy, ln.c);
+  const float fc = tilt_cos[z];
+  const int i = b * L + y;
+  // left <= 0 <= right, so one loop visits the reference's two loops in order
+  int lo = (int)__fmaf_rn((float)region[2 * i], fc, 0.5f);
+  int hi = (int)__fmaf_rn((float)region[2 * i + 1], fc, 0.5f);
+  const float fw = (float)width, fh = (float)height;
+  in_range(&lo, &hi, ln.c, fw, [&](float fx) { return ln.X(fx); });
+  in_range(&lo, &hi, ln.s, fh, [&](float fx) { return ln.Y(fx); });
   float sum = 0.0f;
   int cnt = 0;
-  int left = (int)__fadd_rn(__fmul_rn((float)region[2 * i], fc), 0.5f);
-  int right = (int)__fadd_rn(__fmul_rn((float)region[2 * i + 1], fc), 0.5f);
-  // left <= 0 <= right, so one loop visits the reference's two loops in order;
-  // fy*sin and fy*cos are loop invariant with the same rounding as the reference.
-  // The float copy of x is stepped by 1.0 (exact below 2^24) instead of converted,
-  // and the in-range coordinates (0 <= X < 2^23) are truncated by a round-toward-
-  // zero add of 2^23, which gives the same integer as (int)X.
-  const float ys = __fmul_rn(fy, fsr), yc = __fmul_rn(fy, fcr);
-  const float fw = (float)width, fh = (float)height;
-  float fx = (float)left;
-  for (int x = left; x < right; ++x, fx = __fadd_rn(fx, 1.0f)) {
-    float X = __fadd_rn(__fsub_rn(__fmul_rn(fx, fcr), ys), ox);
-    float Y = __fadd_rn(__fadd_rn(__fmul_rn(fx, fsr), yc), oy);
-    if (!(X >= 0.0f && X < fw && Y >= 0.0f && Y < fh)) continue;
-    int ix = __float_as_int(__fadd_rz(X, 8388608.0f)) - 0x4B000000;
-    int iy = __float_as_int(__fadd_rz(Y, 8388608.0f)) - 0x4B000000;
-    float v = __ldg(proj + (size_t)iy * width + ix);
+  // in-range coordinates (0 <= X < 2^23) are truncated by a round-toward-zero add
+  // of 2^23, which gives the same integer as (int)X
+  float fx = (float)lo;
+#pragma unroll 4
+  for (int x = lo; x < hi; ++x, fx = __fadd_rn(fx, 1.0f)) {
+    const int ix = __float_as_int(__fadd_rz(ln.X(fx), 8388608.0f)) - 0x4B000000;
+    const int iy = __float_as_int(__fadd_rz(ln.Y(fx), 8388608.0f)) - 0x4B000000;
+    const float v = __ldg(proj + (size_t)iy * width + ix);
     if (v < 0) continue;
     sum = __fadd_rn(sum, v);
     cnt++;
@@ -86,33 +148,35 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   lines[((size_t)z * num + b) * (L + 2) + y] = (cnt == 0) ? kSentinel : __fdiv_rn(sum, (float)cnt);
 }
 
-// GCalcMean + GRemoveMean (Rotate.cu:97-157) for one line per block.
-__global__ void k_line_prep(float* __restrict__ lines, int L) {
-  __shared__ double s_sum[256];
-  __shared__ int s_cnt[256];
+// GCalcMean + GRemoveMean (Rotate.cu:97-157) for one line per block of 512
+// threads: float partial sums over x = tid, tid + 512, ..., then the same
+// shared-memory tree; the window's cosine is CUDA's cosf of the same argument.
+__global__ void __launch_bounds__(512) k_line_prep(float* __restrict__ lines, int L) {
+  __shared__ float s_sum[512];
+  __shared__ int s_cnt[512];
   float* p = lines + (size_t)blockIdx.x * (L + 2);
-  double a = 0.0;
+  float a = 0.0f;
   int n = 0;
   for (int y = threadIdx.x; y < L; y += blockDim.x) {
     float v = p[y];
     if (v > -1e10f) {
-      a += v;
+      a = __fadd_rn(a, v);
       n++;
     }
   }
   s_sum[threadIdx.x] = a;
   s_cnt[threadIdx.x] = n;
   __syncthreads();
-  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+  for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
     if (threadIdx.x < h) {
-      s_sum[threadIdx.x] += s_sum[threadIdx.x + h];
+      s_sum[threadIdx.x] = __fadd_rn(s_sum[threadIdx.x], s_sum[threadIdx.x + h]);
       s_cnt[threadIdx.x] += s_cnt[threadIdx.x + h];
     }
     __syncthreads();
   }
-  float mean = s_cnt[0] == 0 ? 0.0f : (float)(s_sum[0] / s_cnt[0]);
+  const float mean = s_cnt[0] == 0 ? 0.0f : __fdiv_rn(s_sum[0], (float)s_cnt[0]);
   __syncthreads();
-  float half = __fmul_rn(0.5f, (float)L);
+  const float half = __fmul_rn(0.5f, (float)L);
   for (int y = threadIdx.x; y < L; y += blockDim.x) {
     float v = p[y];
     if (v < 0)
@@ -120,7 +184,7 @@ __global__ void k_line_prep(float* __restrict__ lines, int L) {
     else
       v = __fsub_rn(v, mean);
     float fr = __fdiv_rn(fabsf(__fsub_rn((float)y, half)), half);
-    fr = __fmul_rn(0.5f, __fsub_rn(1.0f, (float)cos((double)(float)(3.14159 * (double)fr))));
+    fr = __fmul_rn(0.5f, __fsub_rn(1.0f, cosf((float)(3.14159 * (double)fr))));
     fr = __fsub_rn(1.0f, powf(fr, 100.0f));
     p[y] = __fmul_rn(v, __fmul_rn(fr, fr));
   }
@@ -141,37 +205,78 @@ __global__ void k_axis_sum(const cufftComplex* __restrict__ spec, int nz, int nu
   sum[(size_t)b * cmp + k] = make_cuComplex(re, im);
 }
 
-// GConv (1-D, B = 10) + GSum (Rotate.cu:179-251) for (candidate b, tilt z).
-__global__ void k_axis_cc(const cufftComplex* __restrict__ spec,
-                          const cufftComplex* __restrict__ sum, int nz, int num, int cmp,
-                          float* __restrict__ cc_out) {
-  __shared__ double s_cc[128], s_sd[128];
-  int b = blockIdx.x, z = blockIdx.y;
+// GConv (1-D, B = 10) + GSum (Rotate.cu:179-251) for (candidate b, tilt z), with
+// the reference's partition: GConv blocks of blockDim (= CalcWarps(cmp) * 32)
+// threads, one element per thread, a float tree per block; then GSum over the
+// block partials with gsum_threads threads (strided float sums, then a tree).
+__global__ void __launch_bounds__(512) k_axis_cc(const cufftComplex* __restrict__ spec,
+                                                 const cufftComplex* __restrict__ sum, int nz,
+                                                 int num, int cmp, int gsum_threads,
+                                                 float* __restrict__ cc_out) {
+  __shared__ float s_cc[512], s_sd[512];
+  __shared__ float p_cc[64], p_sd[64];
+  const int b = blockIdx.x, z = blockIdx.y;
   const cufftComplex* line = spec + ((size_t)z * num + b) * cmp;
   const cufftComplex* sm = sum + (size_t)b * cmp;
-  double cc = 0.0, sd = 0.0;
-  for (int k = 1 + threadIdx.x; k < cmp; k += blockDim.x) {
-    cufftComplex l = line[k], s = sm[k];
-    float rr = __fsub_rn(s.x, l.x), ri = __fsub_rn(s.y, l.y);  // sum*1 + line*(-1)
-    float f = __fdiv_rn((float)k, __fmul_rn(2.0f, (float)(cmp - 1)));
-    f = (float)exp((double)__fmul_rn(__fmul_rn(-20.0f, f), f));
-    float a1 = sqrtf(__fadd_rn(__fmul_rn(rr, rr), __fmul_rn(ri, ri)));
-    float a2 = sqrtf(__fadd_rn(__fmul_rn(l.x, l.x), __fmul_rn(l.y, l.y)));
-    float num_ = __fmul_rn(__fadd_rn(__fmul_rn(l.x, rr), __fmul_rn(l.y, ri)), f);
-    cc += (double)__fdiv_rn(num_, __fadd_rn(__fmul_rn(a1, a2), 1e-20f));
-    sd += (double)f;
-  }
-  s_cc[threadIdx.x] = cc;
-  s_sd[threadIdx.x] = sd;
-  __syncthreads();
-  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-    if (threadIdx.x < h) {
-      s_cc[threadIdx.x] += s_cc[threadIdx.x + h];
-      s_sd[threadIdx.x] += s_sd[threadIdx.x + h];
+  const int bs = blockDim.x, tid = threadIdx.x;
+  const int nblk = cmp / bs + 1;
+  for (int vb = 0; vb < nblk; ++vb) {
+    const int i = vb * bs + tid;
+    float cc = 0.0f, sd = 0.0f;
+    if (i < cmp && i != 0) {
+      const cufftComplex l = line[i], s = sm[i];
+      const float rx = __fsub_rn(s.x, l.x), ry = __fsub_rn(s.y, l.y);  // sum*1 + line*(-1)
+      float f = __fdiv_rn((float)i, __fmul_rn(2.0f, (float)(cmp - 1)));
+      f = expf(__fmul_rn(__fmul_rn(-20.0f, f), f));
+      const float a1 = sqrtf(__fmaf_rn(rx, rx, __fmul_rn(ry, ry)));
+      const float a2 = sqrtf(__fmaf_rn(l.x, l.x, __fmul_rn(l.y, l.y)));
+      const float dot = __fmaf_rn(l.x, rx, __fmul_rn(l.y, ry));
+      cc = __fdiv_rn(__fmul_rn(dot, f), __fmaf_rn(a1, a2, 1e-20f));
+      sd = f;
+    }
+    s_cc[tid] = cc;
+    s_sd[tid] = sd;
+    __syncthreads();
+    for (int h = bs >> 1; h > 0; h >>= 1) {
+      if (tid < h) {
+        s_cc[tid] = __fadd_rn(s_cc[tid], s_cc[tid + h]);
+        s_sd[tid] = __fadd_rn(s_sd[tid], s_sd[tid + h]);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      p_cc[vb] = s_cc[0];
+      p_sd[vb] = s_sd[0];
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) cc_out[(size_t)b * nz + z] = __fdiv_rn((float)s_cc[0], (float)s_sd[0]);
+  // GSum over the nblk partials
+  float cc = 0.0f, sd = 0.0f;
+  if (tid < gsum_threads)
+    for (int x = tid; x < nblk; x += gsum_threads) {
+      cc = __fadd_rn(cc, p_cc[x]);
+      sd = __fadd_rn(sd, p_sd[x]);
+    }
+  s_cc[tid] = cc;
+  s_sd[tid] = sd;
+  __syncthreads();
+  for (int h = gsum_threads >> 1; h > 0; h >>= 1) {
+    if (tid < h) {
+      s_cc[tid] = __fadd_rn(s_cc[tid], s_cc[tid + h]);
+      s_sd[tid] = __fadd_rn(s_sd[tid], s_sd[tid + h]);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) cc_out[(size_t)b * nz + z] = __fdiv_rn(s_cc[0], s_sd[0]);
+}
+
+// CalcTIltAxis::CalcWarps (Rotate.cu:563-572), host arithmetic as in the reference.
+static int calc_warps(int size, int warp) {
+  float fw = size / (float)warp;
+  if (fw < 1.5f) return 1;
+  int e = (int)(logf(fw) / logf(2.0f) + 0.5f);
+  int w = 1 << e;
+  return w > 16 ? 16 : w;
 }
 
 __global__ void k_axis_score(const float* __restrict__ cc, int nz, int num,
@@ -184,7 +289,7 @@ __global__ void k_axis_score(const float* __restrict__ cc, int nz, int num,
 }
 
 struct AxisBuffers {
-  DevBuf cs, tcos, sx, sy, region, lines, sum, cc, score;
+  DevBuf rot, cs, tcos, sx, sy, region, lines, sum, cc, score;
 };
 
 int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, int ny, int nz,
@@ -193,11 +298,6 @@ int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, i
                      int L, std::vector<float>* scores, cudaStream_t st) {
   const int cmp = L / 2 + 1;
   AxisBuffers B;
-  std::vector<float2> cs(num);
-  for (int b = 0; b < num; ++b) {
-    float a = rot_cand[b] * 3.1415926f / 180.0f;
-    cs[b] = make_float2(cos_f(a), sin_f(a));
-  }
   std::vector<float> tc(nz);
   for (int z = 0; z < nz; ++z) tc[z] = (float)std::cos(angles[z] * kD2R);
   MF_TRY(B.cs.alloc(sizeof(float2) * num));
@@ -209,7 +309,10 @@ int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, i
   MF_TRY(B.sum.alloc(sizeof(cufftComplex) * (size_t)num * cmp));
   MF_TRY(B.cc.alloc(sizeof(float) * (size_t)num * nz));
   MF_TRY(B.score.alloc(sizeof(float) * num));
-  MF_CHECK_CUDA(cudaMemcpyAsync(B.cs.p, cs.data(), sizeof(float2) * num, cudaMemcpyHostToDevice, st));
+  MF_TRY(B.rot.alloc(sizeof(float) * num));
+  MF_CHECK_CUDA(cudaMemcpyAsync(B.rot.p, rot_cand, sizeof(float) * num, cudaMemcpyHostToDevice, st));
+  k_axis_cs<<<(num + 127) / 128, 128, 0, st>>>(B.rot.as<float>(), num, B.cs.as<float2>());
+  c->launches++;
   MF_CHECK_CUDA(cudaMemcpyAsync(B.tcos.p, tc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(B.sx.p, sx, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(B.sy.p, sy, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
@@ -218,15 +321,19 @@ int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, i
   k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
       stack, nx, ny, L, num, B.cs.as<float2>(), B.tcos.as<float>(), B.sx.as<float>(),
       B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>());
-  k_line_prep<<<nz * num, 256, 0, st>>>(B.lines.as<float>(), L);
+  k_line_prep<<<nz * num, 512, 0, st>>>(B.lines.as<float>(), L);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   MF_CHECK_CUFFT(cufftExecR2C(plan, B.lines.as<cufftReal>(), B.lines.as<cufftComplex>()));
   const cufftComplex* spec = B.lines.as<cufftComplex>();
   k_axis_sum<<<dim3((cmp + 127) / 128, num), 128, 0, st>>>(spec, nz, num, cmp,
                                                             B.sum.as<cufftComplex>());
-  k_axis_cc<<<dim3(num, nz), 128, 0, st>>>(spec, B.sum.as<cufftComplex>(), nz, num, cmp,
-                                           B.cc.as<float>());
+  const int bs = calc_warps(cmp, 32) * 32;
+  const int nblk = cmp / bs + 1;
+  if (nblk > 64) return set_error(MF_ERR_ARG, "tilt axis: line of %d bins too long", L);
+  const int gs = calc_warps(nblk, 32) * 32;
+  k_axis_cc<<<dim3(num, nz), bs, 0, st>>>(spec, B.sum.as<cufftComplex>(), nz, num, cmp, gs,
+                                          B.cc.as<float>());
   k_axis_score<<<(num + 127) / 128, 128, 0, st>>>(B.cc.as<float>(), nz, num, B.score.as<float>());
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
