@@ -22,6 +22,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + os.path.join(ROOT, "include")] + ARCH
+if os.environ.get("MF_HOST_DEBUG"):  # host debug information (backtraces, addr2line)
+    CFLAGS += ["-Xcompiler", "-g"]
 LIB_SOURCES = ["mf_common.cpp", "mf_io.cpp", "mf_capi.cpp", "mf_correct.cu", "mf_reproj.cu",
                "mf_reproj_tc.cu", "mf_xcorr.cu", "mf_axis.cu", "mf_series.cu", "mf_batch.cu", "mf_serve.cpp",
                "mf_noalloc.cu"]

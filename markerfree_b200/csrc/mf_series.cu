@@ -13,13 +13,20 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "mf_series.hpp"
 #include "mf_xcorr.hpp"
 
 using namespace mf;
 
+// cuFFT plan creation and destruction are serialised across the process: plans
+// created at the same time from several threads (the serving workers) crashed
+// inside cuFFT's planner.  Execution on distinct plans needs no lock.
+static std::mutex g_plan_mu;
+
 mf_context::~mf_context() {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
   for (auto& kv : plans) cufftDestroy(kv.second);
   plans.clear();
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -33,6 +40,7 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   }
   // key: kind (0 rows R2C in place, 1 rows C2R out of place, 2 2-D R2C in place,
   //            3 2-D C2R in place), nx, ny, batch
+  std::lock_guard<std::mutex> lk(g_plan_mu);
   long long kind = key[0];
   int nx = (int)key[1], ny = (int)key[2], batch = (int)key[3];
   int pad = (nx / 2 + 1) * 2, cmp = nx / 2 + 1;

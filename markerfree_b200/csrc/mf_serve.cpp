@@ -57,6 +57,14 @@ struct Job {
   double t_submit = 0, t_admit = 0, t_ready = 0, t_done = 0;
 };
 
+// Requests that may share a group: same shape and the same options of the
+// projection-matching stage (which a group applies to all its series).
+std::vector<float> group_key(const Job* j) {
+  return {(float)j->nx,          (float)j->ny,        (float)j->nz,
+          (float)j->opt.precision, (float)j->opt.align_z, (float)j->opt.nproj,
+          j->opt.zshift,         (float)j->opt.out_bin};
+}
+
 // Device bytes a request may hold at its peak: the pre-processed stack, the
 // matching buffers (corrected stack, row-FFT scratch, 16-bit copy, operators)
 // and a device copy of the aligned output.
@@ -113,16 +121,14 @@ struct mf_server {
     group->clear();
     *wait_s = 0.25;
     const double t = now_s();
-    // ready jobs grouped by shape and precision, oldest first
-    std::map<std::vector<int>, std::vector<Job*>> by_shape;
-    for (Job* j : ready) by_shape[{j->nx, j->ny, j->nz, j->opt.precision}].push_back(j);
-    auto coming = [&](const std::vector<int>& key) {
+    // ready jobs grouped by shape and by the options a group shares, oldest first
+    std::map<std::vector<float>, std::vector<Job*>> by_shape;
+    for (Job* j : ready) by_shape[group_key(j)].push_back(j);
+    auto coming = [&](const std::vector<float>& key) {
       for (Job* j : admitted)
-        if (j->nx == key[0] && j->ny == key[1] && j->nz == key[2] && j->opt.precision == key[3])
-          return true;
+        if (group_key(j) == key) return true;
       for (Job* j : queued)
-        if (j->nx == key[0] && j->ny == key[1] && j->nz == key[2] && j->opt.precision == key[3])
-          return true;
+        if (group_key(j) == key) return true;
       return preparing > 0;
     };
     for (auto& kv : by_shape) {
