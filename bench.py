@@ -310,15 +310,19 @@ def run_ours(args):
     log("warm-up done")
     l0 = ctx.kernel_launches()
     with ClockSampler(dev) as clk:
+        torch.cuda.nvtx.range_push("timed")  # profilers select this range (ncu --nvtx)
         ms = _time_steps(stream, step, args.steps)
         barrier()
+        torch.cuda.nvtx.range_pop()
         launches = ctx.kernel_launches() - l0
         # one more step with per-stage CUDA events on the library's stream (passes then
         # launch kernels one by one instead of replaying the graph; same kernels)
         ctx.set_profiling(True)
         ctx.stage_times()
+        ctx.stage_breakdown()
         p_ms = _time_steps(stream, step, 1)
         st = ctx.stage_times()
+        stages = ctx.stage_breakdown()
         ctx.set_profiling(False)
     # e2e through the C ABI with host buffers: per step B uploads from pinned memory,
     # the group alignment, B downloads of the aligned stacks
@@ -403,6 +407,7 @@ def run_ours(args):
                       "what": "one series at a time, FP32 operands (mf_align_device)"},
             "batched_over_plain": value / plain_value,
             "gpu_launches": int(launches), "passes_per_series": last.get("passes"),
+            "stage_ms_per_step": {k: round(v, 2) for k, v in stages.items()},
             "roofline": roof, "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_serve:
         log("serving run")

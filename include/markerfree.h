@@ -126,6 +126,10 @@ MF_API int mf_transform_doit(mf_series* s, float* max_err);
 /* CalcTIltAxis::DoIt (Markerfree/src/method/Rotate.cu:292-337): common-line search
  * over `num` candidate axes spanning `range` degrees; sets rotate[] for all tilts. */
 MF_API int mf_tilt_axis(mf_series* s, float range, int num, float* axis_out);
+/* mf_tilt_axis that also returns the score of each of the `num` candidates (the
+ * common-line scores CalcTIltAxis::findTiltAxis ranks, Rotate.cu:468-528). */
+MF_API int mf_tilt_axis_scores(mf_series* s, float range, int num, float* axis_out,
+                               float* scores);
 /* FindOffset::DoIt (Markerfree/src/method/FindOffset.cu:85-96): adds the best of
  * 31 one-degree tilt-angle offsets to param.angle_offset. */
 MF_API int mf_find_offset(mf_series* s, float* offset_out);
@@ -136,6 +140,10 @@ MF_API int mf_projalign_setup(mf_series* s, float zshift, int align_z, int nproj
 MF_API int mf_projalign_doit(mf_series* s, float* max_err);
 /* Rotation-centre z of the last pass (ProjAlign.cpp:459-486). */
 MF_API int mf_projalign_z0(mf_series* s, float* z0);
+/* Shifts measured in the last pass, xy[2*z], xy[2*z+1] for tilt z: un-binned px
+ * before the rotation by the tilt axis, the values ProjAlign.cpp:203 prints
+ * (zero for the zero tilt and for tilts not yet measured). */
+MF_API int mf_projalign_measured(mf_series* s, float* xy);
 /* Process::mCoarseAlign (Markerfree/src/main/Process.cpp:238-270); applies the
  * offset to the series' angles as the reference does. */
 MF_API int mf_coarse_align(mf_series* s, float pitch_angle, float offset);
@@ -169,6 +177,18 @@ MF_API int mf_align_device(mf_context* ctx, const float* d_raw_stack, int nx, in
  * written, banded operator read), [5] re-projection multiply-adds. */
 MF_API int mf_context_set_profiling(mf_context* ctx, int on);
 MF_API int mf_context_stage_times(mf_context* ctx, double* out6);
+/* Wall time per stage of the alignments run while stage timing was on (CUDA
+ * events on the context's stream; each stage waits for its work), accumulated
+ * since the last call and then reset, in ms: [0] series creation (upload,
+ * pre-processing), [1] coarse alignment (stretch correlations, offset search),
+ * [2] tilt-axis searches, [3] projection-matching set-up, [4] projection-matching
+ * passes, [5] aligned-stack output. */
+MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out6);
+/* Diagnostic: CUDA's cosf and sinf of each of n float arguments (host arrays),
+ * the values the kernels use where the reference's device code calls them.  A
+ * CPU model of the path needs them to take the same nearest-neighbour decisions,
+ * since they may differ from the correctly rounded values in the last place. */
+MF_API int mf_device_cos_sin(mf_context* ctx, const float* x, int n, float* c, float* s);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work or timing events after the library's. */
 MF_API void* mf_context_stream(mf_context* ctx);

@@ -79,6 +79,9 @@ SIGNATURES = [
                                           ctypes.c_int]),
     ("mf_projalign_doit", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
     ("mf_projalign_z0", ctypes.c_int, [ctypes.c_void_p, _c_float_p]),
+    ("mf_projalign_measured", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_tilt_axis_scores", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int,
+                                           _c_float_p, _f32p]),
     ("mf_coarse_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float]),
     ("mf_proj_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                      _c_int_p]),
@@ -93,7 +96,10 @@ SIGNATURES = [
     ("mf_context_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mf_context_stage_times", ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_double)]),
+    ("mf_context_stage_breakdown", ctypes.c_int, [ctypes.c_void_p,
+                                                  ctypes.POINTER(ctypes.c_double)]),
     ("mf_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("mf_device_cos_sin", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int, _f32p, _f32p]),
     ("mf_context_set_tc_rows", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mf_group_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                        ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -220,6 +226,22 @@ class Context:
                 "reproj_fma")
         return dict(zip(keys, out))
 
+    def device_cos_sin(self, x):
+        """CUDA's cosf and sinf of each float32 argument (diagnostic)."""
+        x = np.ascontiguousarray(x, np.float32).ravel()
+        c = np.zeros_like(x)
+        s = np.zeros_like(x)
+        _check(lib().mf_device_cos_sin(self.h, x, int(x.size), c, s))
+        return c, s
+
+    def stage_breakdown(self) -> dict:
+        """Wall ms per alignment stage accumulated since the previous call (stage
+        timing on; see set_profiling)."""
+        out = (ctypes.c_double * 6)()
+        _check(lib().mf_context_stage_breakdown(self.h, out))
+        keys = ("prep_ms", "coarse_ms", "axis_ms", "setup_ms", "pass_ms", "output_ms")
+        return dict(zip(keys, out))
+
     def set_tc_rows(self, rows: int):
         """Image rows per tensor-core tile (64, 128, 256; 0 = automatic)."""
         _check(lib().mf_context_set_tc_rows(self.h, int(rows)))
@@ -305,6 +327,13 @@ class Series:
         _check(lib().mf_tilt_axis(self.h, rng, num, ctypes.byref(a)))
         return a.value
 
+    def tilt_axis_scores(self, rng: float, num: int = 100):
+        """tilt_axis that also returns the score of every candidate."""
+        a = ctypes.c_float()
+        sc = np.zeros(num, np.float32)
+        _check(lib().mf_tilt_axis_scores(self.h, rng, num, ctypes.byref(a), sc))
+        return a.value, sc
+
     def find_offset(self) -> float:
         o = ctypes.c_float()
         _check(lib().mf_find_offset(self.h, ctypes.byref(o)))
@@ -326,6 +355,12 @@ class Series:
         z = ctypes.c_float()
         _check(lib().mf_projalign_z0(self.h, ctypes.byref(z)))
         return z.value
+
+    def projalign_measured(self) -> np.ndarray:
+        """(nz, 2) shifts measured in the last pass (un-binned px, before rotation)."""
+        xy = np.zeros(2 * self.nz, np.float32)
+        _check(lib().mf_projalign_measured(self.h, xy))
+        return xy.reshape(-1, 2)
 
     def proj_align(self, zshift: float = 0.0, align_z: int = 600, nproj: int = 10) -> int:
         n = ctypes.c_int()

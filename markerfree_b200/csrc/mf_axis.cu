@@ -23,6 +23,24 @@ __device__ __forceinline__ float lin2(float x, float c, float yprod, float o) {
   return __fadd_rn(__fmaf_rn(x, c, yprod), o);
 }
 
+// CUDA's cosf and sinf of each argument, as the kernels evaluate them.
+__global__ void k_cos_sin(const float* __restrict__ x, int n, float* __restrict__ c,
+                          float* __restrict__ s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  c[i] = cosf(x[i]);
+  s[i] = sinf(x[i]);
+}
+
+int device_cos_sin(Context* ctx, const float* d_x, int n, float* d_c, float* d_s,
+                   cudaStream_t st) {
+  if (n <= 0) return MF_OK;
+  k_cos_sin<<<(n + 255) / 256, 256, 0, st>>>(d_x, n, d_c, d_s);
+  ctx->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 // cs[b] = (cosf(a), sinf(a)), a = rot[b] * 3.1415926f / 180.0f (Rotate.cu:16-18, 50-52)
 __global__ void k_axis_cs(const float* __restrict__ rot, int num, float2* __restrict__ cs) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,12 +119,125 @@ __device__ __forceinline__ void in_range(int* a, int* b, float k, float lim, F f
   }
 }
 
+// Column-major copy of every tilt image: out[z][x][y] = in[z][y][x]; neg[z] is set
+// to 1 when image z holds a value below zero (the caller zeroes neg first).
+__global__ void k_transpose_stack(const float* __restrict__ in, int width, int height,
+                                  float* __restrict__ out, int* __restrict__ neg) {
+  __shared__ float tile[32][33];
+  const size_t pix = (size_t)width * height;
+  const float* src = in + blockIdx.z * pix;
+  float* dst = out + blockIdx.z * pix;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  bool below = false;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int x = x0 + threadIdx.x, y = y0 + j;
+    if (x < width && y < height) {
+      const float v = src[(size_t)y * width + x];
+      below = below || v < 0.0f;
+      tile[j][threadIdx.x] = v;
+    }
+  }
+  if (below) neg[blockIdx.z] = 1;
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int y = y0 + threadIdx.x, x = x0 + j;
+    if (x < width && y < height) dst[(size_t)x * height + y] = tile[threadIdx.x][j];
+  }
+}
+
+int transpose_stack(Context* c, const float* stack, int width, int height, int nz, float* out,
+                    int* neg, cudaStream_t st) {
+  MF_CHECK_CUDA(cudaMemsetAsync(neg, 0, sizeof(int) * nz, st));
+  k_transpose_stack<<<dim3((width + 31) / 32, (height + 31) / 32, nz), dim3(32, 8), 0, st>>>(
+      stack, width, height, out, neg);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Two floats in one 64-bit register, for the packed f32x2 arithmetic of sm_100:
+// each lane of fma.rn.f32x2 / add.rn.f32x2 / add.rz.f32x2 is the scalar IEEE
+// operation with that rounding, so (X, Y) come out bit for bit as from
+// __fmaf_rn / __fadd_rn / __fadd_rz, with one instruction for both coordinates.
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float* a, float* b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(*a), "=f"(*b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma2_rn(unsigned long long a, unsigned long long b,
+                                                      unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
+// Sum and count of the samples x in [lo, hi) of one line, every one of which is
+// inside the image.  kByColumn: pixel (ix, iy) is proj[ix * stride + iy] (the
+// column-major copy, stride = height), else proj[iy * stride + ix] (stride = width).
+// kNonNeg: the image holds no value below zero, so the reference's skip of such
+// samples never fires and every sample counts.
+// An in-range coordinate (0 <= X < 2^23) is truncated by a round-toward-zero add
+// of 2^23: the low bits of the sum are (int)X, and the index is formed from the
+// biased bits in 32-bit modular arithmetic, the bias removed once.
+template <bool kByColumn, bool kNonNeg>
+__device__ __forceinline__ void radon_samples(const float* __restrict__ proj, int stride,
+                                              const RadonLine& ln, int lo, int hi, float* sum_out,
+                                              int* cnt_out) {
+  constexpr unsigned kBias = 0x4B000000u;  // bits of 2^23
+  const unsigned bias_idx = kBias * (unsigned)stride + kBias;  // mod 2^32
+  const unsigned long long cs2 = pack2(ln.c, ln.s), y2 = pack2(ln.ys, ln.yc);
+  const unsigned long long o2 = pack2(ln.ox, ln.oy), big2 = pack2(8388608.0f, 8388608.0f);
+  const unsigned long long one2 = pack2(1.0f, 1.0f);
+  unsigned long long fx2 = pack2((float)lo, (float)lo);
+  float sum = 0.0f;
+  int cnt = 0;
+#pragma unroll 4
+  for (int x = lo; x < hi; ++x) {
+    // X = fma(x, cos, -(y sin)) + ox, Y = fma(x, sin, y cos) + oy, as lin2()
+    const unsigned long long t = add2_rz(add2_rn(fma2_rn(fx2, cs2, y2), o2), big2);
+    fx2 = add2_rn(fx2, one2);
+    float tx, ty;
+    unpack2(t, &tx, &ty);
+    const unsigned bx = __float_as_uint(tx), by = __float_as_uint(ty);
+    const unsigned idx = (kByColumn ? bx * (unsigned)stride + by : by * (unsigned)stride + bx) -
+                         bias_idx;
+    const float v = __ldg(proj + idx);
+    if (!kNonNeg) {
+      if (v < 0) continue;
+      cnt++;
+    }
+    sum = __fadd_rn(sum, v);
+  }
+  *sum_out = sum;
+  *cnt_out = kNonNeg ? max(hi - lo, 0) : cnt;
+}
+
 // GRadon (Rotate.cu:42-95) for every tilt z = blockIdx.z.  The samples that fall
 // inside the image form one interval of x (the coordinates are monotone in x), so
 // it is found once per line by bisection on the same rounded expressions and the
 // loop then runs without bounds tests; the samples taken and their order (left
 // to right, as the reference's two loops) are unchanged.
-__global__ void k_radon(const float* __restrict__ stack, int width, int height, int L, int num,
+//
+// Neighbouring threads take neighbouring lines, whose samples at one x lie one
+// step of (-sin, cos) apart.  For a steep candidate (|sin| >= |cos|) that step
+// runs along an image row, so a warp reads one row segment from the row-major
+// stack; otherwise it runs along a column and the warp reads the column-major copy
+// `stack_t` instead.  Both hold the same values: only the address changes.
+__global__ void k_radon(const float* __restrict__ stack, const float* __restrict__ stack_t,
+                        const int* __restrict__ neg, int width, int height, int L, int num,
                         const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
                         const float* __restrict__ sxs, const float* __restrict__ sys,
                         const int* __restrict__ region, float* __restrict__ lines) {
@@ -114,7 +245,6 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   int b = blockIdx.x;
   int z = blockIdx.z;
   if (y >= L) return;
-  const float* proj = stack + (size_t)z * width * height;
   RadonLine ln;
   ln.s = cs[b].y;
   ln.c = cs[b].x;
@@ -131,19 +261,20 @@ __global__ void k_radon(const float* __restrict__ stack, int width, int height, 
   const float fw = (float)width, fh = (float)height;
   in_range(&lo, &hi, ln.c, fw, [&](float fx) { return ln.X(fx); });
   in_range(&lo, &hi, ln.s, fh, [&](float fx) { return ln.Y(fx); });
-  float sum = 0.0f;
-  int cnt = 0;
-  // in-range coordinates (0 <= X < 2^23) are truncated by a round-toward-zero add
-  // of 2^23, which gives the same integer as (int)X
-  float fx = (float)lo;
-#pragma unroll 4
-  for (int x = lo; x < hi; ++x, fx = __fadd_rn(fx, 1.0f)) {
-    const int ix = __float_as_int(__fadd_rz(ln.X(fx), 8388608.0f)) - 0x4B000000;
-    const int iy = __float_as_int(__fadd_rz(ln.Y(fx), 8388608.0f)) - 0x4B000000;
-    const float v = __ldg(proj + (size_t)iy * width + ix);
-    if (v < 0) continue;
-    sum = __fadd_rn(sum, v);
-    cnt++;
+  const size_t off = (size_t)z * width * height;
+  float sum;
+  int cnt;
+  const bool nonneg = neg != nullptr && neg[z] == 0;
+  if (stack_t != nullptr && fabsf(ln.c) > fabsf(ln.s)) {  // uniform over the block
+    if (nonneg)
+      radon_samples<true, true>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
+    else
+      radon_samples<true, false>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
+  } else {
+    if (nonneg)
+      radon_samples<false, true>(stack + off, width, ln, lo, hi, &sum, &cnt);
+    else
+      radon_samples<false, false>(stack + off, width, ln, lo, hi, &sum, &cnt);
   }
   lines[((size_t)z * num + b) * (L + 2) + y] = (cnt == 0) ? kSentinel : __fdiv_rn(sum, (float)cnt);
 }
@@ -292,8 +423,8 @@ struct AxisBuffers {
   DevBuf rot, cs, tcos, sx, sy, region, lines, sum, cc, score;
 };
 
-int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, int ny, int nz,
-                     const float* angles,
+int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, const float* stack_t,
+                     const int* d_neg, int nx, int ny, int nz, const float* angles,
                      const float* sx, const float* sy, int zt, const float* rot_cand, int num,
                      int L, std::vector<float>* scores, cudaStream_t st) {
   const int cmp = L / 2 + 1;
@@ -319,8 +450,8 @@ int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, i
   k_common_region<<<dim3(num, (L + 127) / 128), dim3(1, 128), 0, st>>>(
       nx, ny, L, B.cs.as<float2>(), sx[zt], sy[zt], B.region.as<int>());
   k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
-      stack, nx, ny, L, num, B.cs.as<float2>(), B.tcos.as<float>(), B.sx.as<float>(),
-      B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>());
+      stack, stack_t, d_neg, nx, ny, L, num, B.cs.as<float2>(), B.tcos.as<float>(),
+      B.sx.as<float>(), B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>());
   k_line_prep<<<nz * num, 512, 0, st>>>(B.lines.as<float>(), L);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());

@@ -36,7 +36,7 @@ struct mf_group {
   DevBuf d_maxerr, d_z0, d_err, d_meas, d_tcerr;
   // device buffers (series-major, contiguous over the group)
   DevBuf corr, scratch, corr16, tflags, rowflags, reproj, cc, recorr, recorr_out;
-  DevBuf mpart, stats, ppart;
+  DevBuf mpart, stats, ppart, mask;
   ReprojOpSet ops;
   TcOpSet tcops;
   TmaDesc imgmap;
@@ -71,6 +71,7 @@ __global__ void k_group_scatter(const float* __restrict__ src, const GroupSeries
 }
 
 static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
+  StageTimer timer(&g->ctx->c, kStageSetup);
   Context* c = &g->ctx->c;
   cudaStream_t st = c->stream;
   const int B = g->B, nx = g->nx, ny = g->ny, nz = g->nz;
@@ -103,6 +104,7 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     zts[b] = zt;
     std::vector<unsigned char> skip(nz, 1);
     skip[zt] = 0;
+    std::vector<ReprojGeom> gb;
     for (int i = 1; i < nz; ++i) {
       for (int side = 0; side < 2; ++side) {
         int ip = side == 0 ? zt + i : zt - i;
@@ -116,21 +118,26 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
                            b, ip, s->angles[ip]);
         ReprojGeom gm;
         reproj_geometry(s->angles.data(), ip, rg[0], rg[1], xb, yb, g->thick, &gm);
-        const int k = (int)g->order[b].size();
-        GroupStepDev& sd = steps[(size_t)k * B + b];
-        sd.ip = ip;
-        sd.i0 = gm.i0;
-        sd.nk = gm.nk;
-        sd.ray_len = gm.ray_len;
-        sd.thick = gm.thick;
-        sd.bp_off = (int)bp.size();
-        sd.fcos = gm.fcos;
-        sd.fsin = gm.fsin;
-        bp.insert(bp.end(), gm.bp.begin(), gm.bp.end());
-        g->order[b].push_back(ip);
-        geoms.push_back(gm);
+        gb.push_back(gm);
         skip[ip] = 0;
       }
+    }
+    MF_TRY(fill_bp_device(c, s->angles.data(), &gb, st));
+    for (const ReprojGeom& gm : gb) {
+      const int k = (int)g->order[b].size();
+      if (k >= n) break;
+      GroupStepDev& sd = steps[(size_t)k * B + b];
+      sd.ip = gm.ip;
+      sd.i0 = gm.i0;
+      sd.nk = gm.nk;
+      sd.ray_len = gm.ray_len;
+      sd.thick = gm.thick;
+      sd.bp_off = (int)bp.size();
+      sd.fcos = gm.fcos;
+      sd.fsin = gm.fsin;
+      bp.insert(bp.end(), gm.bp.begin(), gm.bp.end());
+      g->order[b].push_back(gm.ip);
+      geoms.push_back(gm);
     }
     if ((int)g->order[b].size() != n)
       return set_error(MF_ERR_GEOMETRY, "series %d: %d held-out tilts instead of %d", b,
@@ -146,6 +153,9 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
   MF_TRY(g->recorr_out.alloc(sizeof(float) * g->bpix * B));
   MF_TRY(g->mpart.alloc(sizeof(double2) * moment_parts(yb) * 2 * B));
   MF_TRY(g->stats.alloc(sizeof(float2) * 2 * B));
+  MF_TRY(g->mask.alloc(sizeof(float) * g->bpix));
+  MF_TRY(make_round_mask(c, xb, yb, (float)((pad / 2 - 1) * 2) * 0.5f, (float)yb * 0.5f,
+                         (float)pad, (float)yb, 4.0f, g->mask.as<float>(), st));
   MF_TRY(g->ppart.alloc(sizeof(float2) * kPeakParts * B));
   MF_TRY(g->rowflags.alloc(sizeof(int) * g->ytiles * B));
   MF_TRY(g->d_steps.alloc(sizeof(GroupStepDev) * steps.size()));
@@ -181,6 +191,7 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     mf_series* s = g->ser[b];
     GroupSeriesDev& d = sd[b];
     d.stack = s->stack.as<float>();
+    d.stack_t = s->stack_t.as<float>();
     d.sx = s->d_sx.as<float>();
     d.sy = s->d_sy.as<float>();
     d.rot = s->d_rot.as<float>();
@@ -308,7 +319,8 @@ static int group_enqueue(mf_group* g) {
     // MeaAlignProj for every series: PANorm both images, FFT, filter, inverse, peak
     MF_TRY(norm_mask_pad_group(c, g->d_normptr.as<const float*>() + (size_t)k * 2 * B, active,
                                2 * B, xb, yb, pad, ppix, mcx, mcy, (float)pad, (float)yb, 4.0f,
-                               cc, g->mpart.as<double2>(), g->stats.as<float2>(), st));
+                               g->mask.as<float>(), cc, g->mpart.as<double2>(),
+                               g->stats.as<float2>(), st));
     for (int b = 0; b < B; ++b) {
       float* cb = cc + (size_t)b * 2 * ppix;
       MF_CHECK_CUFFT(cufftExecR2C(g->cc_fwd, cb, (cufftComplex*)cb));
@@ -349,6 +361,7 @@ static int group_enqueue(mf_group* g) {
 // One pass over the series with active[b] != 0; max_err[b] receives each active
 // series' largest measured shift (inactive entries are left as they are).
 static int group_doit(mf_group* g, const int* active, float* max_err) {
+  StageTimer timer(&g->ctx->c, kStagePass);
   Context* c = &g->ctx->c;
   cudaStream_t st = c->stream;
   const int B = g->B;
@@ -470,7 +483,7 @@ int group_proj_align(mf_group* g, int* passes) {
   for (int i = 1; i <= 4; ++i) {
     for (int b = 0; b < B; ++b) {
       float ax;
-      MF_TRY(tilt_axis(g->ser[b], 20.0f / i, 100, &ax));
+      MF_TRY(tilt_axis(g->ser[b], 20.0f / i, 100, &ax, nullptr));
     }
     if (i == 1) MF_TRY(once());
   }

@@ -95,6 +95,34 @@ MF_API int mf_context_stage_times(mf_context* ctx, double* out6) {
   return MF_OK;
 }
 
+MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out6) {
+  if (!ctx || !out6) return set_error(MF_ERR_ARG, "null argument");
+  for (int i = 0; i < kStages; ++i) {
+    out6[i] = ctx->c.breakdown[i];
+    ctx->c.breakdown[i] = 0.0;
+  }
+  return MF_OK;
+}
+
+MF_API int mf_device_cos_sin(mf_context* ctx, const float* x, int n, float* c, float* s) {
+  MF_GUARD_BEGIN
+  if (!ctx || n < 0 || (n > 0 && (!x || !c || !s))) return set_error(MF_ERR_ARG, "bad argument");
+  if (n == 0) return MF_OK;
+  MF_TRY(use_device(ctx));
+  cudaStream_t st = ctx->c.stream;
+  DevBuf d;
+  MF_TRY(d.alloc(sizeof(float) * 3 * (size_t)n));
+  float* dx = d.as<float>();
+  MF_CHECK_CUDA(cudaMemcpyAsync(dx, x, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  MF_TRY(device_cos_sin(&ctx->c, dx, n, dx + n, dx + 2 * (size_t)n, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(c, dx + n, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(s, dx + 2 * (size_t)n, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                                st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+  MF_GUARD_END
+}
+
 MF_API void* mf_context_stream(mf_context* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
 
 MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows) {
@@ -114,6 +142,7 @@ static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_d
   if (!raw || !file_angles) return set_error(MF_ERR_ARG, "null stack or angles");
   if (nx < 8 || ny < 8 || nz < 2)
     return set_error(MF_ERR_ARG, "stack %d x %d x %d too small (need >= 8 x 8 x 2)", nx, ny, nz);
+  StageTimer timer(&ctx->c, kStagePrep);
   mf_series* s = new mf_series();
   int rc = series_init(s, ctx, nx, ny, nz, file_angles);
   size_t pix = (size_t)nx * ny;
@@ -133,6 +162,12 @@ static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_d
   }
   if (rc == MF_OK)
     rc = preprocess_device(&ctx->c, s->stack.as<float>(), nx, ny, nz, file_angles, ctx->c.stream);
+  // the column-major copy read by the resampling and the tilt-axis search
+  if (rc == MF_OK) rc = s->stack_t.alloc(sizeof(float) * pix * nz);
+  if (rc == MF_OK) rc = s->d_neg.alloc(sizeof(int) * nz);
+  if (rc == MF_OK)
+    rc = transpose_stack(&ctx->c, s->stack.as<float>(), nx, ny, nz, s->stack_t.as<float>(),
+                         s->d_neg.as<int>(), ctx->c.stream);
   if (rc != MF_OK) {
     delete s;
     return rc;
@@ -157,9 +192,12 @@ MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw, int nx, 
 
 MF_API void mf_series_destroy(mf_series* s) {
   if (!s) return;
-  // buffers go back to the pool in stream order on the (still alive) context stream
+  // buffers go back to the pool in the order of the stream of the series' current
+  // context (a served series may have been prepared on another worker's stream)
   cudaSetDevice(s->gpu);
+  set_free_stream(s->ctx ? s->ctx->c.stream : nullptr);
   delete s;
+  set_free_stream(nullptr);
 }
 
 MF_API int mf_series_set_precision(mf_series* s, mf_precision p) {
@@ -230,7 +268,16 @@ MF_API int mf_tilt_axis(mf_series* s, float range, int num, float* axis_out) {
   MF_GUARD_BEGIN
   if (!s) return set_error(MF_ERR_ARG, "null series");
   MF_TRY(use_device(s->ctx));
-  return tilt_axis(s, range, num, axis_out);
+  return tilt_axis(s, range, num, axis_out, nullptr);
+  MF_GUARD_END
+}
+
+MF_API int mf_tilt_axis_scores(mf_series* s, float range, int num, float* axis_out,
+                               float* scores) {
+  MF_GUARD_BEGIN
+  if (!s || !scores) return set_error(MF_ERR_ARG, "null argument");
+  MF_TRY(use_device(s->ctx));
+  return tilt_axis(s, range, num, axis_out, scores);
   MF_GUARD_END
 }
 
@@ -263,6 +310,19 @@ MF_API int mf_projalign_z0(mf_series* s, float* z0) {
   if (!s->pa.ready) return set_error(MF_ERR_STATE, "projection matching is not set up");
   *z0 = s->pa.z0;
   return MF_OK;
+}
+
+MF_API int mf_projalign_measured(mf_series* s, float* xy) {
+  MF_GUARD_BEGIN
+  if (!s || !xy) return set_error(MF_ERR_ARG, "null argument");
+  if (!s->pa.ready) return set_error(MF_ERR_STATE, "projection matching is not set up");
+  MF_TRY(use_device(s->ctx));
+  cudaStream_t st = s->ctx->c.stream;
+  MF_CHECK_CUDA(cudaMemcpyAsync(xy, s->pa.d_meas.p, sizeof(float) * 2 * s->nz,
+                                cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+  MF_GUARD_END
 }
 
 MF_API int mf_coarse_align(mf_series* s, float pitch_angle, float offset) {
@@ -402,6 +462,11 @@ MF_API int mf_dev_reproject(mf_context* ctx, const float* d_corr, int xb, int yb
   cudaStream_t st = ctx->c.stream;
   ReprojGeom g;
   reproj_geometry(angles, iproj, istart, iend, xb, yb, thickness, &g);
+  {
+    std::vector<ReprojGeom> gv(1, g);
+    MF_TRY(fill_bp_device(&ctx->c, angles, &gv, st));
+    g = gv[0];
+  }
   mf_context::Scratch* S = scratch_of(ctx);
   MF_TRY(S->b.alloc(sizeof(float) * g.bp.size()));
   MF_CHECK_CUDA(cudaMemcpyAsync(S->b.p, g.bp.data(), sizeof(float) * g.bp.size(),
@@ -475,7 +540,7 @@ MF_API int mf_dev_measure_shift(mf_context* ctx, const float* d_reproj, const fl
   float* cc = S->a.as<float>();
   const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
   MF_TRY(norm_mask_pad(&ctx->c, d_reproj, d_proj, xb, 0, xb, yb, pad, ppix, 2, 0, mcx, mcy,
-                       (float)pad, (float)yb, 4.0f, cc, mpart, stats, st));
+                       (float)pad, (float)yb, 4.0f, nullptr, cc, mpart, stats, st));
   cufftHandle f, i;
   MF_TRY(ctx->plan({2, xb, yb, 2}, &f));
   MF_TRY(ctx->plan({3, xb, yb, 1}, &i));

@@ -19,9 +19,11 @@ int set_error(int code, const char* fmt, ...) {
 const char* last_error() { return g_last_error; }
 
 static thread_local cudaStream_t g_alloc_stream = nullptr;
+static thread_local cudaStream_t g_free_stream = nullptr;
 static thread_local bool g_sync_free = false;
 
 void set_alloc_stream(cudaStream_t s) { g_alloc_stream = s; }
+void set_free_stream(cudaStream_t s) { g_free_stream = s; }
 void set_sync_free(bool on) { g_sync_free = on; }
 
 int DevBuf::alloc(size_t n) {
@@ -44,10 +46,14 @@ int DevBuf::alloc(size_t n) {
 
 void DevBuf::release() {
   if (p) {
-    if (st && !g_sync_free)
-      cudaFreeAsync(p, st);
-    else
+    // freed in the order of the stream that last used it: the allocating stream,
+    // or the one a caller names (a series that moved to another context)
+    cudaStream_t fs = g_free_stream ? g_free_stream : st;
+    if (!fs || g_sync_free || cudaFreeAsync(p, fs) != cudaSuccess) {
+      cudaGetLastError();
       cudaFree(p);
+      cudaGetLastError();
+    }
   }
   p = nullptr;
   bytes = 0;

@@ -12,9 +12,28 @@
 
 namespace mf {
 
+// Where pixel (ix, iy) of an in_x x in_y image sits: ix * xs + iy * ys.  The
+// row-major stack has (xs, ys) = (1, in_x); its column-major copy (in_y, 1).
+struct Layout {
+  int xs, ys;
+  __device__ __forceinline__ size_t at(int ix, int iy) const {
+    return (size_t)ix * xs + (size_t)iy * ys;
+  }
+};
+
+// Neighbouring output pixels of a row sample the source one step of (cos, sin)
+// apart: along a source row when |cos| >= |sin|, else along a source column, which
+// the column-major copy (when there is one) holds contiguously.  Both layouts hold
+// the same values, so the choice changes addresses only.
+__device__ __forceinline__ Layout pick_layout(const float* stack_t, int in_x, int in_y, float cs,
+                                              float sn) {
+  if (stack_t != nullptr && fabsf(sn) > fabsf(cs)) return Layout{in_y, 1};
+  return Layout{1, in_x};
+}
+
 // CorrStack.cu:116-140
 __device__ __forceinline__ float corr_random(int x, int y, int in_x, int in_y,
-                                             const float* __restrict__ img) {
+                                             const float* __restrict__ img, Layout L) {
   if (x < 0) x = -x;
   if (y < 0) y = -y;
   if (x >= in_x) x = in_x - 1 - (x % in_x);
@@ -27,31 +46,33 @@ __device__ __forceinline__ float corr_random(int x, int y, int in_x, int in_y,
     if (ix < 0 || ix >= in_x) continue;
     int iy = (int)(next / (unsigned int)win) - win / 2 + y;
     if (iy < 0 || iy >= in_y) continue;
-    return __ldg(img + (size_t)iy * in_x + ix);
+    return __ldg(img + L.at(ix, iy));
   }
-  return __ldg(img + (size_t)y * in_x + x);
+  return __ldg(img + L.at(x, y));
 }
 
 // CorrStack.cu:151-179 for one resampled pixel (X, Y) of an out_x x in_y grid.
-__device__ __forceinline__ float corr_pixel(const float* __restrict__ img, int in_x, int in_y,
-                                            int X, int Y, int out_x, float sx, float sy,
+__device__ __forceinline__ float corr_pixel(const float* __restrict__ img, Layout L, int in_x,
+                                            int in_y, int X, int Y, int out_x, float sx, float sy,
                                             float cs, float sn, bool random_fill) {
   float ax = __fsub_rn(__fadd_rn((float)X, 0.5f), __fmul_rn((float)out_x, 0.5f));
   float ay = __fsub_rn(__fadd_rn((float)Y, 0.5f), __fmul_rn((float)in_y, 0.5f));
-  float t = __fsub_rn(__fmul_rn(ax, cs), __fmul_rn(ay, sn));
-  ay = __fadd_rn(__fmul_rn(ax, sn), __fmul_rn(ay, cs));
+  // mGCorrect's rotation as nvcc compiles it: the first product of each sum fused
+  float t = __fmaf_rn(ax, cs, -__fmul_rn(ay, sn));
+  ay = __fmaf_rn(ax, sn, __fmul_rn(ay, cs));
   ax = t;
   ax = __fadd_rn(ax, __fadd_rn(sx, __fmul_rn((float)in_x, 0.5f)));
   ay = __fadd_rn(ay, __fadd_rn(sy, __fmul_rn((float)in_y, 0.5f)));
   int ix = (int)__fadd_rn(ax, 0.5f);
   int iy = (int)__fadd_rn(ay, 0.5f);
-  if (ix >= 0 && ix < in_x && iy >= 0 && iy < in_y) return __ldg(img + (size_t)iy * in_x + ix);
-  if (random_fill) return corr_random(ix, iy, in_x, in_y, img);
+  if (ix >= 0 && ix < in_x && iy >= 0 && iy < in_y) return __ldg(img + L.at(ix, iy));
+  if (random_fill) return corr_random(ix, iy, in_x, in_y, img, L);
   return kSentinel;
 }
 
 struct CorrArgs {
   const float* stack;
+  const float* stack_t;  // column-major copy of the stack, or null
   int nx, ny;
   size_t pix;
   const int* tilts;  // tilt index per blockIdx.z (nullptr: blockIdx.z itself)
@@ -74,8 +95,8 @@ __global__ void k_correct_bin(CorrArgs a) {
     float rot = a.sx ? a.rot[z] : a.one_rot;
     float axis = a.only_shift ? 0.0f : rot;
     axis = (float)((double)axis * kD2R);  // CorrStack.cu:376-378
-    s_cs = (float)cos((double)axis);
-    s_sn = (float)sin((double)axis);
+    s_cs = cosf(axis);  // CUDA's cosf/sinf, as mGCorrect (CorrStack.cu:160-161)
+    s_sn = sinf(axis);
     s_sx = a.sx ? a.sx[z] : a.one_sx;
     s_sy = a.sx ? a.sy[z] : a.one_sy;
   }
@@ -83,17 +104,19 @@ __global__ void k_correct_bin(CorrArgs a) {
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
   const int by = blockIdx.y * blockDim.y + threadIdx.y;
   if (bx >= a.xb || by >= a.yb) return;
-  const float* img = a.stack + (size_t)z * a.pix;
+  const Layout L = pick_layout(a.stack_t, a.nx, a.ny, s_cs, s_sn);
+  const float* img = (L.xs == 1 ? a.stack : a.stack_t) + (size_t)z * a.pix;
   float res;
   if (a.bin == 1) {
-    res = corr_pixel(img, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn, a.random_fill);
+    res = corr_pixel(img, L, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn,
+                     a.random_fill);
   } else {
     float sum = 0.0f;
     bool bad = false;
     for (int iy = 0; iy < a.biny && !bad; ++iy) {
       for (int ix = 0; ix < a.binx; ++ix) {
-        float v = corr_pixel(img, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x, s_sx,
-                             s_sy, s_cs, s_sn, a.random_fill);
+        float v = corr_pixel(img, L, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x,
+                             s_sx, s_sy, s_cs, s_sn, a.random_fill);
         if (v < -1e10f) {
           bad = true;
           break;
@@ -117,8 +140,8 @@ __global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int 
   const int z = g.steps ? g.steps[b].ip : j % g.nz;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     const float axis = (float)((double)S.rot[z] * kD2R);  // CorrStack.cu:376-378
-    s_cs = (float)cos((double)axis);
-    s_sn = (float)sin((double)axis);
+    s_cs = cosf(axis);  // CUDA's cosf/sinf, as mGCorrect (CorrStack.cu:160-161)
+    s_sn = sinf(axis);
     s_sx = S.sx[z];
     s_sy = S.sy[z];
   }
@@ -126,17 +149,18 @@ __global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int 
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
   const int by = blockIdx.y * blockDim.y + threadIdx.y;
   if (bx >= xb || by >= yb) return;
-  const float* img = S.stack + (size_t)z * g.nx * g.ny;
+  const Layout L = pick_layout(S.stack_t, g.nx, g.ny, s_cs, s_sn);
+  const float* img = (L.xs == 1 ? S.stack : S.stack_t) + (size_t)z * g.nx * g.ny;
   float res;
   if (g.bin == 1) {
-    res = corr_pixel(img, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
+    res = corr_pixel(img, L, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
   } else {
     float sum = 0.0f;
     bool bad = false;
     for (int iy = 0; iy < biny && !bad; ++iy) {
       for (int ix = 0; ix < binx; ++ix) {
-        float v = corr_pixel(img, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx, s_sy,
-                             s_cs, s_sn, g.random_fill);
+        float v = corr_pixel(img, L, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx,
+                             s_sy, s_cs, s_sn, g.random_fill);
         if (v < -1e10f) {
           bad = true;
           break;
@@ -158,12 +182,13 @@ static void fill_sizes(CorrArgs* a, int nx, int ny, int bin) {
   a->biny = ny / a->yb;
 }
 
-int launch_correct_bin(Context* c, const float* stack, int nx, int ny, const int* d_tilts,
-                       int ntilts, const float* d_sx, const float* d_sy, const float* d_rot,
-                       int only_shift, int bin, int random_fill, float* out, int out_row_stride,
-                       size_t out_tilt_stride, cudaStream_t st) {
+int launch_correct_bin(Context* c, const float* stack, const float* stack_t, int nx, int ny,
+                       const int* d_tilts, int ntilts, const float* d_sx, const float* d_sy,
+                       const float* d_rot, int only_shift, int bin, int random_fill, float* out,
+                       int out_row_stride, size_t out_tilt_stride, cudaStream_t st) {
   CorrArgs a{};
   a.stack = stack;
+  a.stack_t = stack_t;
   a.nx = nx;
   a.ny = ny;
   a.pix = (size_t)nx * ny;
@@ -228,8 +253,9 @@ __global__ void k_rweight(cufftComplex* spec, int cmp, int rows) {
   if (x >= cmp) return;
   float fN = 2 * ((float)cmp - 1.0f);
   float r = __fdiv_rn((float)x, fN);
-  float cw = (float)cos((double)__fmul_rn(6.2831852f, r));
-  r = __fmul_rn(__fmul_rn(2.0f, r), __fadd_rn(0.55f, __fmul_rn(0.45f, cw)));
+  // CUDA's cosf and the contraction of 0.55f + 0.45f * cosf(...), as in GRWeight
+  float cw = cosf(__fmul_rn(6.2831852f, r));
+  r = __fmul_rn(__fmul_rn(2.0f, r), __fmaf_rn(0.45f, cw, 0.55f));
   for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < rows;
        row += gridDim.y * blockDim.y) {
     size_t i = (size_t)row * cmp + x;

@@ -55,6 +55,8 @@ void set_alloc_stream(cudaStream_t s);
 // While set, buffers are released with a synchronous cudaFree (used when the
 // owning stream may already be gone).
 void set_sync_free(bool on);
+// The stream DevBuf::release frees on in this thread (null: each buffer's own).
+void set_free_stream(cudaStream_t s);
 
 struct DevBuf {
   void* p = nullptr;
@@ -81,6 +83,13 @@ struct FftPlan {
   void release();
 };
 
+// Stages of Context::breakdown: series creation (upload, pre-processing, the
+// column-major copy), coarse alignment (stretch correlations, offset search),
+// tilt-axis searches, projection-matching set-up, projection-matching passes,
+// aligned-stack output.
+enum StageSlot { kStagePrep, kStageCoarse, kStageAxis, kStageSetup, kStagePass, kStageFinal,
+                 kStages };
+
 struct Context {
   int gpu = 0;
   cudaStream_t stream = nullptr;
@@ -89,6 +98,39 @@ struct Context {
   bool profiling = false;
   int tc_rows = 0;  // tensor-core tile rows (64/128/256); 0 = chosen per shape
   double stage[6] = {0, 0, 0, 0, 0, 0};  // see mf_context_stage_times
+  double breakdown[kStages] = {};        // ms per stage, see mf_context_stage_breakdown
+};
+
+// Wall time on the context's stream of one stage of an alignment, accumulated in
+// Context::breakdown when profiling is on (events on both sides, then a wait).
+class StageTimer {
+ public:
+  StageTimer(Context* c, int slot) : c_(c), slot_(slot) {
+    if (!c->profiling) return;
+    if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    on_ = cudaEventRecord(a_, c->stream) == cudaSuccess;
+  }
+  ~StageTimer() {
+    if (on_ && cudaEventRecord(b_, c_->stream) == cudaSuccess &&
+        cudaEventSynchronize(b_) == cudaSuccess) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, a_, b_) == cudaSuccess) c_->breakdown[slot_] += ms;
+    }
+    if (a_) cudaEventDestroy(a_);
+    if (b_) cudaEventDestroy(b_);
+    cudaGetLastError();
+  }
+  StageTimer(const StageTimer&) = delete;
+  StageTimer& operator=(const StageTimer&) = delete;
+
+ private:
+  Context* c_;
+  int slot_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+  bool on_ = false;
 };
 
 // ---- per-held-out-tilt banded re-projection operator ----------------------
@@ -173,10 +215,12 @@ struct TcOpSet {
 // (nz x ny x nx) using per-tilt device parameters; tilts listed in d_tilts.
 // Output tilt j (j-th entry of d_tilts) goes to out + j*out_tilt_stride with row
 // stride out_row_stride.
-int launch_correct_bin(Context* c, const float* stack, int nx, int ny, const int* d_tilts,
-                       int ntilts, const float* d_sx, const float* d_sy, const float* d_rot,
-                       int only_shift, int bin, int random_fill, float* out, int out_row_stride,
-                       size_t out_tilt_stride, cudaStream_t st);
+// stack_t: the stack's column-major copy (nz x nx x ny), or null; read for tilts
+// whose axis makes output rows run along source columns.
+int launch_correct_bin(Context* c, const float* stack, const float* stack_t, int nx, int ny,
+                       const int* d_tilts, int ntilts, const float* d_sx, const float* d_sy,
+                       const float* d_rot, int only_shift, int bin, int random_fill, float* out,
+                       int out_row_stride, size_t out_tilt_stride, cudaStream_t st);
 // Same for a single image with scalar parameters.
 int launch_correct_one(Context* c, const float* img, int nx, int ny, float sx, float sy,
                        float axis_deg, int only_shift, int bin, int random_fill, float* out,
@@ -203,6 +247,15 @@ struct ReprojGeom {
 };
 void reproj_geometry(const float* angles, int ip, int i0, int i1, int xb, int yb, int thick,
                      ReprojGeom* g);
+// The (w, cos, sin) table of every geometry evaluated on the device with CUDA's
+// cosf/sinf, as the reference's back-projection kernel does, written back into
+// geoms[i].bp (the host values of reproj_geometry are correctly rounded).
+constexpr int kMaxBpNeighbours = 256;
+int fill_bp_device(Context* c, const float* angles, std::vector<ReprojGeom>* geoms,
+                   cudaStream_t st);
+// The same table for one held-out tilt straight into device memory.
+int bp_table_device(Context* c, const float* angles, int ip, int i0, int nk, float* d_out,
+                    cudaStream_t st);
 // Builds the operators of all geometries (same xb, yb) with two launches.
 int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
                      cudaStream_t st);
@@ -250,14 +303,15 @@ constexpr int kMaxGroup = 32;
 constexpr int kFlagParts = 8;  // column parts of a 16-bit copy's per-tile flags
 
 struct GroupSeriesDev {
-  const float* stack;  // pre-processed stack (nz x ny x nx)
+  const float* stack;    // pre-processed stack (nz x ny x nx)
+  const float* stack_t;  // the same, column-major per tilt (nz x nx x ny)
   float* sx;
   float* sy;
   const float* rot;
   const float* angles;
   float* z0;
   float* err;    // nz: |shift| of the last measurement per tilt
-  float* meas;   // 2 * nz: binned shift of the last measurement per tilt
+  float* meas;   // 2 * nz: shift measured in the last pass (un-binned px, before rotation)
   float* corr;   // corrected stack of this series (nz x yb x xb)
   const int* order;  // outward processing order (nz - 1 entries)
   int zt, pad0;

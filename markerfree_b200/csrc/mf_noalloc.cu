@@ -9,7 +9,8 @@
 // real-time loop in which cudaMalloc/cudaFree, which can synchronise the whole
 // device, would stall the detector stream.  The entry point below keeps the table
 // in a file-scope __device__ array instead, so it performs no device allocation
-// at all (and no host heap allocation either: the table is built on the stack).
+// at all (and no host heap allocation either: the table is written by a kernel
+// whose arguments carry the angles).
 //
 // The array is sized for kStaticMaxNeighbours neighbours (3 floats each, 3 KB),
 // is held by every GPU that loads this library until the process exits, and is
@@ -73,26 +74,16 @@ extern "C" MF_API int mf_dev_reproject_noalloc(void* stream, const float* d_corr
   MF_CHECK_CUDA(cudaGetDevice(&dev));
   float* d_table = nullptr;
   MF_TRY(table_address(dev, &d_table));
-  // geometry of CalcReproj.cu:43-44 and 301-303, as in reproj_geometry()
-  float table[kStaticMaxNeighbours * 3];
+  // geometry of CalcReproj.cu:43-46 and 301-303: the table is written by a small
+  // kernel (its angles travel as kernel arguments), then read by the re-projection
   const float pa = angles[iproj];
-  for (int k = 0; k < nk; ++k) {
-    const float a = angles[istart + k];
-    table[3 * k + 0] = cos_f((pa - a) * kBpD2R);
-    const float v = a * kBpD2R;
-    table[3 * k + 1] = cos_f(v);
-    table[3 * k + 2] = sin_f(v);
-  }
   const float fcos = (float)std::cos(kD2R * pa);
   const float fsin = (float)std::sin(kD2R * pa);
   const int ray_len = (int)((float)thickness / fcos + 0.5f);
   cudaStream_t st = (cudaStream_t)stream;
-  // From pageable memory the copy returns once the table is staged, so the stack
-  // buffer may go out of scope; the kernel is ordered after it on `st`.
-  MF_CHECK_CUDA(cudaMemcpyAsync(d_table, table, sizeof(float) * 3 * nk, cudaMemcpyHostToDevice,
-                                st));
   Context c;  // launch bookkeeping only; owns nothing
   c.gpu = dev;
+  MF_TRY(bp_table_device(&c, angles, iproj, istart, nk, d_table, st));
   return launch_reproject_exact(&c, d_corr, xb, yb, (size_t)xb * yb, d_table, istart, nk, fcos,
                                 fsin, ray_len, thickness, nullptr, d_out, st);
 }

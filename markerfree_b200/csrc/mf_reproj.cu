@@ -56,10 +56,67 @@ void reproj_geometry(const float* angles, int ip, int i0, int i1, int xb, int yb
   g->ray_len = (int)((float)thick / g->fcos + 0.5f);
 }
 
+// Back-projection weights and directions with CUDA's cosf/sinf, as mGBackProj
+// evaluates them (CalcReproj.cu:43-46): per neighbour (w, cos, sin).
+struct BpArgs {
+  float pa;
+  int nk;
+  float a[kMaxBpNeighbours];
+};
+__global__ void k_bp_table(BpArgs args, float* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= args.nk) return;
+  const float a = args.a[k];
+  out[3 * k + 0] = cosf(__fmul_rn(__fsub_rn(args.pa, a), kBpD2R));
+  const float v = __fmul_rn(a, kBpD2R);
+  out[3 * k + 1] = cosf(v);
+  out[3 * k + 2] = sinf(v);
+}
+
+int bp_table_device(Context* c, const float* angles, int ip, int i0, int nk, float* d_out,
+                    cudaStream_t st) {
+  if (nk < 1 || nk > kMaxBpNeighbours)
+    return set_error(MF_ERR_ARG, "%d neighbour tilts (1..%d supported)", nk, kMaxBpNeighbours);
+  BpArgs args{};
+  args.pa = angles[ip];
+  args.nk = nk;
+  for (int k = 0; k < nk; ++k) args.a[k] = angles[i0 + k];
+  k_bp_table<<<(nk + 127) / 128, 128, 0, st>>>(args, d_out);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int fill_bp_device(Context* c, const float* angles, std::vector<ReprojGeom>* geoms,
+                   cudaStream_t st) {
+  size_t total = 0;
+  for (const ReprojGeom& g : *geoms) total += 3 * (size_t)g.nk;
+  if (total == 0) return MF_OK;
+  DevBuf d;
+  MF_TRY(d.alloc(sizeof(float) * total));
+  size_t off = 0;
+  for (const ReprojGeom& g : *geoms) {
+    MF_TRY(bp_table_device(c, angles, g.ip, g.i0, g.nk, d.as<float>() + off, st));
+    off += 3 * (size_t)g.nk;
+  }
+  std::vector<float> h(total);
+  MF_CHECK_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(float) * total, cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  off = 0;
+  for (ReprojGeom& g : *geoms) {
+    g.bp.assign(h.begin() + off, h.begin() + off + 3 * (size_t)g.nk);
+    off += 3 * (size_t)g.nk;
+  }
+  return MF_OK;
+}
+
 // ---------------------------------------------------------------------------
-// Device geometry helpers.  Every step is an explicitly rounded IEEE operation so
-// that no multiply-add is contracted: cell and bin indices then agree bit for bit
-// with a plain C evaluation of the reference expressions.
+// Device geometry helpers.  Every step is an explicitly rounded IEEE operation,
+// and a multiply-add is fused exactly where nvcc fuses the reference's
+// expressions (its default contraction: in a*b + c and c - a*b the product is
+// fused; in a*b + c*d the first product): cell and bin indices then agree bit for
+// bit with the reference binary and with a C evaluation that uses fmaf at the
+// same places.
 struct RayStart {
   float tx, tz, zst;
 };
@@ -68,8 +125,8 @@ __device__ __forceinline__ RayStart ray_start(int bx, int xb, int W, int T, floa
                                               float fsin, int L) {
   float fxp = __fsub_rn(__fadd_rn((float)bx, 0.5f), __fmul_rn((float)xb, 0.5f));
   RayStart r;
-  r.tx = __fadd_rn(__fmul_rn(fxp, fcos), __fmul_rn((float)W, 0.5f));
-  r.tz = __fadd_rn(__fmul_rn(fxp, fsin), __fmul_rn((float)T, 0.5f));
+  r.tx = __fmaf_rn(fxp, fcos, __fmul_rn((float)W, 0.5f));
+  r.tz = __fmaf_rn(fxp, fsin, __fmul_rn((float)T, 0.5f));
   r.zst = __fsub_rn(__fdiv_rn(__fmul_rn(-fxp, fsin), fcos), __fmul_rn(0.5f, (float)L));
   return r;
 }
@@ -78,8 +135,8 @@ __device__ __forceinline__ RayStart ray_start(int bx, int xb, int W, int T, floa
 __device__ __forceinline__ bool ray_cell(const RayStart& r, int j, int W, int T, float fcos,
                                          float fsin, int* ix, int* iz) {
   float fz = __fadd_rn((float)j, r.zst);
-  float X = __fsub_rn(r.tx, __fmul_rn(fz, fsin));
-  float Z = __fadd_rn(r.tz, __fmul_rn(fz, fcos));
+  float X = __fmaf_rn(-fz, fsin, r.tx);
+  float Z = __fmaf_rn(fz, fcos, r.tz);
   if (!(X >= 0.0f && X < (float)(W - 1) && Z >= 0.0f && Z < (float)(T - 1))) return false;
   *ix = (int)X;
   *iz = (int)Z;
@@ -91,7 +148,7 @@ __device__ __forceinline__ int cell_bin(int ix, int iz, int W, int T, float c, f
                                         float cent, int xb) {
   float fx = __fsub_rn(__fadd_rn((float)ix, 0.5f), __fmul_rn((float)W, 0.5f));
   float fz = __fsub_rn(__fadd_rn((float)iz, 0.5f), __fmul_rn((float)T, 0.5f));
-  float v = __fadd_rn(__fadd_rn(__fmul_rn(fx, c), __fmul_rn(fz, s)), cent);
+  float v = __fadd_rn(__fmaf_rn(fx, c, __fmul_rn(fz, s)), cent);
   if (v < 0.0f || v > (float)(xb - 1)) return -1;
   return (int)v;
 }
@@ -144,7 +201,7 @@ __device__ void exact_rows(const float* __restrict__ corr, int xb, size_t pix,
         if (b < 0) continue;
         float v = corr[(size_t)(i0 + k) * pix + (size_t)y * xb + b];
         if (v < -1e10f) continue;  // mDIntProj turns it into -1e30, then skipped
-        fint = __fadd_rn(fint, __fmul_rn(__fmul_rn(v, c), w));
+        fint = __fmaf_rn(__fmul_rn(v, c), w, fint);
         fcount = __fadd_rn(fcount, w);
       }
       float cell = (fcount < 0.001f) ? kSentinel : __fdiv_rn(fint, fcount);

@@ -140,6 +140,7 @@ namespace mf {
 // ---------------------------------------------------------------------------
 // Transform::DoIt + Measure (Transform.cpp:60-97), all tilt pairs batched.
 int transform_doit(mf_series* s, float* max_err_out) {
+  StageTimer timer(&s->ctx->c, kStageCoarse);
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   const int nx = s->nx, ny = s->ny, nz = s->nz;
@@ -160,7 +161,8 @@ int transform_doit(mf_series* s, float* max_err_out) {
   MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
   MF_TRY(pbuf.alloc(sizeof(float) * ppix * nz));
   MF_TRY(refs.alloc(sizeof(float) * ppix * nz));
-  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), nx, ny, nullptr, nz, s->d_sx.as<float>(),
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
+                            nx, ny, nullptr, nz, s->d_sx.as<float>(),
                             s->d_sy.as<float>(), s->d_rot.as<float>(), 1, T.bin, 1,
                             corr.as<float>(), xb, bpix, st));
   k_pad_copy<<<dim3((pad + 63) / 64, (yb + 3) / 4, nz), dim3(64, 4), 0, st>>>(
@@ -196,14 +198,14 @@ int transform_doit(mf_series* s, float* max_err_out) {
     const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
     // references: normalise (mean, std) + round edge, all tilts
     MF_TRY(norm_mask_pad(c, pbuf.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy,
-                         msx, msy, 4.0f, refs.as<float>(), part.as<double2>(), stats.as<float2>(),
-                         st));
+                         msx, msy, 4.0f, nullptr, refs.as<float>(), part.as<double2>(),
+                         stats.as<float2>(), st));
     // images: stretch the padded raw copy, then normalise + round edge
     MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
                         np, 1, imgs.as<float>(), ppix, st));
     MF_TRY(norm_mask_pad(c, imgs.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy,
-                         msx, msy, 4.0f, imgs.as<float>(), part.as<double2>(), stats.as<float2>(),
-                         st));
+                         msx, msy, 4.0f, nullptr, imgs.as<float>(), part.as<double2>(),
+                         stats.as<float2>(), st));
     cufftHandle fr, fi, inv;
     MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));
     MF_TRY(s->ctx->plan({2, xb, yb, np}, &fi));
@@ -268,7 +270,8 @@ int transform_doit(mf_series* s, float* max_err_out) {
 
 // ---------------------------------------------------------------------------
 // CalcTIltAxis::DoIt + CLsetup (Rotate.cu:292-374)
-int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
+int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores_out) {
+  StageTimer timer(&s->ctx->c, kStageAxis);
   if (num < 2) return set_error(MF_ERR_ARG, "tilt axis: need at least 2 candidates");
   Context* c = &s->ctx->c;
   const int nz = s->nz;
@@ -293,9 +296,11 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
   std::vector<float> scores;
   cufftHandle plan;
   MF_TRY(s->ctx->plan({4, L, 0, (long long)nz * num}, &plan));
-  MF_TRY(tilt_axis_scores(c, plan, s->stack.as<float>(), s->nx, s->ny, nz, s->angles.data(),
+  MF_TRY(tilt_axis_scores(c, plan, s->stack.as<float>(), s->stack_t.as<float>(),
+                          s->d_neg.as<int>(), s->nx, s->ny, nz, s->angles.data(),
                           s->sx.data(), s->sy.data(), zt, cand.data(), num, L, &scores,
                           c->stream));
+  if (scores_out) std::copy(scores.begin(), scores.end(), scores_out);
   int best = 0;
   float bs = 0.0f;
   for (int i = 0; i < num; ++i)
@@ -314,6 +319,7 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out) {
 // ---------------------------------------------------------------------------
 // FindOffset::DoIt (FindOffset.cu:85-238)
 int find_offset(mf_series* s, float* offset_out) {
+  StageTimer timer(&s->ctx->c, kStageCoarse);
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   const int nx = s->nx, ny = s->ny, nz = s->nz, bin = 4;
@@ -323,7 +329,8 @@ int find_offset(mf_series* s, float* offset_out) {
   MF_TRY(s->upload_params());
   DevBuf corr, d_pairs, d_out;
   MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
-  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), nx, ny, nullptr, nz, s->d_sx.as<float>(),
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
+                            nx, ny, nullptr, nz, s->d_sx.as<float>(),
                             s->d_sy.as<float>(), s->d_rot.as<float>(), 0, bin, 0,
                             corr.as<float>(), xb, bpix, st));
   const int num = 31;
@@ -397,6 +404,7 @@ int find_offset(mf_series* s, float* offset_out) {
 // that the reference repeats for every pass: processing order, neighbour
 // ranges and the re-projection operators.
 int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
+  StageTimer timer(&s->ctx->c, kStageSetup);
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   if (nproj <= 0) return set_error(MF_ERR_ARG, "nproj must be > 0");
@@ -425,6 +433,10 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_TRY(P.ccbuf.alloc(sizeof(float) * ppix * 2));
   MF_TRY(P.part.alloc(sizeof(double2) * moment_parts(yb) * 2 + sizeof(float2) * kPeakParts));
   MF_TRY(P.stats.alloc(sizeof(float2) * 2));
+  // the round-edge mask of MeaAlignProj (one geometry for every tilt and pass)
+  MF_TRY(P.mask.alloc(sizeof(float) * bpix));
+  MF_TRY(make_round_mask(c, xb, yb, (float)((P.pad / 2 - 1) * 2) * 0.5f, (float)yb * 0.5f,
+                         (float)P.pad, (float)yb, 4.0f, P.mask.as<float>(), c->stream));
   // outward order (ProjAlign.cpp:151-176) and neighbour ranges
   P.zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
   std::vector<unsigned char> skip(nz, 1);
@@ -450,6 +462,7 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
     }
   }
   const int n = (int)P.order.size();
+  MF_TRY(fill_bp_device(c, s->angles.data(), &P.geom, st));
   P.ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
   MF_TRY(P.d_order.alloc(sizeof(int) * std::max(n, 1)));
   MF_TRY(P.d_err.alloc(sizeof(float) * nz));
@@ -524,7 +537,8 @@ static int pa_enqueue(mf_series* s) {
   float2* stats = P.stats.as<float2>();
   MF_CHECK_CUDA(cudaMemsetAsync(P.d_rowflags.p, 0, sizeof(int) * std::max(1, n * P.ytiles), st));
   // CorrTomoStack::DoIt: resample + bin + R-weight every tilt (CorrStack.cu:353-397)
-  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, nullptr, nz,
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
+                            s->nx, s->ny, nullptr, nz,
                             s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
                             P.bin, 1, scratch, pad, ppix, st));
   MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_all, scratch, (cufftComplex*)scratch));
@@ -564,7 +578,8 @@ static int pa_enqueue(mf_series* s) {
     // MeaAlignProj: PANorm both, FFT, filter, inverse FFT, peak
     const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
     MF_TRY(norm_mask_pad(c, reproj, corr + (size_t)ip * bpix, xb, 0, xb, yb, pad, ppix, 2, 0, mcx,
-                         mcy, (float)pad, (float)yb, 4.0f, cc, mpart, stats, st));
+                         mcy, (float)pad, (float)yb, 4.0f, P.mask.as<float>(), cc, mpart, stats,
+                         st));
     MF_CHECK_CUFFT(cufftExecR2C(P.cc_fwd, cc, (cufftComplex*)cc));
     MF_TRY(xcorr_filter(c, (cufftComplex*)cc, 0, nullptr, (cufftComplex*)(cc + ppix), 0, 1, cmp,
                         yb, 500.0f, 1.0f, st));
@@ -574,7 +589,8 @@ static int pa_enqueue(mf_series* s) {
                           s->d_rot.as<float>(), P.d_z0.as<float>(), P.d_err.as<float>(),
                           P.d_meas.as<float>(), st));
     // re-correct the aligned tilt (mCorrectProj)
-    MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, P.d_order.as<int>() + k, 1,
+    MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
+                              s->nx, s->ny, P.d_order.as<int>() + k, 1,
                               s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
                               P.bin, 1, scratch, pad, ppix, st));
     MF_CHECK_CUFFT(cufftExecR2C(P.rows_fwd_one, scratch, (cufftComplex*)scratch));
@@ -590,6 +606,7 @@ static int pa_enqueue(mf_series* s) {
 }
 
 int projalign_doit(mf_series* s, float* max_err_out) {
+  StageTimer timer(&s->ctx->c, kStagePass);
   ProjAlignState& P = s->pa;
   if (!P.ready) return set_error(MF_ERR_STATE, "projection matching is not set up");
   Context* c = &s->ctx->c;
@@ -669,7 +686,7 @@ int coarse_align(mf_series* s, float pitch_angle, float offset) {
     for (int i = 1; i <= 3; ++i) {
       float e, ax;
       MF_TRY(transform_doit(s, &e));
-      MF_TRY(tilt_axis(s, 180.0f / i, 100, &ax));
+      MF_TRY(tilt_axis(s, 180.0f / i, 100, &ax, nullptr));
     }
   } else {
     for (int i = 0; i < s->nz; ++i) s->rot[i] = pitch_angle;
@@ -710,7 +727,7 @@ int proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes) 
   MF_TRY(once());
   for (int i = 1; i <= 4; ++i) {
     float ax;
-    MF_TRY(tilt_axis(s, 20.0f / i, 100, &ax));
+    MF_TRY(tilt_axis(s, 20.0f / i, 100, &ax, nullptr));
     if (i == 1) MF_TRY(once());
   }
   MF_TRY(once());
@@ -720,12 +737,14 @@ int proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes) 
 
 // Process::CorrectStack (Process.cpp:329-372) into device memory.
 int correct_stack_device(mf_series* s, int out_bin, float* d_out) {
+  StageTimer timer(&s->ctx->c, kStageFinal);
   Context* c = &s->ctx->c;
   if (out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
   int xo = s->nx / out_bin / 2 * 2, yo = s->ny / out_bin / 2 * 2;
   if (xo < 2 || yo < 2) return set_error(MF_ERR_ARG, "output binning too large");
   MF_TRY(s->upload_params());
-  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->nx, s->ny, nullptr, s->nz,
+  MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
+                            s->nx, s->ny, nullptr, s->nz,
                             s->d_sx.as<float>(), s->d_sy.as<float>(), s->d_rot.as<float>(), 0,
                             out_bin, 1, d_out, xo, (size_t)xo * yo, c->stream));
   return MF_OK;

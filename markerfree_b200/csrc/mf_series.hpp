@@ -33,6 +33,7 @@ struct ProjAlignState {
   DevBuf ccbuf;     // 2 x yb x pad
   DevBuf part;      // reduction partials
   DevBuf stats;     // float2 x 2
+  DevBuf mask;      // yb x xb round-edge factors of the cross-correlation
   DevBuf d_order, d_err, d_z0, d_maxerr, d_meas, d_rowflags, d_bp;
   std::vector<size_t> bp_off;  // float offset of each tilt's geometry table in d_bp
   int ytiles = 0;
@@ -69,6 +70,8 @@ struct mf_series {
   int gpu = 0;
   int nx = 0, ny = 0, nz = 0;
   mf::DevBuf stack;  // pre-processed stack, nz x ny x nx
+  mf::DevBuf stack_t;  // the same, column-major per tilt (nz x nx x ny)
+  mf::DevBuf d_neg;    // nz ints: 1 when the pre-processed image holds a value below zero
   std::vector<float> file_angles;
   std::vector<float> angles;
   std::vector<float> sx, sy, rot;
@@ -84,7 +87,8 @@ struct mf_series {
 namespace mf {
 int series_init(mf_series* s, mf_context* ctx, int nx, int ny, int nz, const float* file_angles);
 int transform_doit(mf_series* s, float* max_err);
-int tilt_axis(mf_series* s, float range, int num, float* axis_out);
+// scores_out (num floats, may be null): the score of every candidate
+int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores_out);
 int find_offset(mf_series* s, float* offset_out);
 int projalign_setup(mf_series* s, float zshift, int align_z, int nproj);
 int projalign_doit(mf_series* s, float* max_err);

@@ -74,7 +74,9 @@ size_t estimate_bytes(int nx, int ny, int nz, const mf_options& o) {
   const size_t xb = nx / bin / 2 * 2, yb = ny / bin / 2 * 2;
   const size_t stack = (size_t)4 * nx * ny * nz;
   const size_t xo = nx / std::max(1, o.out_bin) / 2 * 2, yo = ny / std::max(1, o.out_bin) / 2 * 2;
-  return stack + (size_t)16 * xb * yb * nz + (size_t)4 * xo * yo * nz + ((size_t)64 << 20);
+  // the stack and its column-major copy (tilt-axis search), the binned working
+  // stacks of projection matching, the aligned output and fixed scratch
+  return 2 * stack + (size_t)16 * xb * yb * nz + (size_t)4 * xo * yo * nz + ((size_t)64 << 20);
 }
 
 }  // namespace

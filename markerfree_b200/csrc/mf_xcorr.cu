@@ -103,13 +103,46 @@ __global__ void __launch_bounds__(256) k_moments_final(const double2* __restrict
   stats[blockIdx.x] = make_float2(mean, sd);
 }
 
-// Normalise with stats, apply GRoundEdge, zero the pad columns; reads rows of
-// `src_stride` floats (first w used) and writes rows of `pad` floats.
+// The GRoundEdge factor of pixel (x, y) (CalcCC.cu:173-193) as nvcc compiles it:
+// fx*fx + fy*fy contracted, CUDA's cosf; -1 where the reference writes 0.
+__device__ __forceinline__ float round_edge(int x, int y, float cx, float cy, float msx,
+                                            float msy, float power) {
+  float fx = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)x, cx))), msx);
+  float fy = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)y, cy))), msy);
+  float fr = sqrtf(__fmaf_rn(fx, fx, __fmul_rn(fy, fy)));
+  if (fr >= 1.0f) return -1.0f;
+  fr = __fmul_rn(0.5f, __fsub_rn(1.0f, cosf(__fmul_rn(3.1415926f, fr))));
+  return __fsub_rn(1.0f, powf(fr, power));
+}
+
+// The factor for every pixel of a w x h image: it depends on the geometry only,
+// so a projection-matching pass reads it instead of evaluating cosf and powf for
+// every pixel of every image.
+__global__ void k_round_mask(int w, int h, float cx, float cy, float msx, float msy, float power,
+                             float* __restrict__ mask) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x < w && y < h) mask[(size_t)y * w + x] = round_edge(x, y, cx, cy, msx, msy, power);
+}
+
+int make_round_mask(Context* c, int w, int h, float cx, float cy, float msx, float msy,
+                    float power, float* d_mask, cudaStream_t st) {
+  dim3 blk(64, 4), grd((w + 63) / 64, (h + 3) / 4);
+  k_round_mask<<<grd, blk, 0, st>>>(w, h, cx, cy, msx, msy, power, d_mask);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Normalise with stats, apply GRoundEdge (from `mask` when given), zero the pad
+// columns; reads rows of `src_stride` floats (first w used) and writes rows of
+// `pad` floats.
 __global__ void k_norm_mask(const float* __restrict__ src, const float* __restrict__ src1,
                             int src_stride, size_t src_img_stride, int w, int h, int pad,
                             size_t dst_img_stride, const float2* __restrict__ stats, float cx,
                             float cy, float msx, float msy, float power,
-                            float* __restrict__ dst, ImgTable tab) {
+                            const float* __restrict__ mask, float* __restrict__ dst,
+                            ImgTable tab) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y * blockDim.y + threadIdx.y;
   int img = blockIdx.z;
@@ -121,29 +154,26 @@ __global__ void k_norm_mask(const float* __restrict__ src, const float* __restri
   }
   float v = table_ptr(tab, src, src1, src_img_stride, img)[(size_t)y * src_stride + x];
   float2 st = stats[img];
-  if (!(v < -1e10f)) v = __fdiv_rn(__fsub_rn(v, st.x), st.y);  // GNormalize
-  if (v < -1e10f) {                                             // GRoundEdge
+  if (!(v < -1e10f)) {  // GNormalize; a division by 1 (PANorm) is exact and skipped
+    v = __fsub_rn(v, st.x);
+    if (st.y != 1.0f) v = __fdiv_rn(v, st.y);
+  }
+  if (v < -1e10f) {  // GRoundEdge
     *d = 0.0f;
     return;
   }
-  float fx = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)x, cx))), msx);
-  float fy = __fdiv_rn(__fmul_rn(2.0f, fabsf(__fsub_rn((float)y, cy))), msy);
-  float fr = sqrtf(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)));
-  if (fr >= 1.0f) {
-    *d = 0.0f;
-    return;
-  }
-  fr = __fmul_rn(0.5f, __fsub_rn(1.0f, (float)cos((double)__fmul_rn(3.1415926f, fr))));
-  fr = __fsub_rn(1.0f, powf(fr, power));
-  *d = __fmul_rn(v, fr);
+  const float fr = mask ? __ldg(mask + (size_t)y * w + x)
+                        : round_edge(x, y, cx, cy, msx, msy, power);
+  *d = fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
 }
 
 int moment_parts(int h) { return (h + kMomRows - 1) / kMomRows; }
 
 int norm_mask_pad(Context* c, const float* src, const float* src1, int src_stride,
                   size_t src_img_stride, int w, int h, int pad, size_t dst_img_stride, int nimg,
-                  int with_std, float cx, float cy, float msx, float msy, float power, float* dst,
-                  double2* d_part, float2* d_stats, cudaStream_t st) {
+                  int with_std, float cx, float cy, float msx, float msy, float power,
+                  const float* mask, float* dst, double2* d_part, float2* d_stats,
+                  cudaStream_t st) {
   const int nb = moment_parts(h);
   const ImgTable tab{nullptr, nullptr};
   k_moments<<<dim3(nb, nimg), 256, 0, st>>>(src, src1, w, h, src_stride, src_img_stride, d_part,
@@ -151,7 +181,8 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
   k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, with_std, d_stats);
   dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
   k_norm_mask<<<grd, blk, 0, st>>>(src, src1, src_stride, src_img_stride, w, h, pad,
-                                   dst_img_stride, d_stats, cx, cy, msx, msy, power, dst, tab);
+                                   dst_img_stride, d_stats, cx, cy, msx, msy, power, mask, dst,
+                                   tab);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -159,15 +190,15 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
 
 int norm_mask_pad_group(Context* c, const float* const* d_ptrs, const int* active, int nimg,
                         int w, int h, int pad, size_t dst_img_stride, float cx, float cy,
-                        float msx, float msy, float power, float* dst, double2* d_part,
-                        float2* d_stats, cudaStream_t st) {
+                        float msx, float msy, float power, const float* mask, float* dst,
+                        double2* d_part, float2* d_stats, cudaStream_t st) {
   const int nb = moment_parts(h);
   const ImgTable tab{d_ptrs, active};
   k_moments<<<dim3(nb, nimg), 256, 0, st>>>(nullptr, nullptr, w, h, w, 0, d_part, tab);
   k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, 0, d_stats);
   dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
   k_norm_mask<<<grd, blk, 0, st>>>(nullptr, nullptr, w, 0, w, h, pad, dst_img_stride, d_stats,
-                                   cx, cy, msx, msy, power, dst, tab);
+                                   cx, cy, msx, msy, power, mask, dst, tab);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -194,16 +225,17 @@ __global__ void k_xcorr_filter(const cufftComplex* __restrict__ ref, size_t ref_
     B.x = __fmul_rn(B.x, scale);
     B.y = __fmul_rn(B.y, scale);
   }
-  float re = __fadd_rn(__fmul_rn(A.x, B.x), __fmul_rn(A.y, B.y));
-  float im = __fsub_rn(__fmul_rn(A.x, B.y), __fmul_rn(A.y, B.x));
+  // GConv + GWiener (CalcCC.cu:95-123) as nvcc compiles them: the first product of
+  // each sum of products fused, CUDA's expf
+  float re = __fmaf_rn(A.x, B.x, __fmul_rn(A.y, B.y));
+  float im = __fmaf_rn(A.x, B.y, -__fmul_rn(A.y, B.x));
   int yy = y;
   if (yy > ny / 2) yy -= ny;
   float fnx = __fmul_rn(2.0f, (float)(cmp - 1));
-  float filt = __fdiv_rn(__fmul_rn(-2.0f, bfactor),
-                         __fadd_rn(__fmul_rn(fnx, fnx), (float)(ny * ny)));
+  float filt = __fdiv_rn(__fmul_rn(-2.0f, bfactor), __fmaf_rn(fnx, fnx, (float)(ny * ny)));
   float k2 = (float)((unsigned)(x * x) + (unsigned)(yy * yy));
-  filt = (float)exp((double)__fmul_rn(filt, k2));
-  float amp = sqrtf(__fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im)));
+  filt = expf(__fmul_rn(filt, k2));
+  float amp = sqrtf(__fmaf_rn(re, re, __fmul_rn(im, im)));
   filt = __fdiv_rn(filt, sqrtf(__fadd_rn(amp, 0.01f)));
   re = __fmul_rn(re, filt);
   im = __fmul_rn(im, filt);
@@ -371,6 +403,10 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
   float a0 = __fmul_rn(shx, binx), a1 = __fmul_rn(shy, biny);
   float fs = __fadd_rn(__fmul_rn(a0, a0), __fmul_rn(a1, a1));
   fs = sqrtf(fs);
+  if (meas) {  // the shift the reference prints (ProjAlign.cpp:203)
+    meas[2 * ip] = a0;
+    meas[2 * ip + 1] = a1;
+  }
   float r = rot[ip];
   rot_shift(a0, a1, r, &a0, &a1);
   float i0, i1;
@@ -380,10 +416,6 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
   sx[ip] = __fadd_rn(sx[ip], a0);
   sy[ip] = __fadd_rn(sy[ip], a1);
   err[ip] = fs;
-  if (meas) {
-    meas[2 * ip] = shx;
-    meas[2 * ip + 1] = shy;
-  }
 }
 
 // Group form: blockIdx.x = series b, map b at maps + b * map_stride, partials
@@ -414,6 +446,8 @@ __global__ void k_pa_peak_update_group(const float* __restrict__ maps, size_t ma
   float a0 = __fmul_rn(shx, binx), a1 = __fmul_rn(shy, biny);
   float fs = __fadd_rn(__fmul_rn(a0, a0), __fmul_rn(a1, a1));
   fs = sqrtf(fs);
+  S.meas[2 * ip] = a0;  // the shift the reference prints (ProjAlign.cpp:203)
+  S.meas[2 * ip + 1] = a1;
   float r = S.rot[ip];
   rot_shift(a0, a1, r, &a0, &a1);
   float i0, i1;
@@ -423,8 +457,6 @@ __global__ void k_pa_peak_update_group(const float* __restrict__ maps, size_t ma
   S.sx[ip] = __fadd_rn(S.sx[ip], a0);
   S.sy[ip] = __fadd_rn(S.sy[ip], a1);
   S.err[ip] = fs;
-  S.meas[2 * ip] = shx;
-  S.meas[2 * ip + 1] = shy;
 }
 
 int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,

@@ -9,17 +9,22 @@ namespace mf {
 // padded FFT layout.  Image i is read from src + i*src_img_stride, except image 1
 // which is read from src1 when src1 is not null.  d_part needs
 // moment_parts(h) * nimg entries.
+// mask: the w x h table of make_round_mask for the same geometry, or null
 int norm_mask_pad(Context* c, const float* src, const float* src1, int src_stride,
                   size_t src_img_stride, int w, int h, int pad, size_t dst_img_stride, int nimg,
-                  int with_std, float cx, float cy, float msx, float msy, float power, float* dst,
-                  double2* d_part, float2* d_stats, cudaStream_t st);
+                  int with_std, float cx, float cy, float msx, float msy, float power,
+                  const float* mask, float* dst, double2* d_part, float2* d_stats,
+                  cudaStream_t st);
+// GRoundEdge factors of a w x h image (-1 where the mask is zero)
+int make_round_mask(Context* c, int w, int h, float cx, float cy, float msx, float msy,
+                    float power, float* d_mask, cudaStream_t st);
 int moment_parts(int h);
 // Group form: image i is d_ptrs[i] (w x h, dense rows); image pairs of series with
 // active[i / 2] == 0 are skipped.
 int norm_mask_pad_group(Context* c, const float* const* d_ptrs, const int* active, int nimg,
                         int w, int h, int pad, size_t dst_img_stride, float cx, float cy,
-                        float msx, float msy, float power, float* dst, double2* d_part,
-                        float2* d_stats, cudaStream_t st);
+                        float msx, float msy, float power, const float* mask, float* dst,
+                        double2* d_part, float2* d_stats, cudaStream_t st);
 // Group forms of the peak + parameter update, FitRotCenterZ and the pass maximum.
 int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,
                          int yb, float2* d_part, const GroupSeriesDev* ser,
@@ -57,10 +62,19 @@ int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
 // Common-line tilt-axis search over all tilts (Rotate.cu).  Scores (num floats)
 // are returned to the host; the caller applies the arg-max rule.
 struct AxisPlanCache;
-int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, int nx, int ny, int nz,
-                     const float* angles,
+// stack_t: the same stack column-major per tilt (transpose_stack); d_neg[z]: image
+// z holds a value below zero (null: assume it may).
+int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, const float* stack_t,
+                     const int* d_neg, int nx, int ny, int nz, const float* angles,
                      const float* sx, const float* sy, int zt, const float* rot_cand, int num,
                      int line_len, std::vector<float>* scores, cudaStream_t st);
+// d_c[i] = cosf(d_x[i]), d_s[i] = sinf(d_x[i]) on the device.
+int device_cos_sin(Context* ctx, const float* d_x, int n, float* d_c, float* d_s,
+                   cudaStream_t st);
+// out[z][x][y] = stack[z][y][x] for every tilt; neg[z] = 1 when image z holds a
+// value below zero, else 0.
+int transpose_stack(Context* c, const float* stack, int width, int height, int nz, float* out,
+                    int* neg, cudaStream_t st);
 
 // Tilt-angle offset search (FindOffset.cu): sums[6] per (offset, pair).
 struct OffsetPair {

@@ -13,8 +13,13 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stdint.h>
+
 #include <algorithm>
 #include <complex>
+#include <mutex>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "oc_fft.hpp"
@@ -24,12 +29,56 @@ namespace {
 const double D2R = 4.0 * atan(1.0) / 180.0;  // Markerfree/src/method/Util.h:33
 const float kBig = (float)-1e30;
 
-// The reference evaluates cosf/sinf/expf on the GPU; the oracle and the CUDA
-// library both use the correctly rounded value so that their index decisions
-// (nearest-neighbour bins, cell membership) agree exactly.
-inline float cosf_cr(float x) { return (float)cos((double)x); }
-inline float sinf_cr(float x) { return (float)sin((double)x); }
+// The reference evaluates cosf/sinf/expf on the GPU.  The oracle uses the
+// correctly rounded value of the same float argument unless a test has
+// registered CUDA's own cosf/sinf values for it (oc_trig_set: measured on the
+// GPU, not restated).  The two differ in the last place for some arguments, and
+// such a difference can move a nearest-neighbour index or a common-region end;
+// with the values registered the oracle takes the reference's decisions.
+// oc_trig_record collects the arguments a call evaluates, for registering.
+struct TrigTable {
+  std::unordered_map<uint32_t, std::pair<float, float>> v;  // bits of x -> (cos, sin)
+  bool recording = false;
+  std::unordered_set<uint32_t> seen;
+  std::mutex mu;
+};
+TrigTable& trig_table() {
+  static TrigTable t;
+  return t;
+}
+inline uint32_t fbits(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  return u;
+}
+inline bool trig_lookup(float x, float* c, float* s) {
+  TrigTable& t = trig_table();
+  if (t.recording) {
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.seen.insert(fbits(x));
+  }
+  if (t.v.empty()) return false;
+  auto it = t.v.find(fbits(x));
+  if (it == t.v.end()) return false;
+  *c = it->second.first;
+  *s = it->second.second;
+  return true;
+}
+inline float cosf_cr(float x) {
+  float c, s;
+  if (trig_lookup(x, &c, &s)) return c;
+  return (float)cos((double)x);
+}
+inline float sinf_cr(float x) {
+  float c, s;
+  if (trig_lookup(x, &c, &s)) return s;
+  return (float)sin((double)x);
+}
 inline float expf_cr(float x) { return (float)exp((double)x); }
+
+// x*c + yprod + o as nvcc compiles the reference's x*c - y*s + o and x*s + y*c + o:
+// the first product fused with the second, then the offset added.
+inline float lin2(float x, float c, float yprod, float o) { return std::fmaf(x, c, yprod) + o; }
 
 typedef std::complex<double> cd;
 
@@ -84,8 +133,9 @@ inline float corr_pixel(const float* img, int in_x, int in_y, int bx, int y, int
                         float sx, float sy, float cs, float sn, bool random_fill) {
   float ax = (float)bx + 0.5f - (float)out_x * 0.5f;
   float ay = (float)y + 0.5f - (float)out_y * 0.5f;
-  float t = ax * cs - ay * sn;
-  ay = ax * sn + ay * cs;
+  // nvcc fuses the first product of each sum in the reference's device code
+  float t = std::fmaf(ax, cs, -(ay * sn));
+  ay = std::fmaf(ax, sn, ay * cs);
   ax = t;
   ax += (sx + (float)in_x * 0.5f);
   ay += (sy + (float)in_y * 0.5f);
@@ -109,7 +159,7 @@ void rweight_rows(float* img, int xb, int yb) {
   std::vector<float> fr(cmp);
   for (int x = 0; x < cmp; ++x) {
     float r = (float)x / fN;
-    r = 2 * r * (0.55f + 0.45f * cosf_cr(6.2831852f * r));
+    r = 2 * r * std::fmaf(0.45f, cosf_cr(6.2831852f * r), 0.55f);
     fr[x] = r;
   }
 #pragma omp parallel
@@ -257,13 +307,13 @@ void reproject(const float* corr, int xb, int yb, int nz, const float* angles, i
           float fx = (float)ix + 0.5f - (float)W * 0.5f;
           float fint = 0.0f, fcount = 0.0f;
           for (int k = 0; k < nk; ++k) {
-            float v = fx * bc[k] + fz * bs[k] + cent_x;
+            float v = std::fmaf(fx, bc[k], fz * bs[k]) + cent_x;
             if (v < 0 || v > iend_x) continue;
             const float* row = corr + (size_t)(istart + k) * pix + (size_t)y * xb;
             float val = row[(int)v];
             if (val < (float)-1e10) val = kBig;
             if (val < (float)-1e20) continue;
-            fint += (val * bc[k] * bw[k]);
+            fint = std::fmaf(val * bc[k], bw[k], fint);
             fcount += bw[k];
           }
           slab[(size_t)iz * W + ix] = (fcount < 0.001f) ? kBig : fint / fcount;
@@ -274,8 +324,8 @@ void reproject(const float* corr, int xb, int yb, int nz, const float* angles, i
       const int nseg = ray_len / 512 + 1;
       for (int bx = 0; bx < xb; ++bx) {
         float fxp = (float)bx + 0.5f - (float)xb * 0.5f;
-        float tx = fxp * fcos + (float)W * 0.5f;
-        float tz = fxp * fsin + (float)T * 0.5f;
+        float tx = std::fmaf(fxp, fcos, (float)W * 0.5f);
+        float tz = std::fmaf(fxp, fsin, (float)T * 0.5f);
         float zst = -fxp * fsin / fcos - 0.5f * (float)ray_len;
         for (int t = 0; t < 512; ++t) {
           float s = 0.0f;
@@ -284,8 +334,8 @@ void reproject(const float* corr, int xb, int yb, int nz, const float* angles, i
             int j = seg * 512 + t;
             if (j >= ray_len) continue;
             float fz = (float)j + zst;
-            float fx = tx - fz * fsin;
-            fz = tz + fz * fcos;
+            float fx = std::fmaf(-fz, fsin, tx);
+            fz = std::fmaf(fz, fcos, tz);
             if (fx >= 0 && fx < iendx && fz >= 0 && fz < iendz) {
               float v = slab[(size_t)(int)fz * W + (int)fx];
               if (v >= (float)-1e10) {
@@ -350,7 +400,7 @@ void round_edge(float* img, int w, int h, int stride, float cx, float cy, float 
       }
       float fx = 2 * fabsf((float)x - cx) / sx;
       float fy = 2 * fabsf((float)y - cy) / sy;
-      float fr = sqrtf(fx * fx + fy * fy);
+      float fr = sqrtf(std::fmaf(fx, fx, fy * fy));
       if (fr >= 1.0f) {
         v = 0.0f;
         continue;
@@ -388,15 +438,15 @@ std::vector<float> xcorr_map(const std::vector<cd>& ref, std::vector<cd> img, in
       size_t i = (size_t)y * cx + x;
       float ar = (float)ref[i].real(), ai = (float)ref[i].imag();
       float br = (float)img[i].real(), bi = (float)img[i].imag();
-      float re = ar * br + ai * bi;
-      float im = ar * bi - ai * br;
+      float re = std::fmaf(ar, br, ai * bi);
+      float im = std::fmaf(ar, bi, -(ai * br));
       // Wiener / B-factor
       int yy = y;
       if (yy > (ny / 2)) yy -= ny;
       float fnx = 2.0f * (float)(cx - 1);
-      float filt = -2.0f * bfactor / (fnx * fnx + (float)(ny * ny));
+      float filt = -2.0f * bfactor / std::fmaf(fnx, fnx, (float)(ny * ny));
       filt = expf_cr(filt * (float)((unsigned)(x * x) + (unsigned)(yy * yy)));
-      float amp = sqrtf(re * re + im * im);
+      float amp = sqrtf(std::fmaf(re, re, im * im));
       filt /= sqrtf(amp + 0.01f);
       re *= filt;
       im *= filt;
@@ -478,6 +528,31 @@ void rot_shift(const float* in, float angle, float* out) {
 
 // ===========================================================================
 extern "C" {
+
+// Register cos/sin values for float arguments (replacing earlier ones); n = 0 clears.
+void oc_trig_set(int n, const float* x, const float* c, const float* s) {
+  TrigTable& t = trig_table();
+  if (n <= 0) t.v.clear();
+  for (int i = 0; i < n; ++i) t.v[fbits(x[i])] = std::make_pair(c[i], s[i]);
+}
+
+// on = 1: start collecting the arguments cosf/sinf are evaluated at; on = 0: stop.
+void oc_trig_record(int on) {
+  TrigTable& t = trig_table();
+  if (on) t.seen.clear();
+  t.recording = on != 0;
+}
+
+// The collected arguments: returns their number, writes at most `max`.
+int oc_trig_recorded(float* out, int max) {
+  TrigTable& t = trig_table();
+  int n = 0;
+  for (uint32_t u : t.seen) {
+    if (n < max) memcpy(out + n, &u, 4);
+    ++n;
+  }
+  return n;
+}
 
 int oc_frame_idx_from_tilt(int nz, const float* a, float t) { return frame_idx_from_tilt(nz, a, t); }
 int oc_find_ref_index(int nz, const float* a, int z) { return find_ref_index(nz, a, z); }
@@ -729,15 +804,15 @@ float oc_tilt_axis_scores(const float* stack, int nx, int ny, int nz, const floa
         size_t i = (size_t)b * L + y;
         float fy = (float)y - (float)L * 0.5f;
         for (int x = 1; x < half; ++x) {
-          float oxx = -x * fc - fy * fs + ox;
-          float oyy = -x * fs + fy * fc + oy;
+          float oxx = lin2((float)-x, fc, -(fy * fs), ox);
+          float oyy = lin2((float)-x, fs, fy * fc, oy);
           if (oxx < 0 || oxx >= nx) break;
           if (oyy < 0 || oyy >= ny) break;
           region[2 * i] = -x;
         }
         for (int x = 1; x < half; ++x) {
-          float oxx = x * fc - fy * fs + ox;
-          float oyy = x * fs + fy * fc + oy;
+          float oxx = lin2((float)x, fc, -(fy * fs), ox);
+          float oyy = lin2((float)x, fs, fy * fc, oy);
           if (oxx < 0 || oxx >= nx) break;
           if (oyy < 0 || oyy >= ny) break;
           region[2 * i + 1] = x;
@@ -763,10 +838,10 @@ float oc_tilt_axis_scores(const float* stack, int nx, int ny, int nz, const floa
         size_t i = (size_t)b * L + y;
         float sum = 0.0f;
         int cnt = 0;
-        int left = (int)((float)region[2 * i] * fcos_t + 0.5f);
+        int left = (int)std::fmaf((float)region[2 * i], fcos_t, 0.5f);
         for (int x = left; x < 0; ++x) {
-          float oxx = x * fcr - fy * fsr + ox;
-          float oyy = x * fsr + fy * fcr + oy;
+          float oxx = lin2((float)x, fcr, -(fy * fsr), ox);
+          float oyy = lin2((float)x, fsr, fy * fcr, oy);
           if (oxx < 0 || oxx >= nx) continue;
           if (oyy < 0 || oyy >= ny) continue;
           float v = proj[(size_t)(int)oyy * nx + (int)oxx];
@@ -774,10 +849,10 @@ float oc_tilt_axis_scores(const float* stack, int nx, int ny, int nz, const floa
           sum += v;
           cnt++;
         }
-        int right = (int)((float)region[2 * i + 1] * fcos_t + 0.5f);
+        int right = (int)std::fmaf((float)region[2 * i + 1], fcos_t, 0.5f);
         for (int x = 0; x < right; ++x) {
-          float oxx = x * fcr - fy * fsr + ox;
-          float oyy = x * fsr + fy * fcr + oy;
+          float oxx = lin2((float)x, fcr, -(fy * fsr), ox);
+          float oyy = lin2((float)x, fsr, fy * fcr, oy);
           if (oxx < 0 || oxx >= nx) continue;
           if (oyy < 0 || oyy >= ny) continue;
           float v = proj[(size_t)(int)oyy * nx + (int)oxx];
@@ -838,8 +913,8 @@ float oc_tilt_axis_scores(const float* stack, int nx, int ny, int nz, const floa
         float ri = sum[k].imag() * 1.0f + li * -1.0f;
         float f = (float)k / (2.0f * (float)(cmp - 1));
         f = expf_cr(-2.0f * 10.0f * f * f);
-        float a1 = sqrtf(rr * rr + ri * ri), a2 = sqrtf(lr * lr + li * li);
-        float c = (lr * rr + li * ri) * f / (a1 * a2 + (float)1e-20);
+        float a1 = sqrtf(std::fmaf(rr, rr, ri * ri)), a2 = sqrtf(std::fmaf(lr, lr, li * li));
+        float c = std::fmaf(lr, rr, li * ri) * f / std::fmaf(a1, a2, (float)1e-20);
         cc += c;
         sd += f;
       }

@@ -33,7 +33,10 @@ def build(force: bool = False) -> str:
                                                            os.path.join(_HERE, "oc_oracle.hpp")])
     if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < newest:
         os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
-        cmd = ["g++", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared", "-std=c++17",
+        # no contraction except the explicit std::fmaf calls, which -mfma makes single
+        # instructions
+        cmd = ["g++", "-O2", "-mfma", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+               "-std=c++17",
                "-o", _LIB_PATH] + _SOURCES
         subprocess.check_call(cmd)
     return _LIB_PATH
@@ -48,6 +51,11 @@ def lib():
         build()
         L = ctypes.CDLL(_LIB_PATH)
         L.oc_frame_idx_from_tilt.argtypes = [ctypes.c_int, _f32p, ctypes.c_float]
+        L.oc_trig_set.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p]
+        L.oc_trig_set.restype = None
+        L.oc_trig_record.argtypes = [ctypes.c_int]
+        L.oc_trig_record.restype = None
+        L.oc_trig_recorded.argtypes = [_f32p, ctypes.c_int]
         L.oc_find_ref_index.argtypes = [ctypes.c_int, _f32p, ctypes.c_int]
         L.oc_preprocess.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p]
         L.oc_binned_size.argtypes = [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int)] * 2
@@ -113,6 +121,14 @@ class Param:
         self.c.rotate = self.rotate.ctypes.data_as(fp)
         self.c.angle_offset = 0.0
 
+    def copy(self) -> "Param":
+        q = Param(self.shift_x.size)
+        q.shift_x[:] = self.shift_x
+        q.shift_y[:] = self.shift_y
+        q.rotate[:] = self.rotate
+        q.angle_offset = self.angle_offset
+        return q
+
     @property
     def angle_offset(self) -> float:
         return float(self.c.angle_offset)
@@ -127,6 +143,36 @@ class Param:
 
 def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def trig_set(x, c, s):
+    """Use these cos/sin values (CUDA's, measured on the GPU) for these float
+    arguments instead of the correctly rounded ones; trig_set([], [], []) clears."""
+    x, c, s = _f32(x), _f32(c), _f32(s)
+    lib().oc_trig_set(int(x.size), x, c, s)
+
+
+def trig_clear():
+    e = np.zeros(0, np.float32)
+    lib().oc_trig_set(0, e, e, e)
+
+
+class trig_recording:
+    """Context manager collecting the float arguments cos/sin are evaluated at;
+    .args holds them afterwards."""
+
+    def __enter__(self):
+        lib().oc_trig_record(1)
+        self.args = None
+        return self
+
+    def __exit__(self, *exc):
+        lib().oc_trig_record(0)
+        n = lib().oc_trig_recorded(np.zeros(1, np.float32), 0)
+        out = np.zeros(max(n, 1), np.float32)
+        lib().oc_trig_recorded(out, n)
+        self.args = out[:n]
+        return False
 
 
 def frame_idx_from_tilt(angles, tilt=0.0):

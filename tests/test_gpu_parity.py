@@ -208,6 +208,42 @@ def test_transform_and_axis_match_oracle(ctx, mflib):
     assert off_g == off_o
 
 
+@pytest.mark.parametrize("holes", [False, True])
+def test_tilt_axis_scores_match_oracle(ctx, mflib, holes):
+    """Every candidate's common-line score against the oracle, over a 180-degree
+    range (steep and flat candidate lines: both stack layouts of the Radon) and a
+    20-degree one.  With holes, some raw pixels hold the reference's sentinel, so
+    the pre-processed images carry values below zero that the Radon must skip."""
+    s0 = small_series(nx=256, ny=192, nz=21, step=3.0, seed=12)
+    raw = s0.stack.copy()
+    nz = raw.shape[0]
+    if holes:
+        rng = np.random.default_rng(4)
+        k = 400
+        raw[rng.integers(0, nz, k), rng.integers(0, raw.shape[1], k),
+            rng.integers(0, raw.shape[2], k)] = np.float32(-1e30)
+    st = O.preprocess(raw, s0.angles)
+    assert (st < 0).any() == holes
+    po = O.Param(nz)
+    s = mflib.Series(ctx, raw, s0.angles)
+    try:
+        for rng_deg in (180.0, 20.0):
+            # the oracle with CUDA's cosf/sinf for the arguments this search evaluates
+            with O.trig_recording() as rec:
+                O.tilt_axis_scores(st, s0.angles, po.copy(), rng_deg)
+            O.trig_set(rec.args, *ctx.device_cos_sin(rec.args))
+            ax_o, sc_o = O.tilt_axis_scores(st, s0.angles, po, rng_deg)
+            ax_g, sc_g = s.tilt_axis_scores(rng_deg)
+            # equal lines; the scores differ only through cuFFT's float spectra
+            np.testing.assert_allclose(sc_g, sc_o, rtol=2e-5, atol=2e-5 * np.abs(sc_o).max())
+            top = np.sort(sc_o)[-2:]
+            if top[1] - top[0] > 1e-4 * abs(top[1]):
+                assert ax_g == pytest.approx(ax_o, abs=1e-4)
+            po.rotate[:] = s.get_param().rotate  # both continue from the same axis
+    finally:
+        O.trig_clear()
+
+
 def test_correct_stack_matches_oracle(ctx, mflib, series):
     nz = series.stack.shape[0]
     st = O.preprocess(series.stack, series.angles)

@@ -11,14 +11,17 @@ the largest shift of each coarse stretch-correlation pass, the tilt axes of the
 coarse searches, and the largest shift and rotation centre of the first
 projection-matching pass.
 
-End to end, the reference is itself sensitive: the same input multiplied by
-1 + 1e-6 * U(-1, 1) (cases "<name>_p1", "<name>_p2") moves its final tilt axis by
-up to 1.8 degrees and its shifts by up to 0.7 px on low-SNR series (near-tied
-axis candidates flip, and nearest-neighbour re-correction amplifies the change
-in later passes), while on the well-conditioned hi384 series it moves by 0
-degrees and < 0.02 px.  So the final parameters must agree with one of the
-reference's runs within max(0.01 deg, its axis spread) and max(0.05 px, its shift
-spread): the north star's tolerances wherever the reference itself is stable.
+The reference is itself sensitive: the same input multiplied by
+1 + 1e-6 * U(-1, 1) (cases "<name>_p1" ... "<name>_p6", seeds 1-6) already moves
+the shifts it prints for the first projection-matching passes by 0.01 px, and
+its final tilt axis by up to 2.5 degrees and its shifts by up to 0.9 px on the
+low-SNR series (near-tied axis candidates flip, and nearest-neighbour
+re-correction amplifies the change in later passes); on the high-SNR hi384
+series five of its seven runs end on the same axis and the other two 0.017
+degrees away.  So each printed stage value is compared with the closest of the
+reference's runs, and the final parameters must agree with one of its runs
+within max(0.01 deg, its axis spread) and max(0.05 px, its shift spread): the
+stated tolerances wherever the reference itself is stable.
 """
 import itertools
 import json
@@ -46,35 +49,44 @@ def load(name):
     return g, s, angles
 
 
-def reference_runs(name):
-    runs = []
-    for suffix in ("", "_p1", "_p2"):
+def reference_logs(name):
+    """The reference's outputs for the case and for each of its perturbations."""
+    out = []
+    for suffix in [""] + [f"_p{k}" for k in range(1, 10)]:
         p = os.path.join(GOLD, f"ref_{name}{suffix}.json")
         if os.path.exists(p):
             with open(p) as f:
-                runs.append(np.array(json.load(f)["params"], np.float64))
-    return runs
+                out.append(json.load(f))
+    return out
+
+
+def reference_runs(name):
+    return [np.array(g["params"], np.float64) for g in reference_logs(name)]
 
 
 def events(g, kind):
     return [e[1:] for e in g["events"] if e[0] == kind]
 
 
+def closest(value, logs, kind, i):
+    """|value - printed| for the reference run that printed the closest value."""
+    return min(abs(value - events(g, kind)[i][0]) for g in logs)
+
+
 @pytest.mark.parametrize("name", ["c1s256", "c1s256b", "cfg1", "hi384"])
 def test_stages_match_reference_log(ctx, mflib, name):
     g, s, angles = load(name)
+    logs = reference_logs(name)
     ser = mflib.Series(ctx, s.stack, angles)
-    maxerr = events(g, "maxerr")
-    axes = events(g, "axis")
     same = True  # our trajectory still equals the reference's (to its printed digits)
     for i in range(3):
         e = ser.transform_doit()
         if same:
-            assert abs(e - maxerr[i][0]) < PRINT_TOL, (i, e, maxerr[i])
+            assert closest(e, logs, "maxerr", i) < PRINT_TOL, (i, e, events(g, "maxerr")[i])
         ax = ser.tilt_axis(180.0 / (i + 1))
         if i == 0:
-            assert abs(ax - axes[0][0]) < PRINT_TOL, (ax, axes[0])
-        same = same and abs(ax - axes[i][0]) < PRINT_TOL
+            assert closest(ax, logs, "axis", 0) < PRINT_TOL, (ax, events(g, "axis")[0])
+        same = same and closest(ax, logs, "axis", i) < PRINT_TOL
     if not same:
         return  # a near-tied axis candidate flipped; the final-parameter test covers the rest
     # -g 1e-4: no offset search, the offset is applied to the angles
@@ -85,16 +97,16 @@ def test_stages_match_reference_log(ctx, mflib, name):
     ser.set_param(p)
     ser.projalign_setup(0.0, g["thickness"], g["nproj"])
     e = ser.projalign_doit()
-    assert abs(e - events(g, "err")[0][0]) < PRINT_TOL
+    assert closest(e, logs, "err", 0) < PRINT_TOL, (e, [events(r, "err")[0] for r in logs])
     ser.projalign_doit()
-    assert abs(ser.z0 - events(g, "z0")[1][0]) < 0.02
+    assert closest(ser.z0, logs, "z0", 1) < 0.02
 
 
-@pytest.mark.parametrize("name", ["c1s256", "cfg1", "hi384"])
+@pytest.mark.parametrize("name", ["c1s256", "c1s256b", "cfg1", "hi384"])
 def test_final_parameters_within_reference_spread(ctx, mflib, name):
     g, s, angles = load(name)
     runs = reference_runs(name)
-    assert len(runs) >= 3, "perturbed reference runs missing"
+    assert len(runs) >= 7, "perturbed reference runs missing"
     ax_spread = max(abs(a[0, 1] - b[0, 1]) for a, b in itertools.combinations(runs, 2))
     sh_spread = max(np.abs(a[:, 2:4] - b[:, 2:4]).max() for a, b in itertools.combinations(runs, 2))
     ax_tol = max(AXIS_TOL, ax_spread)
@@ -113,3 +125,50 @@ def test_final_parameters_within_reference_spread(ctx, mflib, name):
           f"{[round(r[0, 1], 4) for r in runs]}, spread {ax_spread:.4f} deg / {sh_spread:.4f} px; "
           f"closest run: d_axis {best[1]:.4f} deg, d_shift {best[2]:.4f} px")
     assert best[0] <= 1.0, best
+
+
+def printed_pass(g, nz, k):
+    """(nz - 1, 3) rows (tilt angle, x shift, y shift) the run printed in projection-
+    matching pass k."""
+    return np.array(events(g, "meas")[k * (nz - 1):(k + 1) * (nz - 1)])
+
+
+@pytest.mark.parametrize("name", ["hi384", "c1s256", "cfg1"])
+def test_first_passes_match_reference_prints(ctx, mflib, name):
+    """Every per-tilt shift the reference printed in its first two projection-
+    matching passes, against one of its runs: within print rounding plus the
+    spread of the runs that follow that run's trajectory."""
+    g, s, angles = load(name)
+    logs = reference_logs(name)
+    nz = len(angles)
+    ser = mflib.Series(ctx, s.stack, angles)
+    for i in range(3):
+        ser.transform_doit()
+        ax = ser.tilt_axis(180.0 / (i + 1))
+        if closest(ax, logs, "axis", i) >= PRINT_TOL:
+            pytest.skip("coarse axis candidate flipped: later stages follow another trajectory")
+    ang = angles + np.float32(1e-4)
+    ser.angles = ang
+    p = ser.get_param()
+    p.shift_x[:] = 0
+    p.shift_y[:] = 0
+    ser.set_param(p)
+    ser.projalign_setup(0.0, g["thickness"], g["nproj"])
+    near = list(range(len(logs)))  # runs on the trajectory being followed
+    for k in range(2):
+        ser.projalign_doit()
+        m = ser.projalign_measured()
+        dev = {}
+        for i in near:
+            pr = printed_pass(logs[i], nz, k)
+            z = [int(np.argmin(np.abs(ang - a))) for a in pr[:, 0]]
+            dev[i] = float(np.abs(m[z] - pr[:, 1:]).max())
+        best = min(dev, key=dev.get)
+        ref = printed_pass(logs[best], nz, k)[:, 1:]
+        near = [i for i in near if np.abs(printed_pass(logs[i], nz, k)[:, 1:] - ref).max() < 0.1]
+        spread = max(float(np.abs(printed_pass(logs[i], nz, k)[:, 1:] -
+                                  printed_pass(logs[j], nz, k)[:, 1:]).max())
+                     for i in near for j in near)
+        print(f"{name} pass {k + 1}: deviation {dev[best]:.4f} from run {best}, "
+              f"spread of the {len(near)} runs on its trajectory {spread:.3f}")
+        assert dev[best] < PRINT_TOL + spread, (k, dev, spread)
