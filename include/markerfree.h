@@ -182,8 +182,10 @@ MF_API int mf_context_stage_times(mf_context* ctx, double* out6);
  * since the last call and then reset, in ms: [0] series creation (upload,
  * pre-processing), [1] coarse alignment (stretch correlations, offset search),
  * [2] tilt-axis searches, [3] projection-matching set-up, [4] projection-matching
- * passes, [5] aligned-stack output. */
-MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out6);
+ * passes, [5] aligned-stack output; and the tilt-axis Radon kernel alone:
+ * [6] its ms, [7] its launches, [8] the line samples it took, [9] its compulsory
+ * bytes (each tilt image read once, the line values written once). */
+MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out10);
 /* Diagnostic: CUDA's cosf and sinf of each of n float arguments (host arrays),
  * the values the kernels use where the reference's device code calls them.  A
  * CPU model of the path needs them to take the same nearest-neighbour decisions,

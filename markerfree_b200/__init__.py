@@ -237,9 +237,10 @@ class Context:
     def stage_breakdown(self) -> dict:
         """Wall ms per alignment stage accumulated since the previous call (stage
         timing on; see set_profiling)."""
-        out = (ctypes.c_double * 6)()
+        out = (ctypes.c_double * 10)()
         _check(lib().mf_context_stage_breakdown(self.h, out))
-        keys = ("prep_ms", "coarse_ms", "axis_ms", "setup_ms", "pass_ms", "output_ms")
+        keys = ("prep_ms", "coarse_ms", "axis_ms", "setup_ms", "pass_ms", "output_ms",
+                "radon_ms", "radon_launches", "radon_samples", "radon_bytes")
         return dict(zip(keys, out))
 
     def set_tc_rows(self, rows: int):

@@ -240,7 +240,8 @@ __global__ void k_radon(const float* __restrict__ stack, const float* __restrict
                         const int* __restrict__ neg, int width, int height, int L, int num,
                         const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
                         const float* __restrict__ sxs, const float* __restrict__ sys,
-                        const int* __restrict__ region, float* __restrict__ lines) {
+                        const int* __restrict__ region, float* __restrict__ lines,
+                        unsigned long long* __restrict__ samples) {
   int y = blockIdx.y * blockDim.x + threadIdx.x;
   int b = blockIdx.x;
   int z = blockIdx.z;
@@ -277,6 +278,11 @@ __global__ void k_radon(const float* __restrict__ stack, const float* __restrict
       radon_samples<false, false>(stack + off, width, ln, lo, hi, &sum, &cnt);
   }
   lines[((size_t)z * num + b) * (L + 2) + y] = (cnt == 0) ? kSentinel : __fdiv_rn(sum, (float)cnt);
+  if (samples) {  // stage timing: samples taken (one atomic per warp)
+    const unsigned m = __activemask();
+    const unsigned n = __reduce_add_sync(m, (unsigned)max(hi - lo, 0));
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(samples, (unsigned long long)n);
+  }
 }
 
 // GCalcMean + GRemoveMean (Rotate.cu:97-157) for one line per block of 512
@@ -449,9 +455,36 @@ int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, const flo
   MF_CHECK_CUDA(cudaMemcpyAsync(B.sy.p, sy, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
   k_common_region<<<dim3(num, (L + 127) / 128), dim3(1, 128), 0, st>>>(
       nx, ny, L, B.cs.as<float2>(), sx[zt], sy[zt], B.region.as<int>());
+  // with stage timing on, the Radon kernel is timed on its own and counts its samples
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  DevBuf count;
+  if (c->profiling) {
+    MF_TRY(count.alloc(sizeof(unsigned long long)));
+    MF_CHECK_CUDA(cudaMemsetAsync(count.p, 0, sizeof(unsigned long long), st));
+    MF_CHECK_CUDA(cudaEventCreate(&ev[0]));
+    MF_CHECK_CUDA(cudaEventCreate(&ev[1]));
+    MF_CHECK_CUDA(cudaEventRecord(ev[0], st));
+  }
   k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
       stack, stack_t, d_neg, nx, ny, L, num, B.cs.as<float2>(), B.tcos.as<float>(),
-      B.sx.as<float>(), B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>());
+      B.sx.as<float>(), B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>(),
+      count.as<unsigned long long>());
+  if (c->profiling) {
+    MF_CHECK_CUDA(cudaEventRecord(ev[1], st));
+    unsigned long long n = 0;
+    MF_CHECK_CUDA(cudaMemcpyAsync(&n, count.p, sizeof(n), cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    MF_CHECK_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    c->breakdown[kStageRadonMs] += ms;
+    c->breakdown[kStageRadonSamples] += (double)n;
+    c->breakdown[kStageRadonLaunches] += 1.0;
+    // compulsory bytes: every tilt image once, the line values written once
+    c->breakdown[kStageRadonBytes] +=
+        4.0 * (double)nx * ny * nz + 4.0 * (double)nz * num * (L + 2);
+  }
   k_line_prep<<<nz * num, 512, 0, st>>>(B.lines.as<float>(), L);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());

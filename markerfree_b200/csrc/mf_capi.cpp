@@ -95,10 +95,11 @@ MF_API int mf_context_stage_times(mf_context* ctx, double* out6) {
   return MF_OK;
 }
 
-MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out6) {
-  if (!ctx || !out6) return set_error(MF_ERR_ARG, "null argument");
+MF_API int mf_context_stage_breakdown(mf_context* ctx, double* out10) {
+  if (!ctx || !out10) return set_error(MF_ERR_ARG, "null argument");
+  static_assert(kStages == 10, "mf_context_stage_breakdown returns 10 values");
   for (int i = 0; i < kStages; ++i) {
-    out6[i] = ctx->c.breakdown[i];
+    out10[i] = ctx->c.breakdown[i];
     ctx->c.breakdown[i] = 0.0;
   }
   return MF_OK;

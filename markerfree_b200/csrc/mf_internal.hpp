@@ -86,8 +86,10 @@ struct FftPlan {
 // Stages of Context::breakdown: series creation (upload, pre-processing, the
 // column-major copy), coarse alignment (stretch correlations, offset search),
 // tilt-axis searches, projection-matching set-up, projection-matching passes,
-// aligned-stack output.
+// aligned-stack output; then the Radon kernel of the tilt-axis searches on its
+// own: its time, launches, samples taken and compulsory bytes.
 enum StageSlot { kStagePrep, kStageCoarse, kStageAxis, kStageSetup, kStagePass, kStageFinal,
+                 kStageRadonMs, kStageRadonLaunches, kStageRadonSamples, kStageRadonBytes,
                  kStages };
 
 struct Context {

@@ -363,6 +363,101 @@ void reproject(const float* corr, int xb, int yb, int nz, const float* angles, i
   }
 }
 
+// The same re-projection with every value accumulated in FP64 (back-projection
+// sums, slab cells, ray sums and means) and the same index decisions, taken in
+// FP32 exactly as above: the reference's discrete geometry with exact-as-possible
+// arithmetic, against which the FP32, FP16 and BF16 paths state their errors.
+void reproject_f64(const float* corr, int xb, int yb, int nz, const float* angles, int iproj,
+                   int istart, int iend, int thickness, double* out) {
+  (void)nz;
+  const float s_fD2R = 0.01745f;
+  const int W = 2 * xb, T = thickness;
+  const float proj_angle = angles[iproj];
+  int nk = iend - istart + 1;
+  std::vector<float> bw(nk), bc(nk), bs(nk);
+  for (int k = 0; k < nk; ++k) {
+    float a = angles[istart + k];
+    bw[k] = cosf_cr((proj_angle - a) * s_fD2R);
+    float v = a * s_fD2R;
+    bc[k] = cosf_cr(v);
+    bs[k] = sinf_cr(v);
+  }
+  const float fcos = (float)cos(D2R * proj_angle);
+  const float fsin = (float)sin(D2R * proj_angle);
+  const int ray_len = (int)((float)T / fcos + 0.5f);
+  const size_t pix = (size_t)xb * yb;
+#pragma omp parallel
+  {
+    std::vector<double> slab((size_t)W * T);
+    std::vector<double> lane_sum(512);
+    std::vector<int> lane_cnt(512);
+#pragma omp for schedule(dynamic, 4)
+    for (int y = 0; y < yb; ++y) {
+      // back-projection of one xz slice
+      const float cent_x = (float)xb * 0.5f;
+      const int iend_x = xb - 1;
+      for (int iz = 0; iz < T; ++iz) {
+        float fz = (float)iz + 0.5f - (float)T * 0.5f;
+        for (int ix = 0; ix < W; ++ix) {
+          float fx = (float)ix + 0.5f - (float)W * 0.5f;
+          double fint = 0.0, fcount = 0.0;
+          for (int k = 0; k < nk; ++k) {
+            float v = std::fmaf(fx, bc[k], fz * bs[k]) + cent_x;
+            if (v < 0 || v > iend_x) continue;
+            const float* row = corr + (size_t)(istart + k) * pix + (size_t)y * xb;
+            float val = row[(int)v];
+            if (val < (float)-1e10) val = kBig;
+            if (val < (float)-1e20) continue;
+            fint += (double)val * bc[k] * bw[k];
+            fcount += bw[k];
+          }
+          slab[(size_t)iz * W + ix] = (fcount < 0.001) ? (double)kBig : fint / fcount;
+        }
+      }
+      // forward projection: 512 lanes per ray, then a tree reduction
+      const int iendx = W - 1, iendz = T - 1;
+      const int nseg = ray_len / 512 + 1;
+      for (int bx = 0; bx < xb; ++bx) {
+        float fxp = (float)bx + 0.5f - (float)xb * 0.5f;
+        float tx = std::fmaf(fxp, fcos, (float)W * 0.5f);
+        float tz = std::fmaf(fxp, fsin, (float)T * 0.5f);
+        float zst = -fxp * fsin / fcos - 0.5f * (float)ray_len;
+        for (int t = 0; t < 512; ++t) {
+          double s = 0.0;
+          int c = 0;
+          for (int seg = 0; seg < nseg; ++seg) {
+            int j = seg * 512 + t;
+            if (j >= ray_len) continue;
+            float fz = (float)j + zst;
+            float fx = std::fmaf(-fz, fsin, tx);
+            fz = std::fmaf(fz, fcos, tz);
+            if (fx >= 0 && fx < iendx && fz >= 0 && fz < iendz) {
+              double v = slab[(size_t)(int)fz * W + (int)fx];
+              if (v >= -1e10) {
+                s += v;
+                c += 1;
+              }
+            }
+          }
+          lane_sum[t] = s;
+          lane_cnt[t] = c;
+        }
+        for (int h = 256; h > 0; h /= 2)
+          for (int t = 0; t < h; ++t) {
+            lane_sum[t] += lane_sum[t + h];
+            lane_cnt[t] += lane_cnt[t + h];
+          }
+        double r;
+        if ((float)lane_cnt[0] < 0.8f * (float)ray_len)
+          r = kBig;
+        else
+          r = lane_sum[0] / (double)lane_cnt[0];
+        out[(size_t)y * xb + bx] = r;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // CalcCC.cu:48-92 (CalcMoment: masked sum / (w*h)); accumulated in FP64 here.
 float calc_moment(const float* img, int w, int h, int stride, int e) {
@@ -573,6 +668,11 @@ void oc_find_proj_range(const float* angles, int nz, const unsigned char* skip, 
 void oc_reproject(const float* corr, int xb, int yb, int nz, const float* angles, int iproj,
                   int istart, int iend, int thickness, float* out) {
   reproject(corr, xb, yb, nz, angles, iproj, istart, iend, thickness, out);
+}
+
+void oc_reproject_f64(const float* corr, int xb, int yb, int nz, const float* angles, int iproj,
+                      int istart, int iend, int thickness, double* out) {
+  reproject_f64(corr, xb, yb, nz, angles, iproj, istart, iend, thickness, out);
 }
 
 void oc_measure_shift(const float* reproj, const float* proj, int xb, int yb, float* shift2,

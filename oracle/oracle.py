@@ -66,6 +66,9 @@ def lib():
                                          _i32p]
         L.oc_reproject.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p]
+        L.oc_reproject_f64.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]
         L.oc_measure_shift.argtypes = [_f32p, _f32p, ctypes.c_int, ctypes.c_int, _f32p,
                                        ctypes.POINTER(ctypes.c_float)]
         L.oc_projalign_create.restype = ctypes.c_void_p
@@ -218,6 +221,16 @@ def reproject(corr, angles, iproj, istart, iend, thickness):
     nz, yb, xb = corr.shape
     out = np.empty((yb, xb), np.float32)
     lib().oc_reproject(corr, xb, yb, nz, _f32(angles), iproj, istart, iend, thickness, out)
+    return out
+
+
+def reproject_f64(corr, angles, iproj, istart, iend, thickness):
+    """reproject() with every value accumulated in FP64 and the same FP32 index
+    decisions: the reference for the error statements of each precision."""
+    corr = _f32(corr)
+    nz, yb, xb = corr.shape
+    out = np.empty((yb, xb), np.float64)
+    lib().oc_reproject_f64(corr, xb, yb, nz, _f32(angles), iproj, istart, iend, thickness, out)
     return out
 
 

@@ -5,8 +5,8 @@ Measurement helper, not a test.  It needs the reference binary built by
 oracle/ref/build_ref.sh (oracle/_ref/Markerfree), this repository's build
 (markerfree_b200/_build/Markerfree) and one GPU.  It writes the 2048 x 2048 x 61
 tilt series (+-60 degrees in 2-degree steps, 300-px slab, seeded phantom) as an
-MRC (mode 2) + .rawtlt, then runs each program once to warm the file cache and
-the driver, then times RUNS runs of each with the same command-line options:
+MRC (mode 2) + .rawtlt, then times RUNS runs of each program (this library's
+after one untimed run that loads its kernels) with the same command-line options:
 
     -g 0.0001,0,0,0,300,1,0 -p 10 -s 0
 
@@ -17,7 +17,7 @@ each process is the series time including its file input and output.  Prints
 one JSON line with both times, the numbers of projection-matching passes and
 final tilt axes each printed, and the parameter differences.
 
-usage: python tests/golden/time_reference_b200.py OUTDIR [RUNS] [SCALE]
+usage: python tests/golden/time_reference_b200.py OUTDIR [RUNS] [SCALE] [REF_TIMEOUT_S]
 """
 from __future__ import annotations
 
@@ -60,6 +60,7 @@ def main():
     outdir = sys.argv[1]
     runs = int(sys.argv[2]) if len(sys.argv) > 2 else 2
     scale = float(sys.argv[3]) if len(sys.argv) > 3 else 1.0
+    ref_timeout = float(sys.argv[4]) if len(sys.argv) > 4 else 1800.0
     os.makedirs(outdir, exist_ok=True)
     s = synth.config(2, scale=scale)
     mrc = os.path.join(outdir, "series.mrc")
@@ -71,20 +72,24 @@ def main():
     flags = ["-a", tlt, "-g", f"0.0001,0,0,0,{s.thickness},1,0", "-p", "10", "-s", "0"]
     res = {"series": f"{s.stack.shape[2]}x{s.stack.shape[1]}x{s.stack.shape[0]}",
            "flags": " ".join(flags[2:]), "runs": runs}
-    for name, binary, tmo in (("reference", REF_BIN, 1800), ("ours", OUR_BIN, 600)):
+    for name, binary, tmo, warm in (("reference", REF_BIN, ref_timeout, 0),
+                                    ("ours", OUR_BIN, 600.0, 1)):
         out = os.path.join(outdir, f"{name}.mrc")
         cmd = [binary, "-i", mrc, "-o", out] + flags
         times = []
-        for k in range(runs + 1):  # the first run warms caches and is not counted
+        for k in range(runs + warm):
             log = os.path.join(outdir, f"{name}_{k}.log")
-            rc, wall = run(cmd, log, tmo)
+            try:
+                rc, wall = run(cmd, log, tmo)
+            except subprocess.TimeoutExpired:
+                rc, wall = "timeout", tmo
             if rc != 0:
                 res[name] = {"rc": rc, "log": log}
                 break
-            if k > 0:
+            if k >= warm:
                 times.append(wall)
         else:
-            passes, axis = passes_and_axis(os.path.join(outdir, f"{name}_1.log"))
+            passes, axis = passes_and_axis(os.path.join(outdir, f"{name}_{warm}.log"))
             res[name] = {"wall_s": times, "median_s": float(np.median(times)),
                          "series_per_min": 60.0 / float(np.median(times)),
                          "passes_printed": passes, "final_axis": axis}

@@ -152,3 +152,34 @@ def test_mixed_precision_pass_matches_oracle(ctx, mflib, prec):
         assert abs(e_g - e_o) < SHIFT_TOL_MIXED, (k, e_g, e_o)
         assert np.abs(g.shift_x - po.shift_x).max() < SHIFT_TOL_MIXED
         assert np.abs(g.shift_y - po.shift_y).max() < SHIFT_TOL_MIXED
+
+
+# relative L2 error of each path's re-projection against the FP64 restatement
+# (same discrete geometry, every value accumulated in FP64)
+REL_L2_VS_FP64 = {0: 1e-6, 1: 1e-6, 2: 2e-3, 3: 1.5e-2}
+
+
+@pytest.mark.parametrize("iproj,thick", [(10, 30), (2, 40)])
+def test_precision_errors_against_fp64(ctx, mflib, tall, iproj, thick):
+    """The error of every re-projection path against the FP64 oracle: the exact
+    FP32 gather (0), the FP32 banded operator (1), FP16 (2) and BF16 (3) operands
+    with FP32 accumulation.  The valid-pixel masks are identical."""
+    import torch
+    s, corr = tall
+    nz, yb, xb = corr.shape
+    ang = s.angles
+    i0, i1 = neighbours(ang, iproj)
+    want = O.reproject_f64(corr, ang, iproj, i0, i1, thick)
+    valid = want > -1e10
+    assert valid.any()
+    d_corr = to_dev(corr)
+    errs = {}
+    for method in (0, 1, 2, 3):
+        d_out = torch.full((yb, xb), 7.0, dtype=torch.float32, device="cuda")
+        mflib.dev_reproject(ctx, d_corr, xb, yb, nz, ang, iproj, i0, i1, thick, method, d_out)
+        got = d_out.cpu().numpy()
+        assert np.array_equal(got > -1e10, valid), method
+        errs[method] = rel_l2(got, want, valid)
+    print("relative L2 against FP64:", {k: f"{v:.2e}" for k, v in errs.items()})
+    for method, e in errs.items():
+        assert e < REL_L2_VS_FP64[method], (method, e)

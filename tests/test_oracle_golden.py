@@ -177,3 +177,22 @@ def test_xf_writer_layout(mflib, tmp_path):
     T2 = 4.0 - cy + s * cx + c * cy
     assert abs(first[4] - (T1 * c + T2 * s - cx + c * cx + s * cy)) < 2e-3
     assert txt[0].endswith(" ")  # the reference's trailing blank before the newline
+
+
+def test_fp64_reprojection_agrees_with_fp32_restatement():
+    """The FP64 re-projection (the reference for the precision error statements)
+    takes the same index decisions as the FP32 restatement and differs from it by
+    FP32 rounding only."""
+    s = synth.make_series(nx=120, ny=96, vol_z=24, n_blobs=40, tilt_min=-24, tilt_max=24,
+                          tilt_step=4.0, axis=86.0, shift_sd=2.0, snr=1.0, seed=9, thickness=20)
+    rng = np.random.default_rng(1)
+    corr = np.stack([O.correct_proj(s.stack[z], float(rng.normal(0, 2)), float(rng.normal(0, 2)),
+                                    86.0, binning=1, rweight=True)
+                     for z in range(s.stack.shape[0])])
+    w32 = O.reproject(corr, s.angles, 9, 3, 8, 20)
+    w64 = O.reproject_f64(corr, s.angles, 9, 3, 8, 20)
+    valid = w64 > -1e10
+    assert valid.any()
+    assert np.array_equal(valid, w32 > -1e10)
+    err = np.linalg.norm(w32[valid] - w64[valid]) / np.linalg.norm(w64[valid])
+    assert err < 1e-6, err
