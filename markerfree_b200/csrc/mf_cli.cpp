@@ -32,6 +32,7 @@ struct Options {
   int iteration = 0;
   float gamma = 0;
   int precision = MF_PREC_FP32;  // --precision (not in the reference)
+  bool timing = false;           // --timing (not in the reference): phase times on stderr
 };
 
 void usage() {
@@ -47,6 +48,7 @@ void usage() {
             << "[-s SAVE_MODE]\n    SaveParameter (0 or 1)\n"
             << "[--precision fp32|fp16|bf16]\n"
             << "    Re-projection operands (fp32 is the reference's arithmetic)\n"
+            << "[--timing]\n    Seconds spent reading, starting the GPU, aligning and writing\n"
             << "[-h]\n    Help\n";
 }
 
@@ -80,6 +82,7 @@ int get_opts(int argc, char** argv, Options* o) {
                                      {"savemode", required_argument, nullptr, 's'},
                                      {"nproj", required_argument, nullptr, 'p'},
                                      {"precision", required_argument, nullptr, 1000},
+                                     {"timing", no_argument, nullptr, 1001},
                                      {nullptr, 0, nullptr, 0}};
   int ch;
   while ((ch = getopt_long(argc, argv, "hi:o:n:a:g:m:s:p:", longopts, nullptr)) != -1) {
@@ -95,6 +98,9 @@ int get_opts(int argc, char** argv, Options* o) {
       case 'h':
         usage();
         return 0;
+      case 1001:
+        o->timing = true;
+        break;
       case 1000:
         if (strcmp(optarg, "fp32") == 0) {
           o->precision = MF_PREC_FP32;
@@ -179,9 +185,21 @@ int get_opts(int argc, char** argv, Options* o) {
 }
 
 // Process::DoIt (Process.cpp:34-92)
+double now_s() {
+  struct timeval t;
+  gettimeofday(&t, nullptr);
+  return t.tv_sec + t.tv_usec / 1e6;
+}
+
 void run(const Options& o) {
   struct timeval t0, t1;
   gettimeofday(&t0, nullptr);
+  double tp = now_s();
+  auto phase = [&](const char* name) {  // --timing: seconds since the previous phase
+    const double t = now_s();
+    if (o.timing) fprintf(stderr, "[timing] %s %.3f s\n", name, t - tp);
+    tp = t;
+  };
   int nx, ny, nz, mode;
   if (mf_mrc_info(o.input, &nx, &ny, &nz, &mode) != MF_OK) {
     printf("[Error] Cannot open input file: %s\n", o.input);
@@ -209,11 +227,13 @@ void run(const Options& o) {
   std::vector<float> angles(na);
   mf_read_angles(o.angle, angles.data(), na, &na);
   angles.resize(nz);
+  phase("read");
   mf_context* ctx = nullptr;
   if (mf_context_create(o.gpu, &ctx) != MF_OK) {
     printf("[Error] %s\n", mf_last_error());
     return;
   }
+  phase("gpu-init");
   mf_options mo;
   mo.offset = o.offset;
   mo.pitch_angle = o.pitch_angle;
@@ -232,6 +252,7 @@ void run(const Options& o) {
   std::vector<float> out((size_t)xo * yo * nz);
   int passes = 0;
   int rc = mf_align(ctx, raw.data(), nx, ny, nz, angles.data(), &mo, &p, out.data(), &passes);
+  phase("align");
   mf_context_destroy(ctx);
   if (rc != MF_OK) {
     printf("[Error] alignment failed: %s\n", mf_last_error());
@@ -241,6 +262,7 @@ void run(const Options& o) {
     printf("[Error] %s\n", mf_last_error());
     return;
   }
+  phase("write");
   gettimeofday(&t1, nullptr);
   double elapsed = (t1.tv_sec - t0.tv_sec) + (t1.tv_usec - t0.tv_usec) / 1e6;
   if (o.align_z != 0) {

@@ -102,31 +102,33 @@ __global__ void k_correct_bin(CorrArgs a) {
   }
   __syncthreads();
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= a.xb || by >= a.yb) return;
+  if (bx >= a.xb) return;
   const Layout L = pick_layout(a.stack_t, a.nx, a.ny, s_cs, s_sn);
   const float* img = (L.xs == 1 ? a.stack : a.stack_t) + (size_t)z * a.pix;
-  float res;
-  if (a.bin == 1) {
-    res = corr_pixel(img, L, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn,
-                     a.random_fill);
-  } else {
-    float sum = 0.0f;
-    bool bad = false;
-    for (int iy = 0; iy < a.biny && !bad; ++iy) {
-      for (int ix = 0; ix < a.binx; ++ix) {
-        float v = corr_pixel(img, L, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x,
-                             s_sx, s_sy, s_cs, s_sn, a.random_fill);
-        if (v < -1e10f) {
-          bad = true;
-          break;
+  // rows in a grid-stride loop: the set-up above is paid once per block
+  for (int by = blockIdx.y * blockDim.y + threadIdx.y; by < a.yb; by += gridDim.y * blockDim.y) {
+    float res;
+    if (a.bin == 1) {
+      res = corr_pixel(img, L, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn,
+                       a.random_fill);
+    } else {
+      float sum = 0.0f;
+      bool bad = false;
+      for (int iy = 0; iy < a.biny && !bad; ++iy) {
+        for (int ix = 0; ix < a.binx; ++ix) {
+          float v = corr_pixel(img, L, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x,
+                               s_sx, s_sy, s_cs, s_sn, a.random_fill);
+          if (v < -1e10f) {
+            bad = true;
+            break;
+          }
+          sum = __fadd_rn(sum, v);
         }
-        sum = __fadd_rn(sum, v);
       }
+      res = bad ? kSentinel : sum;
     }
-    res = bad ? kSentinel : sum;
+    a.out[(size_t)j * a.out_tilt_stride + (size_t)by * a.out_row_stride + bx] = res;
   }
-  a.out[(size_t)j * a.out_tilt_stride + (size_t)by * a.out_row_stride + bx] = res;
 }
 
 // k_correct_bin for a group of series: job j is tilt (j % nz) of series j / nz,
@@ -147,30 +149,39 @@ __global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int 
   }
   __syncthreads();
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= xb || by >= yb) return;
+  if (bx >= xb) return;
   const Layout L = pick_layout(S.stack_t, g.nx, g.ny, s_cs, s_sn);
   const float* img = (L.xs == 1 ? S.stack : S.stack_t) + (size_t)z * g.nx * g.ny;
-  float res;
-  if (g.bin == 1) {
-    res = corr_pixel(img, L, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
-  } else {
-    float sum = 0.0f;
-    bool bad = false;
-    for (int iy = 0; iy < biny && !bad; ++iy) {
-      for (int ix = 0; ix < binx; ++ix) {
-        float v = corr_pixel(img, L, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx,
-                             s_sy, s_cs, s_sn, g.random_fill);
-        if (v < -1e10f) {
-          bad = true;
-          break;
+  // rows in a grid-stride loop: the set-up above is paid once per block
+  for (int by = blockIdx.y * blockDim.y + threadIdx.y; by < yb; by += gridDim.y * blockDim.y) {
+    float res;
+    if (g.bin == 1) {
+      res = corr_pixel(img, L, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
+    } else {
+      float sum = 0.0f;
+      bool bad = false;
+      for (int iy = 0; iy < biny && !bad; ++iy) {
+        for (int ix = 0; ix < binx; ++ix) {
+          float v = corr_pixel(img, L, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx,
+                               s_sy, s_cs, s_sn, g.random_fill);
+          if (v < -1e10f) {
+            bad = true;
+            break;
+          }
+          sum = __fadd_rn(sum, v);
         }
-        sum = __fadd_rn(sum, v);
       }
+      res = bad ? kSentinel : sum;
     }
-    res = bad ? kSentinel : sum;
+    g.out[(size_t)j * g.out_tilt_stride + (size_t)by * g.out_row_stride + bx] = res;
   }
-  g.out[(size_t)j * g.out_tilt_stride + (size_t)by * g.out_row_stride + bx] = res;
+}
+
+// Row blocks of a resampling launch: each block walks about 16 of its row
+// groups, so the per-block set-up (parameter loads, cosf/sinf) is amortised.
+static int corr_row_blocks(int rows, int rows_per_block) {
+  const int groups = (rows + rows_per_block - 1) / rows_per_block;
+  return std::max(1, (groups + 15) / 16);
 }
 
 static void fill_sizes(CorrArgs* a, int nx, int ny, int bin) {
@@ -203,7 +214,7 @@ int launch_correct_bin(Context* c, const float* stack, const float* stack_t, int
   a.out = out;
   a.out_row_stride = out_row_stride;
   a.out_tilt_stride = out_tilt_stride;
-  dim3 blk(32, 8), grd((a.xb + 31) / 32, (a.yb + 7) / 8, ntilts);
+  dim3 blk(32, 8), grd((a.xb + 31) / 32, corr_row_blocks(a.yb, 8), ntilts);
   k_correct_bin<<<grd, blk, 0, st>>>(a);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
@@ -213,7 +224,7 @@ int launch_correct_bin(Context* c, const float* stack, const float* stack_t, int
 int launch_correct_group(Context* c, const GroupCorrArgs& g, int njobs, cudaStream_t st) {
   CorrArgs a{};
   fill_sizes(&a, g.nx, g.ny, g.bin);
-  dim3 blk(64, 4), grd((a.xb + 63) / 64, (a.yb + 3) / 4, njobs);
+  dim3 blk(64, 4), grd((a.xb + 63) / 64, corr_row_blocks(a.yb, 4), njobs);
   k_correct_group<<<grd, blk, 0, st>>>(g, a.out_x, a.xb, a.yb, a.binx, a.biny);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
@@ -238,7 +249,7 @@ int launch_correct_one(Context* c, const float* img, int nx, int ny, float sx, f
   a.out = out;
   a.out_row_stride = out_row_stride;
   a.out_tilt_stride = 0;
-  dim3 blk(32, 8), grd((a.xb + 31) / 32, (a.yb + 7) / 8, 1);
+  dim3 blk(32, 8), grd((a.xb + 31) / 32, corr_row_blocks(a.yb, 8), 1);
   k_correct_bin<<<grd, blk, 0, st>>>(a);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());

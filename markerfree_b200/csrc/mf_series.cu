@@ -196,15 +196,19 @@ int transform_doit(mf_series* s, float* max_err_out) {
     MF_CHECK_CUDA(cudaMemcpyAsync(d_refidx.p, ref_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
     MF_CHECK_CUDA(cudaMemcpyAsync(d_mats.p, mats.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
     const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
+    if (!T.mask.p) {  // one geometry for every stretch correlation of the series
+      MF_TRY(T.mask.alloc(sizeof(float) * bpix));
+      MF_TRY(make_round_mask(c, xb, yb, cx, cy, msx, msy, 4.0f, T.mask.as<float>(), st));
+    }
     // references: normalise (mean, std) + round edge, all tilts
     MF_TRY(norm_mask_pad(c, pbuf.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy,
-                         msx, msy, 4.0f, nullptr, refs.as<float>(), part.as<double2>(),
+                         msx, msy, 4.0f, T.mask.as<float>(), refs.as<float>(), part.as<double2>(),
                          stats.as<float2>(), st));
     // images: stretch the padded raw copy, then normalise + round edge
     MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
                         np, 1, imgs.as<float>(), ppix, st));
     MF_TRY(norm_mask_pad(c, imgs.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy,
-                         msx, msy, 4.0f, nullptr, imgs.as<float>(), part.as<double2>(),
+                         msx, msy, 4.0f, T.mask.as<float>(), imgs.as<float>(), part.as<double2>(),
                          stats.as<float2>(), st));
     cufftHandle fr, fi, inv;
     MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));

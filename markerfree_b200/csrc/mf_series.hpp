@@ -61,6 +61,7 @@ struct TransformState {
   bool ready = false;
   int bin = 1, xb = 0, yb = 0;
   std::vector<float> pshx, pshy;
+  DevBuf mask;  // yb x xb round-edge factors of the stretch correlations
 };
 
 }  // namespace mf

@@ -57,7 +57,14 @@ __device__ __forceinline__ double2 block_sum2(double a, double b) {
 }
 
 // Masked moments: part[img][blk] = (sum v, sum v^2) over the valid pixels of
-// kMomRows rows.  Image 1 is read from src1 when it is given.
+// kMomRows rows.  Image 1 is read from src1 when it is given.  Rows and images
+// start on 8-byte boundaries (even widths and strides), so each thread reads
+// column pairs, the kMomRows rows of a pair all in flight before it adds them.
+__device__ __forceinline__ void moment_add(float v, double* a, double* b) {
+  const bool ok = !(v < -1e10f);  // sentinels are skipped
+  *a += ok ? (double)v : 0.0;
+  *b += ok ? (double)__fmul_rn(v, v) : 0.0;
+}
 __global__ void __launch_bounds__(256) k_moments(const float* __restrict__ src0,
                                                  const float* __restrict__ src1, int w, int h,
                                                  int stride, size_t img_stride,
@@ -65,16 +72,23 @@ __global__ void __launch_bounds__(256) k_moments(const float* __restrict__ src0,
   if (table_skip(tab, blockIdx.y)) return;
   const float* p = table_ptr(tab, src0, src1, img_stride, blockIdx.y);
   double a = 0.0, b = 0.0;
-  const int y0 = blockIdx.x * kMomRows, y1 = min(h, y0 + kMomRows);
-  for (int y = y0; y < y1; ++y) {
-    const float* r = p + (size_t)y * stride;
-    for (int x = threadIdx.x; x < w; x += blockDim.x) {
-      float v = __ldg(r + x);
-      if (v < -1e10f) continue;
-      a += v;
-      b += (double)__fmul_rn(v, v);
+  const int y0 = blockIdx.x * kMomRows, nrows = min(h - y0, kMomRows);
+  const int npair = w >> 1;
+  for (int q = threadIdx.x; q < npair; q += blockDim.x) {
+    float2 v[kMomRows];
+#pragma unroll
+    for (int k = 0; k < kMomRows; ++k)
+      v[k] = k < nrows ? __ldg(reinterpret_cast<const float2*>(p + (size_t)(y0 + k) * stride) + q)
+                       : make_float2(-1e30f, -1e30f);
+#pragma unroll
+    for (int k = 0; k < kMomRows; ++k) {
+      moment_add(v[k].x, &a, &b);
+      moment_add(v[k].y, &a, &b);
     }
   }
+  if ((w & 1) && threadIdx.x == 0)  // an odd last column
+    for (int k = 0; k < nrows; ++k)
+      moment_add(__ldg(p + (size_t)(y0 + k) * stride + w - 1), &a, &b);
   double2 s = block_sum2(a, b);
   if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
@@ -278,6 +292,7 @@ __global__ void __launch_bounds__(256) k_peak_partial(const float* __restrict__ 
   float bv = -INFINITY;
   int bi = INT_MAX;
   for (int y = r0; y < r1; ++y) {
+#pragma unroll 4
     for (int x = sx + threadIdx.x; x < ex; x += blockDim.x) {
       int li = y * stride + x;
       float v = __ldg(m + li);

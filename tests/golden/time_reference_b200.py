@@ -13,7 +13,8 @@ after one untimed run that loads its kernels) with the same command-line options
 (a non-zero angle offset, so the reference's offset search, which reduces with a
 __syncthreads() inside a divergent branch, never runs).  Both programs read the
 MRC, align and write the aligned stack and the parameter file; the wall time of
-each process is the series time including its file input and output.  Prints
+each process is the series time including its file input and output (this
+library's program also prints the split: read, GPU start-up, align, write).  Prints
 one JSON line with both times, the numbers of projection-matching passes and
 final tilt axes each printed, and the parameter differences.
 
@@ -75,7 +76,8 @@ def main():
     for name, binary, tmo, warm in (("reference", REF_BIN, ref_timeout, 0),
                                     ("ours", OUR_BIN, 600.0, 1)):
         out = os.path.join(outdir, f"{name}.mrc")
-        cmd = [binary, "-i", mrc, "-o", out] + flags
+        # this library's program also reports its phases (--timing, on stderr)
+        cmd = [binary, "-i", mrc, "-o", out] + flags + (["--timing"] if name == "ours" else [])
         times = []
         for k in range(runs + warm):
             log = os.path.join(outdir, f"{name}_{k}.log")
@@ -93,6 +95,10 @@ def main():
             res[name] = {"wall_s": times, "median_s": float(np.median(times)),
                          "series_per_min": 60.0 / float(np.median(times)),
                          "passes_printed": passes, "final_axis": axis}
+            txt = open(os.path.join(outdir, f"{name}_{warm}.log"), errors="replace").read()
+            phases = re.findall(r"\[timing\] (\S+) ([0-9.]+) s", txt)
+            if phases:
+                res[name]["phases_s"] = {k: float(v) for k, v in phases}
             p = parse_txt(out.replace(".mrc", ".txt"))
             res[name + "_params"] = p
         if os.path.exists(out):
