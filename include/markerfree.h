@@ -167,6 +167,18 @@ MF_API int mf_align(mf_context* ctx, const float* raw_stack, int nx, int ny, int
 MF_API int mf_align_device(mf_context* ctx, const float* d_raw_stack, int nx, int ny, int nz,
                            const float* file_angles, const mf_options* opt, mf_align_param* param,
                            float* d_aligned_out, int* passes);
+/* Process::DoIt (Markerfree/src/main/Process.cpp:34-92) from file to file, minus
+ * the parameter file (write it with mf_save_param): reads the MRC stack (modes
+ * 0/1/2) at in_mrc, aligns it with the angles as read from the .rawtlt file
+ * (nz of them, nz from mf_mrc_info) and writes the aligned float32 stack to
+ * out_mrc (NULL: no stack) with mf_mrc_write's header.  Slices stream through
+ * two page-locked buffers in blocks of about 64 MB: a block is read from the
+ * file while the previous one is copied to the GPU (8- and 16-bit samples are
+ * converted to float there), and on output a block is written while the next is
+ * copied back.  Results equal mf_align's on the same data. */
+MF_API int mf_align_file(mf_context* ctx, const char* in_mrc, const float* file_angles,
+                         const mf_options* opt, mf_align_param* param, const char* out_mrc,
+                         int* passes);
 
 /* Stage timing: when enabled, every projection-matching pass records CUDA events
  * around each held-out tilt's re-projection and cross-correlation work (also
@@ -230,7 +242,7 @@ MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_ra
 /* ---- serving: continuous batching of requests ------------------------------
  * Not in the reference.  A server keeps `workers` streams busy with requests
  * (tilt series) that arrive at any time: a request is admitted when its
- * estimated device memory fits in `hbm_budget` bytes (0 = 90% of the free
+ * estimated device memory fits in `hbm_budget` bytes (0 = 80% of the free
  * memory), prepared on its own (upload, pre-processing, coarse alignment), then
  * projection-matched in a group with other prepared requests of its shape (up to
  * `max_group`; a request waits at most `group_wait_ms` for companions while more

@@ -93,6 +93,9 @@ SIGNATURES = [
     ("mf_align_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, _f32p, ctypes.POINTER(OptionsC),
                                        ctypes.POINTER(AlignParamC), ctypes.c_void_p, _c_int_p]),
+    ("mf_align_file", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _f32p,
+                                     ctypes.POINTER(OptionsC), ctypes.POINTER(AlignParamC),
+                                     ctypes.c_char_p, _c_int_p]),
     ("mf_context_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mf_context_stage_times", ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_double)]),
@@ -396,6 +399,23 @@ def align(ctx: Context, raw_stack, file_angles, offset=0.0, pitch_angle=0.0, zsh
     return p, out, n.value
 
 
+def align_file(ctx: Context, in_mrc: str, file_angles, out_mrc=None, offset=0.0,
+               pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10,
+               precision=PREC_FP32):
+    """mf_align_file: MRC stack in, aligned MRC stack out (streamed through pinned
+    buffers).  Returns (Param, passes)."""
+    nx, ny, nz, _ = mrc_info(in_mrc)
+    p = Param(nz)
+    c = p.c()
+    o = OptionsC(offset, pitch_angle, zshift, 0, align_z, out_bin, 0, nproj, 0, precision)
+    n = ctypes.c_int()
+    _check(lib().mf_align_file(ctx.h, in_mrc.encode(), _f32(file_angles)[:nz], ctypes.byref(o),
+                               ctypes.byref(c), out_mrc.encode() if out_mrc else None,
+                               ctypes.byref(n)))
+    p.angle_offset = c.angle_offset
+    return p, n.value
+
+
 def align_device(ctx: Context, d_raw, nx, ny, nz, file_angles, d_out, offset=0.0,
                  pitch_angle=0.0, zshift=0.0, align_z=600, out_bin=1, nproj=10,
                  precision=PREC_FP32):
@@ -585,6 +605,14 @@ def dev_measure_shift(ctx: Context, d_reproj, d_proj, xb, yb):
 
 
 # -- files --
+def mrc_info(path: str):
+    """(nx, ny, nz, mode) of an MRC file."""
+    nx, ny, nz, mode = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().mf_mrc_info(path.encode(), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz),
+                             ctypes.byref(mode)))
+    return nx.value, ny.value, nz.value, mode.value
+
+
 def mrc_read(path: str):
     nx, ny, nz, mode = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     _check(lib().mf_mrc_info(path.encode(), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz),

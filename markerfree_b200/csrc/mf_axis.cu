@@ -190,17 +190,14 @@ __device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsi
 // kNonNeg: the image holds no value below zero, so the reference's skip of such
 // samples never fires and every sample counts.
 // An in-range coordinate (0 <= X < 2^23) is truncated by a round-toward-zero add
-// of 2^23: the low bits of the sum are (int)X, and the address is formed from the
-// biased bits, the biases removed from the base address once.
+// of 2^23: the low bits of the sum are (int)X, and the index is formed from the
+// biased bits in 32-bit modular arithmetic, the bias removed once.
 template <bool kByColumn, bool kNonNeg>
 __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, int stride,
                                               const RadonLine& ln, int lo, int hi, float* sum_out,
                                               int* cnt_out) {
-  constexpr uint64_t kBias = 0x4B000000u;  // bits of 2^23
-  // address of pixel (major, minor) = base + 4 * (major_bits * stride + minor_bits),
-  // the biases of both coordinates taken off the base once (64-bit modular sums)
-  const uint64_t base = (uint64_t)(uintptr_t)proj - 4ull * (kBias * (uint64_t)stride + kBias);
-  const uint64_t row_bytes = 4ull * (uint64_t)stride;
+  constexpr unsigned kBias = 0x4B000000u;  // bits of 2^23
+  const unsigned bias_idx = kBias * (unsigned)stride + kBias;  // mod 2^32
   const unsigned long long cs2 = pack2(ln.c, ln.s), y2 = pack2(ln.ys, ln.yc);
   const unsigned long long o2 = pack2(ln.ox, ln.oy), big2 = pack2(8388608.0f, 8388608.0f);
   const unsigned long long one2 = pack2(1.0f, 1.0f);
@@ -215,9 +212,9 @@ __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, in
     float tx, ty;
     unpack2(t, &tx, &ty);
     const unsigned bx = __float_as_uint(tx), by = __float_as_uint(ty);
-    const unsigned major = kByColumn ? bx : by, minor = kByColumn ? by : bx;
-    const float v = __ldg(reinterpret_cast<const float*>(base + (uint64_t)major * row_bytes +
-                                                         4ull * (uint64_t)minor));
+    const unsigned idx = (kByColumn ? bx * (unsigned)stride + by : by * (unsigned)stride + bx) -
+                         bias_idx;
+    const float v = __ldg(proj + idx);
     if (!kNonNeg) {
       if (v < 0) continue;
       cnt++;

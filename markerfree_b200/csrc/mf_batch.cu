@@ -378,9 +378,11 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   if (g->use_graph && !g->graph && !c->profiling) {
     int64_t l0 = c->launches;
     cudaGraph_t gr = nullptr;
+    std::unique_lock<std::recursive_mutex> fft_lock(fft_mutex());
     MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = group_enqueue(g);
     cudaError_t ec = cudaStreamEndCapture(st, &gr);
+    fft_lock.unlock();
     g->graph_kernels = c->launches - l0;
     c->launches = l0;
     if (rc != MF_OK || ec != cudaSuccess) {

@@ -1,4 +1,5 @@
 // extern "C" entry points (include/markerfree.h).
+#include <algorithm>
 #include <cstring>
 #include <new>
 
@@ -412,6 +413,164 @@ MF_API int mf_align_device(mf_context* ctx, const float* d_raw, int nx, int ny, 
   MF_GUARD_BEGIN
   return align_common(ctx, d_raw, true, nx, ny, nz, file_angles, opt, param, d_aligned_out,
                       passes);
+  MF_GUARD_END
+}
+
+}  // extern "C"
+
+namespace {
+
+// File samples of MRC mode 0 (8-bit), 1 (16-bit) or 2 (float) to float, as
+// mrcstack.cpp:56-116 converts them on the host.
+__global__ void k_mrc_to_float(const void* __restrict__ src, int mode, size_t n,
+                               float* __restrict__ dst) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float v;
+    if (mode == 0)
+      v = (float)static_cast<const unsigned char*>(src)[i];
+    else if (mode == 1)
+      v = (float)static_cast<const short*>(src)[i];
+    else
+      v = static_cast<const float*>(src)[i];
+    dst[i] = v;
+  }
+}
+
+// Two page-locked host buffers for streaming between a file and the device.
+struct PinnedPair {
+  void* p[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int init(size_t bytes) {
+    for (int k = 0; k < 2; ++k) {
+      MF_CHECK_CUDA(cudaHostAlloc(&p[k], bytes, cudaHostAllocDefault));
+      MF_CHECK_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+    }
+    return MF_OK;
+  }
+  ~PinnedPair() {
+    for (int k = 0; k < 2; ++k) {
+      if (ev[k]) cudaEventSynchronize(ev[k]);
+      if (ev[k]) cudaEventDestroy(ev[k]);
+      if (p[k]) cudaFreeHost(p[k]);
+    }
+    cudaGetLastError();
+  }
+};
+
+struct FileCloser {
+  FILE* f = nullptr;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+
+constexpr size_t kStreamChunk = (size_t)64 << 20;  // bytes per streamed block of slices
+
+// Read the stack of an MRC file into d_raw (float, file order): whole slices in
+// blocks of about kStreamChunk bytes, each read into one of two pinned buffers
+// while the other one's block is copied to the device (and converted there for
+// modes 0 and 1).
+int upload_mrc(mf_context* ctx, FILE* f, int nx, int ny, int nz, int mode, float* d_raw) {
+  cudaStream_t st = ctx->c.stream;
+  const size_t pix = (size_t)nx * ny, psize = mode == 0 ? 1 : (mode == 1 ? 2 : 4);
+  const size_t slice = pix * psize;
+  const int per = (int)std::max<size_t>(1, kStreamChunk / slice);
+  PinnedPair pin;
+  MF_TRY(pin.init(slice * per));
+  DevBuf stage[2];
+  if (mode != 2)
+    for (int k = 0; k < 2; ++k) MF_TRY(stage[k].alloc(slice * per));
+  for (int z0 = 0, c = 0; z0 < nz; z0 += per, ++c) {
+    const int k = c & 1, n = std::min(per, nz - z0);
+    MF_CHECK_CUDA(cudaEventSynchronize(pin.ev[k]));  // the block that used this buffer is done
+    if (fread(pin.p[k], 1, slice * n, f) != slice * n)
+      return set_error(MF_ERR_FORMAT, "MRC file is truncated at slice %d", z0);
+    float* dst = d_raw + (size_t)z0 * pix;
+    if (mode == 2) {
+      MF_CHECK_CUDA(cudaMemcpyAsync(dst, pin.p[k], slice * n, cudaMemcpyHostToDevice, st));
+    } else {
+      MF_CHECK_CUDA(cudaMemcpyAsync(stage[k].p, pin.p[k], slice * n, cudaMemcpyHostToDevice, st));
+      k_mrc_to_float<<<ctx->c.sm_count * 4, 256, 0, st>>>(stage[k].p, mode, pix * n, dst);
+      ctx->c.launches++;
+      MF_CHECK_CUDA(cudaGetLastError());
+    }
+    MF_CHECK_CUDA(cudaEventRecord(pin.ev[k], st));
+  }
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+// Write the aligned stack d_out (nz x yo x xo float) as an MRC file: the header
+// from the middle slice, then blocks of slices, each copied from the device into
+// one pinned buffer while the previous block is written from the other.
+int download_mrc(mf_context* ctx, const float* d_out, int xo, int yo, int nz, const char* path) {
+  cudaStream_t st = ctx->c.stream;
+  const size_t pix = (size_t)xo * yo, slice = pix * sizeof(float);
+  const int per = (int)std::max<size_t>(1, kStreamChunk / slice);
+  PinnedPair pin;
+  MF_TRY(pin.init(slice * per));
+  // header: statistics of the middle slice (mf_mrc_write's rule)
+  const int zm = (int)(nz * .5);
+  MF_CHECK_CUDA(cudaMemcpyAsync(pin.p[0], d_out + (size_t)zm * pix, slice, cudaMemcpyDeviceToHost,
+                                st));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  unsigned char hdr[1024];
+  mrc_float_header(static_cast<const float*>(pin.p[0]), xo, yo, nz, hdr);
+  FileCloser fc;
+  fc.f = fopen(path, "wb");
+  if (!fc.f) return set_error(MF_ERR_IO, "cannot open %s for writing", path);
+  if (fwrite(hdr, 1, sizeof(hdr), fc.f) != sizeof(hdr))
+    return set_error(MF_ERR_IO, "write failed on %s", path);
+  const int nblk = (nz + per - 1) / per;
+  auto issue = [&](int c) -> int {
+    const int z0 = c * per, n = std::min(per, nz - z0);
+    MF_CHECK_CUDA(cudaMemcpyAsync(pin.p[c & 1], d_out + (size_t)z0 * pix, slice * n,
+                                  cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaEventRecord(pin.ev[c & 1], st));
+    return MF_OK;
+  };
+  MF_TRY(issue(0));
+  for (int c = 0; c < nblk; ++c) {
+    if (c + 1 < nblk) MF_TRY(issue(c + 1));  // its buffer's previous block was written
+    MF_CHECK_CUDA(cudaEventSynchronize(pin.ev[c & 1]));
+    const size_t n = (size_t)std::min(per, nz - c * per);
+    if (fwrite(pin.p[c & 1], 1, slice * n, fc.f) != slice * n)
+      return set_error(MF_ERR_IO, "write failed on %s", path);
+  }
+  const int rc = fclose(fc.f);
+  fc.f = nullptr;
+  if (rc != 0) return set_error(MF_ERR_IO, "write failed on %s", path);
+  return MF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+MF_API int mf_align_file(mf_context* ctx, const char* in_mrc, const float* file_angles,
+                         const mf_options* opt, mf_align_param* param, const char* out_mrc,
+                         int* passes) {
+  MF_GUARD_BEGIN
+  if (!in_mrc || !file_angles || !opt || !param) return set_error(MF_ERR_ARG, "null argument");
+  MF_TRY(use_device(ctx));
+  FileCloser in;
+  int nx = 0, ny = 0, nz = 0, mode = 0;
+  MF_TRY(mrc_open_stack(in_mrc, &in.f, &nx, &ny, &nz, &mode));
+  DevBuf raw;
+  MF_TRY(raw.alloc(sizeof(float) * (size_t)nx * ny * nz));
+  MF_TRY(upload_mrc(ctx, in.f, nx, ny, nz, mode, raw.as<float>()));
+  fclose(in.f);
+  in.f = nullptr;
+  int xo = 0, yo = 0;
+  mf_binned_size(nx, ny, std::max(1, opt->out_bin), &xo, &yo);
+  DevBuf out;
+  if (out_mrc) MF_TRY(out.alloc(sizeof(float) * (size_t)xo * yo * nz));
+  MF_TRY(align_common(ctx, raw.as<float>(), true, nx, ny, nz, file_angles, opt, param,
+                      out_mrc ? out.as<float>() : nullptr, passes));
+  raw.release();
+  if (out_mrc) MF_TRY(download_mrc(ctx, out.as<float>(), xo, yo, nz, out_mrc));
+  return MF_OK;
   MF_GUARD_END
 }
 

@@ -48,7 +48,7 @@ void usage() {
             << "[-s SAVE_MODE]\n    SaveParameter (0 or 1)\n"
             << "[--precision fp32|fp16|bf16]\n"
             << "    Re-projection operands (fp32 is the reference's arithmetic)\n"
-            << "[--timing]\n    Seconds spent reading, starting the GPU, aligning and writing\n"
+            << "[--timing]\n    Seconds spent starting the GPU and streaming + aligning\n"
             << "[-h]\n    Help\n";
 }
 
@@ -207,12 +207,6 @@ void run(const Options& o) {
     printf("[Abort] DoIt() stopped due to input file loading failure.\n");
     return;
   }
-  std::vector<float> raw((size_t)nx * ny * nz);
-  if (mf_mrc_read(o.input, raw.data()) != MF_OK) {
-    printf("[Error] %s\n", mf_last_error());
-    printf("[Abort] DoIt() stopped due to input file loading failure.\n");
-    return;
-  }
   int na = 0;
   if (mf_read_angles(o.angle, nullptr, 0, &na) != MF_OK) {
     printf("[Error] Cannot open angle file: %s\n", o.angle);
@@ -227,7 +221,7 @@ void run(const Options& o) {
   std::vector<float> angles(na);
   mf_read_angles(o.angle, angles.data(), na, &na);
   angles.resize(nz);
-  phase("read");
+  phase("header+angles");
   mf_context* ctx = nullptr;
   if (mf_context_create(o.gpu, &ctx) != MF_OK) {
     printf("[Error] %s\n", mf_last_error());
@@ -247,22 +241,16 @@ void run(const Options& o) {
   mo.precision = o.precision;
   std::vector<float> sx(nz), sy(nz), rot(nz);
   mf_align_param p{sx.data(), sy.data(), rot.data(), 0.0f};
-  int xo, yo;
-  mf_binned_size(nx, ny, o.out_bin, &xo, &yo);
-  std::vector<float> out((size_t)xo * yo * nz);
   int passes = 0;
-  int rc = mf_align(ctx, raw.data(), nx, ny, nz, angles.data(), &mo, &p, out.data(), &passes);
-  phase("align");
+  // the stack streams from the input file to the GPU and the aligned stack back to
+  // the output file (reading, copies and writing overlapped)
+  int rc = mf_align_file(ctx, o.input, angles.data(), &mo, &p, o.output, &passes);
+  phase("read-align-write");
   mf_context_destroy(ctx);
   if (rc != MF_OK) {
     printf("[Error] alignment failed: %s\n", mf_last_error());
     return;
   }
-  if (mf_mrc_write(o.output, out.data(), xo, yo, nz) != MF_OK) {
-    printf("[Error] %s\n", mf_last_error());
-    return;
-  }
-  phase("write");
   gettimeofday(&t1, nullptr);
   double elapsed = (t1.tv_sec - t0.tv_sec) + (t1.tv_usec - t0.tv_usec) / 1e6;
   if (o.align_z != 0) {

@@ -63,7 +63,10 @@ void DevBuf::release() {
 FftPlan::~FftPlan() { release(); }
 
 void FftPlan::release() {
-  if (valid) cufftDestroy(h);
+  if (valid) {
+    std::lock_guard<std::recursive_mutex> lk(fft_mutex());
+    cufftDestroy(h);
+  }
   valid = false;
 }
 

@@ -6,6 +6,8 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -20,6 +22,8 @@ constexpr float kSentinel = -1e30f;
 
 // ---- error reporting ------------------------------------------------------
 int set_error(int code, const char* fmt, ...);
+// The lock every cuFFT call and stream capture of the process holds (mf_series.cu).
+std::recursive_mutex& fft_mutex();
 #define MF_CHECK_CUDA(call)                                                          \
   do {                                                                               \
     cudaError_t e_ = (call);                                                         \
@@ -29,6 +33,7 @@ int set_error(int code, const char* fmt, ...);
   } while (0)
 #define MF_CHECK_CUFFT(call)                                                         \
   do {                                                                               \
+    std::lock_guard<std::recursive_mutex> fft_lk_(mf::fft_mutex());                  \
     cufftResult r_ = (call);                                                         \
     if (r_ != CUFFT_SUCCESS)                                                         \
       return mf::set_error(MF_ERR_CUFFT, "%s:%d %s: cufft error %d", __FILE__,       \
@@ -57,6 +62,11 @@ void set_alloc_stream(cudaStream_t s);
 void set_sync_free(bool on);
 // The stream DevBuf::release frees on in this thread (null: each buffer's own).
 void set_free_stream(cudaStream_t s);
+
+// MRC helpers shared by the file entry points (mf_io.cpp): the float32 output
+// header from the middle slice, and an input stack opened at its first data byte.
+void mrc_float_header(const float* mid, int nx, int ny, int nz, void* out1024);
+int mrc_open_stack(const char* path, FILE** fp, int* nx, int* ny, int* nz, int* mode);
 
 struct DevBuf {
   void* p = nullptr;

@@ -108,8 +108,12 @@ MF_API int mf_mrc_read(const char* path, float* out) {
   return MF_OK;
 }
 
-MF_API int mf_mrc_write(const char* path, const float* data, int nx, int ny, int nz) {
-  if (!path || !data || nx <= 0 || ny <= 0 || nz <= 0) return set_error(MF_ERR_ARG, "invalid MRC write");
+}  // extern "C"
+
+namespace mf {
+
+// The float32 output header: InitializeHeader + SetSize + UpdateHeader.
+void mrc_float_header(const float* mid, int nx, int ny, int nz, void* out1024) {
   MrcHeader h;
   memset(&h, 0, sizeof(h));
   // InitializeHeader + SetSize (mrcstack.cpp:421-454, mrcstack.h:170-175)
@@ -129,7 +133,6 @@ MF_API int mf_mrc_write(const char* path, const float* data, int nx, int ny, int
   // UpdateHeader (mrcstack.cpp:456-501): statistics of the middle slice only,
   // amax starting from FLT_MIN, sentinels skipped.
   size_t pix = (size_t)nx * ny;
-  const float* mid = data + (size_t)(int)(nz * .5) * pix;
   float amin = FLT_MAX, amax = FLT_MIN;
   long double amean = 0;
   int count = 0;
@@ -146,9 +149,41 @@ MF_API int mf_mrc_write(const char* path, const float* data, int nx, int ny, int
   h.amax = amax;
   h.amean = (float)amean;
   h.nlabl = 0;
+  memcpy(out1024, &h, sizeof(h));
+}
+
+// Open an MRC stack for reading, positioned at its first data byte.
+int mrc_open_stack(const char* path, FILE** fp, int* nx, int* ny, int* nz, int* mode) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return set_error(MF_ERR_IO, "Cannot open input file: %s", path);
+  MrcHeader h;
+  int rc = read_header(f, &h);
+  if (rc == MF_OK && fseeko(f, (off_t)sizeof(MrcHeader) + h.next, SEEK_SET) != 0)
+    rc = set_error(MF_ERR_IO, "seek failed in %s", path);
+  if (rc != MF_OK) {
+    fclose(f);
+    return rc;
+  }
+  *fp = f;
+  *nx = h.nx;
+  *ny = h.ny;
+  *nz = h.nz;
+  *mode = h.mode;
+  return MF_OK;
+}
+
+}  // namespace mf
+
+extern "C" {
+
+MF_API int mf_mrc_write(const char* path, const float* data, int nx, int ny, int nz) {
+  if (!path || !data || nx <= 0 || ny <= 0 || nz <= 0) return set_error(MF_ERR_ARG, "invalid MRC write");
+  const size_t pix = (size_t)nx * ny;
+  unsigned char h[1024];
+  mf::mrc_float_header(data + (size_t)(int)(nz * .5) * pix, nx, ny, nz, h);
   FILE* f = fopen(path, "wb");
   if (!f) return set_error(MF_ERR_IO, "cannot open %s for writing", path);
-  bool ok = fwrite(&h, 1, sizeof(h), f) == sizeof(h);
+  bool ok = fwrite(h, 1, sizeof(h), f) == sizeof(h);
   ok = ok && fwrite(data, sizeof(float), pix * nz, f) == pix * nz;
   ok = (fclose(f) == 0) && ok;
   if (!ok) return set_error(MF_ERR_IO, "write failed on %s", path);

@@ -20,13 +20,18 @@
 
 using namespace mf;
 
-// cuFFT plan creation and destruction are serialised across the process: plans
-// created at the same time from several threads (the serving workers) crashed
-// inside cuFFT's planner.  Execution on distinct plans needs no lock.
-static std::mutex g_plan_mu;
+// Every cuFFT call of the process (planning, execution, destruction) and every
+// stream capture (which records cuFFT launches) holds one lock: plans created
+// while other threads (the serving workers) planned, executed or captured
+// crashed inside cuFFT's planner.  Executions are asynchronous launches, so the
+// lock is held for microseconds.
+std::recursive_mutex& mf::fft_mutex() {
+  static std::recursive_mutex m;
+  return m;
+}
 
 mf_context::~mf_context() {
-  std::lock_guard<std::mutex> lk(g_plan_mu);
+  std::lock_guard<std::recursive_mutex> lk(fft_mutex());
   for (auto& kv : plans) cufftDestroy(kv.second);
   plans.clear();
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -40,7 +45,17 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   }
   // key: kind (0 rows R2C in place, 1 rows C2R out of place, 2 2-D R2C in place,
   //            3 2-D C2R in place), nx, ny, batch
-  std::lock_guard<std::mutex> lk(g_plan_mu);
+  std::lock_guard<std::recursive_mutex> lk(fft_mutex());
+  // cuFFT allocates its work areas with cudaMalloc, outside the stream-ordered
+  // pool: refuse (instead of letting the planner fail inside cuFFT) when the
+  // device is nearly full.
+  {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < ((size_t)1 << 30))
+      return set_error(MF_ERR_NOMEM, "%zu MB of device memory left for an FFT plan",
+                       fr >> 20);
+    cudaGetLastError();
+  }
   long long kind = key[0];
   int nx = (int)key[1], ny = (int)key[2], batch = (int)key[3];
   int pad = (nx / 2 + 1) * 2, cmp = nx / 2 + 1;
@@ -630,9 +645,11 @@ int projalign_doit(mf_series* s, float* max_err_out) {
     // later pass replays it unchanged.
     int64_t l0 = c->launches;
     cudaGraph_t g = nullptr;
+    std::unique_lock<std::recursive_mutex> fft_lock(fft_mutex());
     MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = pa_enqueue(s);
     cudaError_t ec = cudaStreamEndCapture(st, &g);
+    fft_lock.unlock();
     P.graph_kernels = c->launches - l0;
     c->launches = l0;
     if (rc != MF_OK || ec != cudaSuccess) {

@@ -19,6 +19,7 @@ one JSON line with both times, the numbers of projection-matching passes and
 final tilt axes each printed, and the parameter differences.
 
 usage: python tests/golden/time_reference_b200.py OUTDIR [RUNS] [SCALE] [REF_TIMEOUT_S]
+(REF_TIMEOUT_S <= 0 times this library's program only)
 """
 from __future__ import annotations
 
@@ -73,8 +74,10 @@ def main():
     flags = ["-a", tlt, "-g", f"0.0001,0,0,0,{s.thickness},1,0", "-p", "10", "-s", "0"]
     res = {"series": f"{s.stack.shape[2]}x{s.stack.shape[1]}x{s.stack.shape[0]}",
            "flags": " ".join(flags[2:]), "runs": runs}
-    for name, binary, tmo, warm in (("reference", REF_BIN, ref_timeout, 0),
-                                    ("ours", OUR_BIN, 600.0, 1)):
+    programs = [("reference", REF_BIN, ref_timeout, 0), ("ours", OUR_BIN, 600.0, 1)]
+    if ref_timeout <= 0:
+        programs = programs[1:]
+    for name, binary, tmo, warm in programs:
         out = os.path.join(outdir, f"{name}.mrc")
         # this library's program also reports its phases (--timing, on stderr)
         cmd = [binary, "-i", mrc, "-o", out] + flags + (["--timing"] if name == "ours" else [])
