@@ -245,9 +245,11 @@ MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_ra
  * estimated device memory fits in `hbm_budget` bytes (0 = 80% of the free
  * memory), prepared on its own (upload, pre-processing, coarse alignment), then
  * projection-matched in a group with other prepared requests of its shape (up to
- * `max_group`; a request waits at most `group_wait_ms` for companions while more
- * of its shape are on their way).  A request's result equals the one it gets
- * when aligned alone. */
+ * `max_group`).  A worker runs a full group first, then prepares admitted
+ * requests (so that same-shape requests join the ready groups), then runs a group
+ * whose oldest request has waited `group_wait_ms` or has no companion on the way;
+ * no request waits longer than 20 x `group_wait_ms` once prepared.  A request's
+ * result equals the one it gets when aligned alone. */
 typedef struct mf_server mf_server;
 MF_API int mf_server_create(int gpu, size_t hbm_budget, int max_group, int workers,
                             double group_wait_ms, mf_server** out);

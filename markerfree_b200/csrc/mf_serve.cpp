@@ -133,28 +133,39 @@ struct mf_server {
         if (group_key(j) == key) return true;
       return preparing > 0;
     };
-    for (auto& kv : by_shape) {
-      std::vector<Job*>& v = kv.second;
-      std::sort(v.begin(), v.end(), [](Job* a, Job* b) { return a->t_ready < b->t_ready; });
-      const bool full = (int)v.size() >= max_group;
-      const bool waited = t - v.front()->t_ready >= group_wait_s;
-      if (full || waited || !coming(kv.first)) {
-        const int m = std::min((int)v.size(), max_group);
-        group->assign(v.begin(), v.begin() + m);
-        for (Job* j : *group) {
-          j->state = kMatching;
-          ready.erase(std::find(ready.begin(), ready.end(), j));
-        }
-        return true;
+    auto take = [&](std::vector<Job*>& v) {
+      const int m = std::min((int)v.size(), max_group);
+      group->assign(v.begin(), v.begin() + m);
+      for (Job* j : *group) {
+        j->state = kMatching;
+        ready.erase(std::find(ready.begin(), ready.end(), j));
       }
-      *wait_s = std::min(*wait_s, std::max(1e-3, group_wait_s - (t - v.front()->t_ready)));
-    }
+      return true;
+    };
+    for (auto& kv : by_shape)
+      std::sort(kv.second.begin(), kv.second.end(),
+                [](Job* a, Job* b) { return a->t_ready < b->t_ready; });
+    // 1. a full group, or one whose oldest job has waited too long, runs first
+    const double starve_s = 20.0 * group_wait_s;
+    for (auto& kv : by_shape)
+      if ((int)kv.second.size() >= max_group || t - kv.second.front()->t_ready >= starve_s)
+        return take(kv.second);
+    // 2. preparing admitted jobs comes next: it lets same-shape jobs join the
+    //    ready groups, so the matching that follows runs on larger groups
     if (!admitted.empty()) {
       *prep = admitted.front();
       admitted.erase(admitted.begin());
       (*prep)->state = kPreparing;
       preparing++;
       return true;
+    }
+    // 3. with nothing to prepare, a group runs once it has waited the grouping
+    //    window or no job of its shape is on the way
+    for (auto& kv : by_shape) {
+      std::vector<Job*>& v = kv.second;
+      const bool waited = t - v.front()->t_ready >= group_wait_s;
+      if (waited || !coming(kv.first)) return take(v);
+      *wait_s = std::min(*wait_s, std::max(1e-3, group_wait_s - (t - v.front()->t_ready)));
     }
     return false;
   }
