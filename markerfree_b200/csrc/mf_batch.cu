@@ -45,7 +45,10 @@ struct mf_group {
   cufftHandle cc_fwd = 0, cc_inv = 0;
   cudaGraphExec_t graph = nullptr;
   int64_t graph_kernels = 0;
-  bool use_graph = true;
+  // Group passes launch eagerly: capturing and instantiating the graph of a group
+  // pass (thousands of nodes, 8 series) cost more than its six replays saved
+  // (bench step 2058 ms with the graph, 1564 ms without).
+  bool use_graph = false;
   std::vector<cudaEvent_t> events;  // 3 per step when the context profiles
   double op_bytes = 0, op_fma = 0;  // mean compulsory bytes / MACs of one operator apply
   ~mf_group() {
