@@ -8,10 +8,11 @@
 // precision and runs the i-th held-out tilt of every series together: each stage
 // of the pass (correction, R-weight FFTs, re-projection, normalisation,
 // cross-correlation FFTs, filter, peak and parameter update, re-correction) is
-// one launch over the whole group.  The pass is captured once into a CUDA graph;
-// a per-series `active` flag in device memory lets the same graph serve every
-// iteration of ProjAlignOnce even though each series leaves that loop after its
-// own number of passes.  Results per series are the same as when the series is
+// one launch over the whole group.  A per-series `active` flag in device memory
+// lets the same launches serve every iteration of ProjAlignOnce even though each
+// series leaves that loop after its own number of passes (the pass can also be
+// captured once into a CUDA graph; `use_graph` below says why it is not by
+// default).  Results per series are the same as when the series is
 // aligned alone: the per-series arithmetic and its order are unchanged.
 #include <algorithm>
 #include <cstring>
