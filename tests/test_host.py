@@ -162,3 +162,26 @@ def test_oracle_fft_matches_numpy():
         back = np.zeros((ny, nx))
         L.oc_irfft2(np.ascontiguousarray(out), back, nx, ny)
         assert np.abs(back / (nx * ny) - x).max() < 1e-9
+
+
+def test_entry_points_reject_bad_arguments_before_touching_the_gpu(mflib):
+    """Argument checks of the serving, group, file and tilt-axis entry points come
+    before any CUDA call, so they hold on a host without a GPU."""
+    import ctypes
+    L = mflib.lib()
+    srv = ctypes.c_void_p()
+    # groups hold 1..32 series, servers run 1..16 workers
+    for max_group, workers in ((0, 1), (33, 1), (4, 0), (4, 17)):
+        rc = L.mf_server_create(0, 0, max_group, workers, 10.0, ctypes.byref(srv))
+        assert rc == -1 and not srv.value, (max_group, workers)
+    assert L.mf_server_create(0, 0, 4, 2, 10.0, None) == -1
+    assert L.mf_group_create(None, 0, 0.0, 30, 10, ctypes.byref(ctypes.c_void_p())) == -1
+    o = mflib.OptionsC(0.0, 0.0, 0.0, 0, 30, 1, 0, 10, 0, 0)
+    p = mflib.Param(3)
+    a = np.zeros(3, np.float32)
+    assert L.mf_align_file(None, b"in.mrc", a, ctypes.byref(o), ctypes.byref(p.c()), None,
+                           None) == -1
+    assert L.mf_align_file(None, None, a, ctypes.byref(o), ctypes.byref(p.c()), None,
+                           None) == -1
+    assert L.mf_device_cos_sin(None, a, 3, a, a) == -1
+    assert L.mf_projalign_measured(None, a) == -1
