@@ -110,6 +110,16 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(values, device, pg=None):
+    """Element-wise maximum of per-rank timings over all ranks (the slowest rank
+    sets the job's time); `pg` is torch.distributed when a process group is up."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if pg is not None:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
 def make_workload(scale: float):
     from markerfree_b200 import synth
     return synth.config(2, scale=scale)
@@ -395,10 +405,7 @@ def run_ours(args):
     barrier()
     pl_ms = _time_steps(stream, step_plain, args.steps)
     log("plain timing done")
-    t = torch.tensor([ms, e_ms, pl_ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if pg is not None:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    ms, e_ms, pl_ms = (float(v) for v in t)
+    ms, e_ms, pl_ms = max_over_ranks([ms, e_ms, pl_ms], f"cuda:{dev}", pg)
     ms_step = ms / args.steps
     value = 60000.0 * B / ms_step * world
     e2e_value = 60000.0 * B / (e_ms / args.steps) * world
