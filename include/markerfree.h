@@ -215,7 +215,7 @@ MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
  * Not in the reference, which aligns one series per process.  A group runs the
  * projection-matching pass (ProjAlign::DoIt, Markerfree/src/method/ProjAlign.cpp:
  * 127-179) of up to 32 series of one context, shape and precision together: each
- * stage of the pass is one launch over all of them, and a pass is one CUDA graph.
+ * stage of the pass is one launch over all of them.
  * Per-series results equal those of aligning each series alone.  Destroy a group
  * before its series. */
 typedef struct mf_group mf_group;
