@@ -196,3 +196,31 @@ def test_fp64_reprojection_agrees_with_fp32_restatement():
     assert np.array_equal(valid, w32 > -1e10)
     err = np.linalg.norm(w32[valid] - w64[valid]) / np.linalg.norm(w64[valid])
     assert err < 1e-6, err
+
+
+def test_first_passes_on_the_stable_series_match_reference():
+    """hi384 (SNR 4), on which the reference's own runs agree: the oracle follows its
+    coarse stage to the printed digits and every per-tilt shift of its first two
+    projection-matching passes to print rounding plus the runs' own spread."""
+    g, s, angles = load("hi384")
+    logs = reference_logs("hi384")
+    nz = len(angles)
+    st = O.preprocess(s.stack, angles)
+    p = O.Param(nz)
+    t = O.Transform(st, angles, p)
+    for i in (1, 2, 3):
+        e = t.doit()
+        ax = O.tilt_axis(st, angles, p, 180.0 / i)
+        assert min(abs(e - events(r, "maxerr")[i - 1][1]) for r in logs) < PRINT_TOL
+        assert min(abs(ax - events(r, "axis")[i - 1][1]) for r in logs) < PRINT_TOL
+    ang = angles + np.float32(0.0001)
+    p.shift_x[:] = 0
+    p.shift_y[:] = 0
+    pa = O.ProjAlign(st, ang, p, 0.0, g["thickness"], g["nproj"])
+    for k in range(2):
+        pa.doit()
+        meas = pa.measured()
+        dev = [pass_deviation(meas, ang, events(r, "meas")[k * (nz - 1):(k + 1) * (nz - 1)])
+               for r in logs]
+        best = int(np.argmin(dev))
+        assert dev[best] < pass_tolerance(logs, best, nz, k), (k, dev)
