@@ -747,6 +747,8 @@ struct oc_projalign {
   std::vector<unsigned char> skip;
   std::vector<float> reproj;
   std::vector<float> meas;  // per tilt: measured shift (un-binned px) of the last pass
+  bool f64 = false;         // re-project with every value accumulated in FP64
+  std::vector<double> reproj64;
 };
 
 static void pa_correct(oc_projalign* pa, int i) {
@@ -796,6 +798,9 @@ void oc_projalign_measured(const oc_projalign* pa, float* xy) {
 int oc_projalign_bin(const oc_projalign* pa) { return pa->bin; }
 void oc_projalign_destroy(oc_projalign* pa) { delete pa; }
 
+// on = 1: later passes re-project in FP64 (reproject_f64) instead of FP32.
+void oc_projalign_set_f64(oc_projalign* pa, int on) { pa->f64 = on != 0; }
+
 // ProjAlign.cpp:133-179 (DoItBin) + 181-241 (ClacAlignProj) + 459-501.
 float oc_projalign_doit(oc_projalign* pa) {
   int nz = pa->nz;
@@ -841,8 +846,15 @@ float oc_projalign_doit(oc_projalign* pa) {
         fprintf(stderr, "oracle: no neighbour in range for tilt %d\n", ip);
         return -1.0f;
       }
-      reproject(pa->corr.data(), pa->xb, pa->yb, nz, pa->angles.data(), ip, rg[0], rg[1],
-                pa->thick, pa->reproj.data());
+      if (pa->f64) {  // FP64 re-projection, rounded once to the FP32 image
+        pa->reproj64.resize(pa->reproj.size());
+        reproject_f64(pa->corr.data(), pa->xb, pa->yb, nz, pa->angles.data(), ip, rg[0], rg[1],
+                      pa->thick, pa->reproj64.data());
+        for (size_t q = 0; q < pa->reproj.size(); ++q) pa->reproj[q] = (float)pa->reproj64[q];
+      } else {
+        reproject(pa->corr.data(), pa->xb, pa->yb, nz, pa->angles.data(), ip, rg[0], rg[1],
+                  pa->thick, pa->reproj.data());
+      }
       float sh[2];
       measure_shift(pa->reproj.data(), pa->corr.data() + ip * bpix, pa->xb, pa->yb, sh);
       float af[2];

@@ -51,6 +51,8 @@ def lib():
         build()
         L = ctypes.CDLL(_LIB_PATH)
         L.oc_frame_idx_from_tilt.argtypes = [ctypes.c_int, _f32p, ctypes.c_float]
+        L.oc_projalign_set_f64.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oc_projalign_set_f64.restype = None
         L.oc_trig_set.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p]
         L.oc_trig_set.restype = None
         L.oc_trig_record.argtypes = [ctypes.c_int]
@@ -285,6 +287,10 @@ class ProjAlign:
 
     def doit(self) -> float:
         return lib().oc_projalign_doit(self._h)
+
+    def set_f64(self, on: bool = True):
+        """Re-project in FP64 in later passes (the reference for precision errors)."""
+        lib().oc_projalign_set_f64(self._h, int(bool(on)))
 
     @property
     def z0(self) -> float:

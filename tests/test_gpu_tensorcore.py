@@ -183,3 +183,34 @@ def test_precision_errors_against_fp64(ctx, mflib, tall, iproj, thick):
     print("relative L2 against FP64:", {k: f"{v:.2e}" for k, v in errs.items()})
     for method, e in errs.items():
         assert e < REL_L2_VS_FP64[method], (method, e)
+
+
+@pytest.mark.parametrize("prec", [0, 2, 1])
+def test_pass_shift_errors_against_fp64_oracle(ctx, mflib, prec):
+    """The per-tilt shift error, in px, of two projection-matching passes in each
+    precision (mf_precision 0 = FP32, 2 = FP16, 1 = BF16 operands) against the oracle whose
+    re-projection accumulates in FP64: within 0.05 px, and stated."""
+    s0 = synth.make_series(nx=160, ny=128, vol_z=40, n_blobs=60, tilt_min=-28, tilt_max=28,
+                           tilt_step=4.0, axis=86.0, shift_sd=3.0, snr=1.0, seed=5,
+                           thickness=30)
+    nz = s0.stack.shape[0]
+    st = O.preprocess(s0.stack, s0.angles)
+    s = mflib.Series(ctx, s0.stack, s0.angles)
+    s.set_precision(prec)
+    p = mflib.Param(nz)
+    p.rotate[:] = 86.0
+    s.set_param(p)
+    po = O.Param(nz)
+    po.rotate[:] = 86.0
+    pa = O.ProjAlign(st, s0.angles, po, 0.0, 30, 10)
+    pa.set_f64(True)
+    s.projalign_setup(0.0, 30, 10)
+    worst = 0.0
+    for _ in range(2):
+        pa.doit()
+        s.projalign_doit()
+        g = s.get_param()
+        worst = max(worst, float(np.abs(g.shift_x - po.shift_x).max()),
+                    float(np.abs(g.shift_y - po.shift_y).max()))
+    print(f"precision {prec}: largest per-tilt shift error against FP64 {worst:.4f} px")
+    assert worst < SHIFT_TOL_MIXED, worst
