@@ -207,8 +207,10 @@ MF_API int mf_device_cos_sin(mf_context* ctx, const float* x, int n, float* c, f
  * work or timing events after the library's. */
 MF_API void* mf_context_stream(mf_context* ctx);
 /* Image rows per tensor-core tile of the FP16/BF16 re-projection (64, 128 or
- * 256; 0 = chosen from the image shape and the SM count).  Read when a pass is
- * set up (mf_projalign_setup) or a single re-projection is queued. */
+ * 256; 0 = automatic: groups time each candidate on their first step and keep
+ * the fastest per shape, single series choose from the image shape and the SM
+ * count).  Read when a pass or a group is set up or a single re-projection is
+ * queued. */
 MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
 
 /* ---- groups: many series in lockstep ---------------------------------------

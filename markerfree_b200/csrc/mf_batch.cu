@@ -225,9 +225,6 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     g->xpitch = (xb + 7) / 8 * 8;
     MF_TRY(g->corr16.alloc((size_t)2 * g->xpitch * yb * nz * B));
     MF_TRY(g->tflags.alloc(sizeof(int) * (size_t)nz * B * g->ytiles * kFlagParts));
-    g->tc_nb = tc_pick_rows(c, xb, yb);
-    MF_TRY(tc_prepare(c, g->tc_nb));
-    MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, g->tc_nb, &g->imgmap));
     MF_TRY(build_reproj_tc_ops(c, geoms, g->prec, &g->tcops, st));
     g->tcjobs.resize((size_t)n * B);
     for (int b = 0; b < B; ++b)
@@ -236,6 +233,20 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
         g->tcjobs[(size_t)k * B + b] =
             TcJob{v.xt, v.colvalid, g->reproj.as<float>() + (size_t)b * g->bpix, b * nz, 0};
       }
+    // tile rows: timed on the first step of this group's shape (the launches
+    // only write the re-projection buffers, which every pass overwrites)
+    MF_TRY(tc_autotune_rows(
+        c, xb, yb, B, g->prec,
+        [&](int nb) -> int {
+          TmaDesc m;
+          MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, nb, &m));
+          return launch_reproject_tc_group(c, g->tcops, g->tcjobs.data(), B, nullptr, xb, yb, m,
+                                           nb, g->d_tcerr.as<int>(), st);
+        },
+        &g->tc_nb, st));
+    MF_TRY(tc_prepare(c, g->tc_nb));
+    MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, g->tc_nb, &g->imgmap));
+    MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
   } else {
     MF_TRY(build_reproj_ops(c, geoms, &g->ops, st));
     std::vector<ApplyJob> jobs((size_t)n * B);

@@ -5,8 +5,10 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <array>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -109,6 +111,8 @@ struct Context {
   int sm_count = 148;
   bool profiling = false;
   int tc_rows = 0;  // tensor-core tile rows (64/128/256); 0 = chosen per shape
+  // tile rows the autotuner chose, per (xb, yb, jobs, precision)
+  std::vector<std::array<int, 5>> tc_tuned;
   double stage[6] = {0, 0, 0, 0, 0, 0};  // see mf_context_stage_times
   double breakdown[kStages] = {};        // ms per stage, see mf_context_stage_breakdown
 };
@@ -284,6 +288,13 @@ int tc_image_map(const void* base, int half_kind, int xb, int xpitch, int yb, in
 // Rows per tensor-core tile (the MMA's N) for an image shape: the context's
 // override if set, else the widest of 256/128/64 that still gives most SMs a tile.
 int tc_pick_rows(const Context* c, int xb, int yb);
+// Autotuner of the tile rows: times `launch(nb)` (one re-projection step with
+// tiles of nb rows, queued on st) for nb = 64, 128, 256, keeps the fastest for
+// the shape (xb, yb, jobs, precision) in the context and returns it in *nb_out.
+// A shape seen before, or tile rows fixed with mf_context_set_tc_rows, is not
+// timed again.
+int tc_autotune_rows(Context* c, int xb, int yb, int jobs, int prec,
+                     const std::function<int(int)>& launch, int* nb_out, cudaStream_t st);
 // Sets the kernel attributes of the tile-rows variant `nb` on the current device
 // (done outside any stream capture).
 int tc_prepare(Context* c, int nb);
