@@ -224,3 +224,78 @@ def test_first_passes_on_the_stable_series_match_reference():
                for r in logs]
         best = int(np.argmin(dev))
         assert dev[best] < pass_tolerance(logs, best, nz, k), (k, dev)
+
+
+# ---------------------------------------------------------------------------
+# Aligned output stack (Process::CorrectStack, Markerfree/src/main/Process.cpp:329-372;
+# CorrStack.cu:142-179): the reference kept a 64 x 64 crop of the middle slice of
+# its aligned stack and the per-slice sums of the whole stack.
+SHIFT_PRINT = 0.0005   # the .txt prints shifts with 3 decimals
+ROT_PRINT = 0.00005    # and the tilt axis with 4
+
+
+def run_input(g):
+    """The stack the reference was given for run g (perturbed for "_p<k>" runs)."""
+    import sys as _sys
+    _sys.path.insert(0, GOLD)
+    from make_reference_golden import perturbed
+    s = synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+    angles = np.array([float(f"{a:.2f}") for a in s.angles], np.float32)
+    seed = g.get("perturbation_seed")
+    return (s.stack if seed is None else perturbed(s.stack, seed)), angles
+
+
+def determined_pixels(params, nx, ny, z, y0, x0, h, w, margin=SHIFT_PRINT + 2e-4):
+    """Pixels of the crop whose nearest source pixel the printed parameters fix:
+    the source coordinate x + 0.5 stays on one side of an integer over the
+    print-rounding interval of the shifts and the axis (CorrStack.cu:160-170)."""
+    th = np.deg2rad(params[z, 1])
+    r = np.hypot(w, h)
+    m = margin + r * np.deg2rad(ROT_PRINT)
+    yy, xx = np.mgrid[y0:y0 + h, x0:x0 + w].astype(np.float64)
+    u, v = xx + 0.5 - nx * 0.5, yy + 0.5 - ny * 0.5
+    X = u * np.cos(th) - v * np.sin(th) + params[z, 2] + nx * 0.5 + 0.5
+    Y = u * np.sin(th) + v * np.cos(th) + params[z, 3] + ny * 0.5 + 0.5
+    return (np.abs(X - np.round(X)) > m) & (np.abs(Y - np.round(Y)) > m)
+
+
+def reference_aligned_runs():
+    out = []
+    for name in ["c1s256", "c1s256b", "cfg1", "hi384"]:
+        for g in reference_logs(name):
+            sfx = "" if g.get("perturbation_seed") is None else f"_p{g['perturbation_seed']}"
+            out.append(f"{name}{sfx}")
+    return out
+
+
+@pytest.mark.parametrize("run", reference_aligned_runs())
+def test_aligned_stack_matches_reference_output(run):
+    """The oracle's output writer, given the parameters the reference wrote, against
+    the reference's own aligned stack: the crop is equal bit for bit on every pixel
+    whose source pixel the printed parameters determine (all but a few per cent),
+    and every slice sum agrees to the rounding those undetermined pixels allow."""
+    with open(os.path.join(GOLD, f"ref_{run}.json")) as f:
+        g = json.load(f)
+    raw, angles = run_input(g)
+    nz, ny, nx = raw.shape
+    st = O.preprocess(raw, angles)
+    params = np.array(g["params"], np.float64)
+    p = O.Param(nz)
+    p.rotate[:] = params[:, 1]
+    p.shift_x[:] = params[:, 2]
+    p.shift_y[:] = params[:, 3]
+    al = O.correct_stack(st, p, 1)
+    crop_ref = np.load(os.path.join(GOLD, f"ref_{run}_crop.npy"))
+    mid, cy, cx = nz // 2, ny // 2, nx // 2
+    crop = al[mid, cy - 32:cy + 32, cx - 32:cx + 32]
+    det = determined_pixels(params, nx, ny, mid, cy - 32, cx - 32, 64, 64)
+    assert det.mean() > 0.95, det.mean()
+    assert np.array_equal(crop[det], crop_ref[det])
+    rel = np.linalg.norm((crop - crop_ref).astype(np.float64)) / np.linalg.norm(crop_ref)
+    assert rel <= 1e-5, rel
+    sums = al.astype(np.float64).sum((1, 2))
+    ref_sums = np.array(g["aligned_slice_sum"])
+    srel = float(np.abs(sums - ref_sums).max() / np.abs(ref_sums).max())
+    print(f"{run}: {det.mean():.4f} of the crop determined; crop rel-L2 {rel:.2e}, "
+          f"largest slice-sum difference {srel:.2e}")
+    assert srel < 2e-4
