@@ -120,89 +120,141 @@ def max_over_ranks(values, device, pg=None):
     return [float(v) for v in t]
 
 
-def make_workload(scale: float):
+SEED0 = 2000  # series j of a step uses seed SEED0 + j
+# Projection-matching passes per series of this workload, the FP32 library path's
+# mean over the seeds SEED0 .. SEED0 + 7 (bench runs report the live count as
+# `passes_per_series`); the CPU restatement's series time is scaled with it.
+PASSES_PER_SERIES = 6.0
+
+
+def make_batch(n: int, device, scale: float = 1.0):
+    """n distinct seeded series of the 2048^2 x 61-tilt workload (torch tensors)."""
     from markerfree_b200 import synth
-    return synth.config(2, scale=scale)
+    return [synth.config_fast(2, seed=SEED0 + j, device=device, scale=scale) for j in range(n)]
 
 
-def workload_config(s, scale):
+def workload_config(s, scale, batch):
     nz, ny, nx = s.stack.shape
     return {"workload": f"{nx}x{ny}x{nz}-tilt series (+-60 deg, 2 deg), T=300, -p 10: "
                         "pre-processing, coarse alignment, projection matching, aligned stack",
             "nx": nx, "ny": ny, "tilts": nz, "thickness": s.thickness, "nproj": 10,
-            "scale": scale, "l2": "inputs (1 GiB raw stack) larger than L2 (126 MB)",
+            "scale": scale, "series_per_step": batch,
+            "series": f"{batch} distinct seeded series per step (seeds {SEED0}..{SEED0 + batch - 1})",
+            "grouping": f"{batch} series per group (lockstep passes)",
+            "l2": "inputs (1 GiB raw stack per series) larger than L2 (126 MB)",
             "parallelism": "independent series per GPU"}
 
 
-# ---------------------------------------------------------------------------
-def cpu_sample(s, passes=14, target_s=8.0):
-    """Reference algorithm on the host cores (oracle), bounded sample, scaled to
-    one series.  Sample: for one held-out tilt at full size, the re-projection of
-    a block of the Yb rows (grown until it takes about `target_s`), one correction
-    (resample + R-weight) and one cross-correlation measurement; per-pass cost =
-    (Z-1) x that tilt cost + Z corrections; a series = `passes` passes (14 in the
-    reference's own example run)."""
+def cpu_sample(s, passes=PASSES_PER_SERIES, rows_target_s=0.8):
+    """The reference algorithm on the host cores (the oracle's FP32 C++ restatement,
+    OpenMP over all threads) on a bounded sample of one series of the workload,
+    and the series time it implies.
+
+    Sample (about 4 s): pre-processing of 4 tilts; one stretch cross-correlation
+    pass (Transform::DoIt) over 3 tilts; a 180-degree and a 20-degree tilt-axis
+    search (CalcTIltAxis) over 3 tilts; the offset search (FindOffset) over 3
+    tilts; and for one held-out tilt of a projection-matching pass the re-
+    projection of a block of rows (grown to about `rows_target_s`), one
+    correction (resample + R-weight) and one cross-correlation measurement.
+    Series time = pre-processing x Z/4 + 3 stretch passes x (Z-1)/2 + 3 180-degree
+    and 4 20-degree searches x Z/3 + the offset search x (Z-1)/2 + `passes` x
+    ((Z-1) x (re-projection of all rows + measurement + correction) + Z
+    corrections): the reference's schedule (Process.cpp:238-319)."""
     from oracle import oracle as O
-    nz, ny, nx = s.stack.shape
+    raw = s.stack.cpu().numpy() if hasattr(s.stack, "cpu") else s.stack
+    nz, ny, nx = raw.shape
     ang = s.angles
-    t0 = time.time()
-    st = O.preprocess(s.stack, ang)
-    t_pre = time.time() - t0
     zt = int(np.argmin(np.abs(ang)))
+    t_all = time.time()
+    t0 = time.time()
+    O.preprocess(np.ascontiguousarray(raw[zt - 2:zt + 2]), ang[zt - 2:zt + 2])
+    t_pre = (time.time() - t0) * nz / 4
+    st = O.preprocess(raw, ang) if not hasattr(s, "_pre") else s._pre
+    s._pre = st
+    sub = np.ascontiguousarray(st[zt - 1:zt + 2])
+    sa = np.ascontiguousarray(ang[zt - 1:zt + 2])
+    p = O.Param(3)
+    t0 = time.time()
+    O.Transform(sub, sa, p).doit()
+    t_tr = (time.time() - t0) * (nz - 1) / 2
+    t0 = time.time()
+    O.tilt_axis(sub, sa, p, 180.0)
+    t_ax180 = (time.time() - t0) * nz / 3
+    p.rotate[:] = float(s.axis)
+    t0 = time.time()
+    O.tilt_axis(sub, sa, p, 20.0)
+    t_ax20 = (time.time() - t0) * nz / 3
+    t0 = time.time()
+    O.find_offset(sub, sa, p)
+    t_off = (time.time() - t0) * (nz - 1) / 2
     ip = zt + 6
     skip = np.ones(nz, np.uint8)
     skip[zt - 5:zt + 6] = 0
     i0, i1 = O.find_proj_range(ang, skip, ip, 10)
     t0 = time.time()
-    corr = np.stack([O.correct_proj(st[i], 0.0, 0.0, 84.7, rweight=True) for i in range(i0, i1 + 1)]
-                    + [O.correct_proj(st[ip], 0.0, 0.0, 84.7, rweight=True)])
-    t_corr = (time.time() - t0) / corr.shape[0]
-    ncpu = os.cpu_count() or 1
-    rows = min(ny, 2 * ncpu)
+    corr = np.stack([O.correct_proj(st[i], 0.0, 0.0, float(s.axis), rweight=True)
+                     for i in (i0, ip)])
+    t_corr = (time.time() - t0) / 2
+    rows = 16
     while True:
-        sub = np.ascontiguousarray(corr[:-1, ny // 2 - rows // 2: ny // 2 - rows // 2 + rows, :])
-        full = np.zeros((nz, rows, sub.shape[2]), np.float32)
-        full[i0:i1 + 1] = sub
+        blk = np.zeros((nz, rows, nx), np.float32)
+        for i in range(i0, i1 + 1):
+            blk[i] = corr[0, ny // 2 - rows // 2: ny // 2 - rows // 2 + rows]
         t0 = time.time()
-        O.reproject(full, ang, ip, i0, i1, s.thickness)
+        O.reproject(blk, ang, ip, i0, i1, s.thickness)
         dt = time.time() - t0
-        if dt > target_s / 4 or rows >= ny:
+        if dt > rows_target_s / 3 or rows >= ny:
             break
-        rows = min(ny, int(rows * max(2.0, target_s / max(dt, 1e-3) * 0.8)))
-    t_rep = dt * (ny / rows)
+        rows = min(ny, int(rows * max(2.0, rows_target_s / max(dt, 1e-3) * 0.8)))
+    t_rep = dt * ny / rows
     t0 = time.time()
-    O.measure_shift(corr[-1], corr[-1])
+    O.measure_shift(corr[1], corr[1])
     t_cc = time.time() - t0
     t_pass = (nz - 1) * (t_rep + t_cc + t_corr) + nz * t_corr
-    series_s = t_pre + passes * t_pass
-    return {"value": 60.0 / series_s, "unit": "series/min", "cores": os.cpu_count(),
-            "kind": "port",
-            "sample": (f"oracle/ (FP32 C++ restatement, OpenMP, all {os.cpu_count()} host threads): "
-                       f"re-projection of {rows}/{ny} rows of one held-out tilt with "
-                       f"{i1 - i0 + 1} neighbours ({t_rep:.1f} s scaled to all rows), one "
-                       f"resample+R-weight ({t_corr:.2f} s), one 2-D cross-correlation "
-                       f"({t_cc:.2f} s), pre-processing ({t_pre:.1f} s); series = {passes} passes x "
-                       f"({nz - 1} held-out tilts + {nz} corrections), coarse stages and "
-                       f"tilt-axis searches not counted"),
-            "seconds_per_series": series_s}
+    series_s = t_pre + 3 * t_tr + 3 * t_ax180 + 4 * t_ax20 + t_off + passes * t_pass
+    sample_s = time.time() - t_all
+    ncpu = os.cpu_count() or 1
+    return {"value": 60.0 / series_s, "unit": "series/min", "cores": ncpu, "kind": "port",
+            "sample": (f"oracle/ FP32 C++ restatement, OpenMP over {ncpu} host threads, one "
+                       f"{nx}x{ny}x{nz} series: pre-processing of 4 tilts, one stretch pass, "
+                       f"a 180- and a 20-degree tilt-axis search and the offset search over 3 "
+                       f"tilts, {rows}/{ny} re-projected rows of one held-out tilt with "
+                       f"{i1 - i0 + 1} neighbours, one correction, one cross-correlation; "
+                       f"scaled to the reference's schedule with {passes:g} projection-matching "
+                       f"passes (mean of the library's FP32 runs on these seeds)"),
+            "seconds_per_series": series_s, "sample_s": sample_s,
+            "stage_s_per_series": {"pre": t_pre, "stretch_passes": 3 * t_tr,
+                                   "axis_searches": 3 * t_ax180 + 4 * t_ax20, "offset": t_off,
+                                   "projection_matching": passes * t_pass}}
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path, timed on the host cores.  The
+    reference program runs every stage on the GPU and has no CPU implementation,
+    so the oracle's FP32 restatement stands in.  A step is one bounded sample of
+    the workload (cpu_sample); `ms_per_step` is its wall time and `value` the
+    series/min that sample implies, so value = series_fraction_per_step x 60000 /
+    ms_per_step."""
     rank, world, local = dist_env()
     if rank != 0:
         return 0
-    s = make_workload(args.scale)
+    s = make_batch(1, "cpu", args.scale)[0]
+    for _ in range(args.warmup):
+        cpu_sample(s)
     t0 = time.time()
     samples = [cpu_sample(s) for _ in range(max(1, args.steps))]
     wall = time.time() - t0
     v = statistics.median(x["value"] for x in samples)
-    cb = dict(samples[0])
+    ms_step = 1000.0 * wall / len(samples)
+    cb = dict(samples[len(samples) // 2])
     cb["value"] = v
     line = {"metric": "series/min (2k^2, 61 tilts)", "value": v, "unit": "series/min",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 60000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom series)",
-            "config": workload_config(s, args.scale), "impl": "reference", "cpu_baseline": cb,
+            "config": workload_config(s, args.scale, args.batch), "impl": "reference",
+            "series_fraction_per_step": v * ms_step / 60000.0,
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "series/min", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "wall_s": wall}
@@ -235,45 +287,58 @@ def _time_steps(stream, fn, steps):
     return sum(a.elapsed_time(b) for a, b in evs)
 
 
-def served_run(mf, s, dev, n_req, seed=5):
-    """The serving loop (continuous batching) on the served-request workload: sizes
-    50% 2048^2, 30% 1024^2, 20% 4096^2; the 1024^2 and 4096^2 series are derived from
-    the 2048^2 one by 2 x 2 binning and 2 x pixel replication, so one phantom serves
-    all sizes.  Requests come from pinned host memory and return their parameters.
+def served_pool(dev):
+    """Distinct seeded series for the serving run, by size class: 2048^2 (the bench
+    workload's generator), 1024^2 and 4096^2 (the same generator at half and double
+    the size; 4096^2 is auto-binned to 2048^2 for matching, as the reference does).
+    Returns {class: [(pinned host tensor, angles, thickness), ...]}."""
+    import torch
+    from markerfree_b200 import synth
+    pool = {}
+    for key, scale, count, seed0 in (("2048", 1.0, 4, 3000), ("1024", 0.5, 3, 3100),
+                                     ("4096", 2.0, 2, 3200)):
+        out = []
+        for j in range(count):
+            s = synth.config_fast(2, seed=seed0 + j, device=f"cuda:{dev}", scale=scale)
+            h = torch.empty(s.stack.shape, dtype=torch.float32).pin_memory()
+            h.copy_(s.stack)
+            out.append((h, s.angles, s.thickness))
+            del s
+        pool[key] = out
+    torch.cuda.empty_cache()
+    return pool
+
+
+def served_run(mf, dev, n_req, precision, seed=5):
+    """The serving loop (continuous batching) on the served-request mix: sizes 50%
+    2048^2, 30% 1024^2, 20% 4096^2, each request one of a pool of distinct seeded
+    series of its size class, from pinned host memory; results are the per-tilt
+    parameters.
 
     Capacity: all n_req requests arrive at once; series/min = n_req / makespan
     (also in 2048^2-equivalents, weighting each request by its pixel count).
     Latency: a Poisson stream of n_req requests at 80% of that capacity; p50/p99
     of arrival-to-result."""
-    import torch
-    nz = s.stack.shape[0]
-    st2 = s.stack
-    st1 = st2.reshape(nz, st2.shape[1] // 2, 2, st2.shape[2] // 2, 2).mean(axis=(2, 4))
-    st4 = np.repeat(np.repeat(st2, 2, axis=1), 2, axis=2)
-    pinned = {}
-    for key, arr, az in (("2048", st2, s.thickness), ("1024", st1, max(8, s.thickness // 2)),
-                         ("4096", st4, s.thickness)):
-        t = torch.from_numpy(np.ascontiguousarray(arr, np.float32)).pin_memory()
-        pinned[key] = (t, arr.shape, az)
-    del st4
+    pool = served_pool(dev)
     weight = {"2048": 1.0, "1024": 0.25, "4096": 4.0}
     rng = np.random.default_rng(seed)
     n4 = max(1, round(0.2 * n_req))
     n1 = max(1, round(0.3 * n_req))
     kinds = ["4096"] * n4 + ["1024"] * n1 + ["2048"] * (n_req - n4 - n1)
     rng.shuffle(kinds)
+    picks = [int(rng.integers(len(pool[k]))) for k in kinds]
 
-    def submit(srv, k):
-        t, shape, az = pinned[k]
-        return srv.submit(None, s.angles, raw_ptr=t.data_ptr(), shape=shape, align_z=az,
-                          nproj=10, precision=PRECISIONS["fp16"])
+    def submit(srv, k, j):
+        t, ang, az = pool[k][j]
+        return srv.submit(None, ang, raw_ptr=t.data_ptr(), shape=tuple(t.shape), align_z=az,
+                          nproj=10, precision=precision)
 
     # capacity: everything queued at once
     srv = mf.Server(gpu=dev, hbm_budget=0, max_group=8, workers=3, group_wait_ms=40.0)
     t0 = time.perf_counter()
-    ids = [submit(srv, k) for k in kinds]
-    for j in ids:
-        srv.wait(j, timeout_s=1800.0)
+    ids = [submit(srv, k, j) for k, j in zip(kinds, picks)]
+    for i in ids:
+        srv.wait(i, timeout_s=1800.0)
     makespan = time.perf_counter() - t0
     st_cap = srv.stats()
     srv.close()
@@ -285,24 +350,34 @@ def served_run(mf, s, dev, n_req, seed=5):
     srv = mf.Server(gpu=dev, hbm_budget=0, max_group=8, workers=3, group_wait_ms=40.0)
     ids = []
     t0 = time.perf_counter()
-    for k, ta in zip(kinds, arrivals):
+    for k, j, ta in zip(kinds, picks, arrivals):
         wait = ta - (time.perf_counter() - t0)
         if wait > 0:
             time.sleep(wait)
-        ids.append(submit(srv, k))
-    lats = [srv.wait(j, timeout_s=1800.0)[2] for j in ids]
+        ids.append(submit(srv, k, j))
+    lats = [srv.wait(i, timeout_s=1800.0)[2] for i in ids]
     st_lat = srv.stats()
     srv.close()
     return {"requests": n_req, "mix": {"2048": kinds.count("2048"), "1024": kinds.count("1024"),
                                        "4096": kinds.count("4096")},
+            "distinct_series": {k: len(v) for k, v in pool.items()},
             "series_per_min": cap_spm, "equiv_2048_series_per_min": cap_eq,
             "capacity_makespan_s": makespan, "capacity_mean_group_size": st_cap["mean_group"],
             "peak_admitted_gb": st_cap["peak_bytes"] / 1e9,
             "latency_arrival_rate_per_min": rate_per_s * 60.0,
             "p50_s": st_lat["p50_s"], "p99_s": st_lat["p99_s"],
             "mean_latency_s": float(np.mean(lats)), "latency_mean_group_size": st_lat["mean_group"],
-            "precision": "fp16 operands, f32 accumulation",
+            "precision": {0: "f32", 1: "bf16 operands, f32 accumulation",
+                          2: "fp16 operands, f32 accumulation"}[precision],
             "returns": "per-tilt parameters (aligned stacks not copied back)"}
+
+
+def _params_diff(pa, pb):
+    """Largest tilt-axis (deg) and shift (px) difference between two Param lists."""
+    ax = max(float(np.abs(a.rotate.astype(np.float64) - b.rotate).max()) for a, b in zip(pa, pb))
+    sh = max(float(max(np.abs(a.shift_x - b.shift_x).max(), np.abs(a.shift_y - b.shift_y).max()))
+             for a, b in zip(pa, pb))
+    return ax, sh
 
 
 def run_ours(args):
@@ -319,19 +394,23 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", dev))
         pg = dist
-    s = make_workload(args.scale)
-    nz, ny, nx = s.stack.shape
+    log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
+    B = args.batch
+    series = make_batch(B, f"cuda:{dev}", args.scale)
+    s0 = series[0]
+    nz, ny, nx = s0.stack.shape
     xo, yo = mf.binned_size(nx, ny, 1)
+    d_raws = [s.stack for s in series]
+    angs = [s.angles for s in series]
     ctx = mf.Context(dev)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
-    B = args.batch
     prec = PRECISIONS[args.precision]
-    kw = dict(offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=s.thickness, out_bin=1, nproj=10,
+    kw = dict(offset=0.0, pitch_angle=0.0, zshift=0.0, align_z=s0.thickness, out_bin=1, nproj=10,
               precision=prec)
-    d_raw = torch.from_numpy(s.stack).to(f"cuda:{dev}")
     d_outs = [torch.empty((nz, yo, xo), dtype=torch.float32, device=f"cuda:{dev}")
               for _ in range(B)]
-    angs = [s.angles] * B
+    torch.cuda.synchronize()
+    log(f"workload ready: {B} distinct {nx}x{ny}x{nz} series")
 
     def barrier():
         if pg is not None:
@@ -341,12 +420,10 @@ def run_ours(args):
     last = {}
 
     def step():
-        ps, passes = mf.align_many_device(ctx, [d_raw] * B, nx, ny, nz, angs, d_outs, **kw)
-        last["passes"] = int(passes[0])
-        last["axis"] = float(ps[0].rotate[0])
+        ps, passes = mf.align_many_device(ctx, d_raws, nx, ny, nz, angs, d_outs, **kw)
+        last["params"] = ps
+        last["passes"] = float(np.mean(passes))
 
-    log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
-    log(f"workload ready {nx}x{ny}x{nz}, batch {B}")
     for _ in range(args.warmup):
         step()
     barrier()
@@ -358,8 +435,7 @@ def run_ours(args):
         barrier()
         torch.cuda.nvtx.range_pop()
         launches = ctx.kernel_launches() - l0
-        # one more step with per-stage CUDA events on the library's stream (passes then
-        # launch kernels one by one instead of replaying the graph; same kernels)
+        # one more step with per-stage CUDA events on the library's stream
         ctx.set_profiling(True)
         ctx.stage_times()
         ctx.stage_breakdown()
@@ -367,68 +443,108 @@ def run_ours(args):
         st = ctx.stage_times()
         stages = ctx.stage_breakdown()
         ctx.set_profiling(False)
+    params_main = last["params"]
+    passes_main = last["passes"]
+    log("batched timing done")
     # e2e through the C ABI with host buffers: per step B uploads from pinned memory,
     # the group alignment, B downloads of the aligned stacks
-    h_raw = torch.from_numpy(s.stack).pin_memory()
+    h_raws = []
+    for d in d_raws:
+        h = torch.empty(d.shape, dtype=torch.float32).pin_memory()
+        h.copy_(d)
+        h_raws.append(h)
     h_out = torch.empty((nz, yo, xo), dtype=torch.float32).pin_memory()
-    d_ins = [torch.empty_like(d_raw) for _ in range(B)]
+    d_ins = [torch.empty_like(d_raws[0]) for _ in range(B)]
 
     def step_e2e():
         with torch.cuda.stream(stream):
-            for d in d_ins:
-                d.copy_(h_raw, non_blocking=True)
+            for d, h in zip(d_ins, h_raws):
+                d.copy_(h, non_blocking=True)
         mf.align_many_device(ctx, d_ins, nx, ny, nz, angs, d_outs, **kw)
         with torch.cuda.stream(stream):
             for d in d_outs:
                 h_out.copy_(d, non_blocking=True)
 
-    log("batched timing done")
     step_e2e()
     barrier()
     e_ms = _time_steps(stream, step_e2e, args.steps)
     log("e2e timing done")
-    h2d_bytes = int(s.stack.nbytes) * B
+    h2d_bytes = int(sum(h.numel() for h in h_raws) * 4)
     d2h_bytes = int(h_out.numel() * 4 + 3 * nz * 4) * B
     # the pinned buffers recorded their copies on the library's stream: release them
     # while that stream exists
-    del d_ins, h_raw, h_out, step_e2e
+    del d_ins, h_raws, h_out, step_e2e
     torch.cuda.synchronize()
-    # the plain path: one series at a time, FP32 (the reference's arithmetic)
+    k_extra = max(1, min(args.steps, 3))
+    # the 16-bit operand forms of the same step, with their distance from the FP32 result
+    mixed = {}
+    for name in ("fp16", "bf16"):
+        if args.no_mixed or PRECISIONS[name] == prec:
+            continue
+        kwm = dict(kw, precision=PRECISIONS[name])
+
+        def step_m():
+            ps, passes = mf.align_many_device(ctx, d_raws, nx, ny, nz, angs, d_outs, **kwm)
+            last["m_params"], last["m_passes"] = ps, float(np.mean(passes))
+
+        step_m()
+        barrier()
+        if name == "fp16":
+            ctx.set_profiling(True)
+            ctx.stage_times()
+            ctx.stage_breakdown()
+            pm_ms = _time_steps(stream, step_m, 1)
+            st_m = ctx.stage_times()
+            ctx.stage_breakdown()
+            ctx.set_profiling(False)
+        m_ms = _time_steps(stream, step_m, k_extra)
+        dax, dsh = _params_diff(last["m_params"], params_main)
+        mixed[name] = {"value": 60000.0 * B / (m_ms / k_extra) * world, "unit": "series/min",
+                       "steps": k_extra, "passes_per_series": last["m_passes"],
+                       "max_axis_diff_vs_f32_deg": dax, "max_shift_diff_vs_f32_px": dsh}
+        if name == "fp16":
+            mixed[name]["reproject_stage_times"] = st_m
+            mixed[name]["profiled_ms_per_step"] = pm_ms
+    log("mixed-precision timing done")
+    # the plain path: one series at a time (mf_align_device), FP32, the same series
     kw32 = dict(kw, precision=PRECISIONS["fp32"])
-    d_one = d_outs[0]
 
     def step_plain():
-        mf.align_device(ctx, d_raw, nx, ny, nz, s.angles, d_one, **kw32)
+        for d, a, o in zip(d_raws, angs, d_outs):
+            mf.align_device(ctx, d, nx, ny, nz, a, o, **kw32)
 
-    for _ in range(2):
-        step_plain()
+    step_plain()
     barrier()
-    pl_ms = _time_steps(stream, step_plain, args.steps)
+    pl_ms = _time_steps(stream, step_plain, k_extra)
     log("plain timing done")
     ms, e_ms, pl_ms = max_over_ranks([ms, e_ms, pl_ms], f"cuda:{dev}", pg)
     ms_step = ms / args.steps
     value = 60000.0 * B / ms_step * world
     e2e_value = 60000.0 * B / (e_ms / args.steps) * world
-    plain_value = 60000.0 / (pl_ms / args.steps) * world
+    plain_value = 60000.0 * B / (pl_ms / k_extra) * world
     pk, src = peaks()
-    # dominant kernel: the re-projection, one launch per step of a pass for the group
-    launches_rep = max(st["reproj_launches"], 1)
-    t_launch = st["reproj_ms"] / launches_rep / 1e3
-    bytes_launch = st["reproj_bytes"] / launches_rep
-    achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
-    tensor_tflops = 2.0 * st["reproj_fma"] / launches_rep / t_launch / 1e12 if t_launch else 0.0
-    kname = ("k_op_apply (FP32 banded operator)" if prec == 0 else
-             "k_reproject_tc (tcgen05, 16-bit operands, FP32 accumulation in TMEM)")
-    roof_rep = {"kernel": kname + f", one launch per held-out tilt step for a group of {B}",
+
+    def reproj_roof(stt, kname, prof_ms, traffic_file):
+        launches_rep = max(stt["reproj_launches"], 1)
+        t_launch = stt["reproj_ms"] / launches_rep / 1e3
+        bytes_launch = stt["reproj_bytes"] / launches_rep
+        achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
+        flops = 2.0 * stt["reproj_fma"] / launches_rep / t_launch / 1e12 if t_launch else 0.0
+        return {"kernel": kname + f", one launch per held-out tilt step for a group of {B}",
                 "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"], "peak_source": src,
-                "traffic": profiled_traffic("traffic_reproject.json"),
+                "traffic": profiled_traffic(traffic_file),
                 "avg_launch_ms": t_launch * 1e3, "bytes_per_launch": bytes_launch,
-                "tensor_tflops": tensor_tflops,
-                "tensor_frac_of_bf16_peak": tensor_tflops / (pk.get("bf16_tflops", 1590.0)),
-                "share_of_step": st["reproj_ms"] / max(p_ms, 1e-9),
-                "rest_of_pass_share_of_step": st["xcorr_ms"] / max(p_ms, 1e-9),
-                "profiled_ms_per_step": p_ms}
+                "tflops": flops, "share_of_step": stt["reproj_ms"] / max(prof_ms, 1e-9),
+                "rest_of_pass_share_of_step": stt["xcorr_ms"] / max(prof_ms, 1e-9),
+                "profiled_ms_per_step": prof_ms}
+
+    roof_rep = reproj_roof(st, "k_op_apply (FP32 banded operator, SIMT FMA)" if prec == 0 else
+                           "k_reproject_tc (tcgen05, 16-bit operands, FP32 accumulation in TMEM)",
+                           p_ms, "traffic_op_apply.json" if prec == 0 else
+                           "traffic_reproject.json")
+    roof_rep["note"] = ("FP32 FMA-bound on the banded operator; the HBM fraction counts "
+                        "compulsory bytes (neighbour rows, operator, output)") if prec == 0 else ""
     # the tilt-axis Radon kernel, timed on its own in the profiled step: compulsory
     # bytes (each tilt image once, the lines once) over its time, and its gather rate
     n_rad = max(stages["radon_launches"], 1.0)
@@ -447,13 +563,18 @@ def run_ours(args):
                 "profiled_ms_per_step": p_ms,
                 "note": "gather-bound: the tilt images are L2-resident while a launch "
                         "samples them; the HBM fraction counts compulsory bytes only"}
-    # the dominant kernel of the step carries the roofline; the other is kept beside it
+    # the dominant kernel of the step carries the roofline; the others are kept beside it
     if roof_rad["share_of_step"] >= roof_rep["share_of_step"]:
-        roof, roof_other = roof_rad, roof_rep
+        roof, others = roof_rad, [roof_rep]
     else:
-        roof, roof_other = roof_rep, roof_rad
-    cfg = workload_config(s, args.scale)
-    cfg.update({"series_per_step": B, "grouping": f"{B} series per group (lockstep passes)"})
+        roof, others = roof_rep, [roof_rad]
+    if "fp16" in mixed:
+        others.append(reproj_roof(mixed["fp16"].pop("reproject_stage_times"),
+                                  "k_reproject_tc (tcgen05, FP16 operands, FP32 accumulation in "
+                                  "TMEM; fp16 form of the step)",
+                                  mixed["fp16"].pop("profiled_ms_per_step"),
+                                  "traffic_reproject.json"))
+    cfg = workload_config(s0, args.scale, B)
     line = {"metric": "series/min (2k^2, 61 tilts)", "value": value, "unit": "series/min",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -462,22 +583,28 @@ def run_ours(args):
             "config": cfg,
             "e2e": {"value": e2e_value, "unit": "series/min",
                     "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
-            "plain": {"value": plain_value, "unit": "series/min",
-                      "what": "one series at a time, FP32 operands (mf_align_device)"},
+            "plain": {"value": plain_value, "unit": "series/min", "steps": k_extra,
+                      "what": "the same series one at a time, FP32 (mf_align_device)"},
             "batched_over_plain": value / plain_value,
-            "gpu_launches": int(launches), "passes_per_series": last.get("passes"),
+            "mixed_precision": mixed,
+            "gpu_launches": int(launches), "passes_per_series": passes_main,
+            "tc_tuning": ctx.tc_tuning(),
             "stage_ms_per_step": {k: round(v, 2) for k, v in stages.items()},
-            "roofline": roof, "roofline_other": roof_other, "clocks": clk.summary()}
+            "roofline": roof, "roofline_other": others, "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_serve:
         log("serving run")
-        line["served"] = served_run(mf, s, dev, args.serve_requests)
+        del d_outs
+        torch.cuda.empty_cache()
+        line["served"] = served_run(mf, dev, args.serve_requests, PRECISIONS["fp16"])
         log("serving run done")
         line["served_over_plain"] = line["served"]["equiv_2048_series_per_min"] / plain_value
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(s, passes=max(last.get("passes", 1), 1))
+        cpu = make_batch(1, "cpu", args.scale)[0]
+        cpu_sample(cpu)  # pre-processes the series once
+        line["cpu_baseline"] = cpu_sample(cpu)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del d_outs, d_one, d_raw
+    del d_raws, series
     torch.cuda.synchronize()
     ctx.close()
     if pg is not None:
@@ -493,7 +620,8 @@ def run_kernel_case(args):
     tilt-axis search (100 candidates over 20 degrees)."""
     import torch
     import markerfree_b200 as mf
-    s = make_workload(args.scale)
+    s = make_batch(1, "cuda:0", args.scale)[0]
+    s.stack = s.stack.cpu().numpy()
     nz, ny, nx = s.stack.shape
     ctx = mf.Context(0)
     ang = s.angles
@@ -536,12 +664,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests only)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--precision", default="fp16", choices=list(PRECISIONS),
-                    help="re-projection operands of the batched path (fp32 = the reference's "
-                         "arithmetic; the plain line is always fp32)")
+    ap.add_argument("--precision", default="fp32", choices=list(PRECISIONS),
+                    help="re-projection operands of the headline batched path (fp32 = the "
+                         "reference's arithmetic; the plain line is always fp32)")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the fp16/bf16 forms of the batched step")
     ap.add_argument("--batch", type=int, default=8, help="series per group (one step)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
-    ap.add_argument("--serve-requests", type=int, default=20)
+    ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--kernel-method", type=int, default=1,
                     help="re-projection method of --kernel-case reproject (1 FP32, 2 FP16, 3 BF16)")
     args = ap.parse_args()

@@ -128,3 +128,89 @@ def config(cfg: int, scale: float = 1.0, seed: int | None = None) -> Series:
                            tilt_step=2.0, axis=84.7, shift_sd=12.0, snr=0.05, seed=s,
                            thickness=max(8, int(300 * scale)) // 2 * 2, nproj=20, name="cfg3")
     raise ValueError(f"unknown configuration {cfg}")
+
+
+def make_series_fast(nx=512, ny=512, vol_z=128, n_blobs=200, sigma=(2.0, 6.0), amp=(0.5, 1.5),
+                     tilt_min=-60.0, tilt_max=60.0, tilt_step=3.0, axis=86.3, shift_sd=4.0,
+                     drift=0.0, snr=0.1, poisson=False, background=False, seed=1001,
+                     thickness=100, nproj=10, name="synthetic", n_tilts=None, device="cpu"):
+    """make_series' distribution, generated with torch on `device` in seconds.
+
+    The phantom, the tilt geometry and the shifts are drawn exactly as make_series
+    draws them (same numpy generator and order).  Each tilt image is the sum of
+    the blobs' separable Gaussians, evaluated over the whole image as one matrix
+    product (make_series truncates each blob at 4 sigma and adds blob by blob),
+    in float32; the noise comes from a torch generator seeded with `seed` on
+    `device`, so images are reproducible per device kind but not equal to
+    make_series' bit for bit.  Returns a Series whose `stack` is a float32 torch
+    tensor on `device`."""
+    import torch
+    rng = np.random.default_rng(seed)
+    if n_tilts is None:
+        n_tilts = int(round((tilt_max - tilt_min) / tilt_step)) + 1
+    angles = np.linspace(tilt_min, tilt_max, n_tilts).astype(np.float32)
+    cx = rng.uniform(-nx / 2, nx / 2, n_blobs)
+    cy = rng.uniform(-ny / 2, ny / 2, n_blobs)
+    cz = rng.uniform(-vol_z / 2, vol_z / 2, n_blobs)
+    sg = rng.uniform(sigma[0], sigma[1], n_blobs)
+    am = rng.uniform(amp[0], amp[1], n_blobs)
+    if background:
+        nb = 12
+        bx = rng.uniform(-nx / 2, nx / 2, nb)
+        by = rng.uniform(-ny / 2, ny / 2, nb)
+        bz = rng.uniform(-vol_z / 4, vol_z / 4, nb)
+        bs = rng.uniform(nx / 6, nx / 3, nb)
+        ba = rng.uniform(0.002, 0.006, nb)
+        cx, cy, cz = np.r_[cx, bx], np.r_[cy, by], np.r_[cz, bz]
+        sg, am = np.r_[sg, bs], np.r_[am, ba]
+    zt = int(np.argmin(np.abs(angles)))
+    shifts = rng.normal(0.0, shift_sd, (n_tilts, 2))
+    shifts[:, 0] += drift * (np.arange(n_tilts) - zt)
+    shifts[zt] = 0.0
+    ca, sa = math.cos(math.radians(axis)), math.sin(math.radians(axis))
+    dev = torch.device(device)
+    f32 = dict(dtype=torch.float32, device=dev)
+    px = torch.arange(nx, **f32)
+    py = torch.arange(ny, **f32)
+    inv2s2 = torch.tensor(1.0 / (2.0 * sg * sg), **f32)
+    coef = torch.tensor(am * sg * math.sqrt(2 * math.pi), **f32)
+    stack = torch.empty((n_tilts, ny, nx), **f32)
+    for k, t in enumerate(angles.astype(np.float64)):
+        tr = math.radians(t)
+        u = cx * math.cos(tr) + cz * math.sin(tr)
+        v = cy
+        rx = torch.tensor(ca * u - sa * v + nx / 2 + shifts[k, 0], **f32)
+        ry = torch.tensor(sa * u + ca * v + ny / 2 + shifts[k, 1], **f32)
+        gx = torch.exp(-(px[None, :] - rx[:, None]) ** 2 * inv2s2[:, None])   # (nb, nx)
+        gy = torch.exp(-(py[None, :] - ry[:, None]) ** 2 * inv2s2[:, None])   # (nb, ny)
+        torch.matmul(gy.t() * coef[None, :], gx, out=stack[k])
+    if snr and snr > 0:
+        gen = torch.Generator(device=dev).manual_seed(int(seed))
+        sig_sd = float(stack.double().std())
+        noise_sd = sig_sd / math.sqrt(snr)
+        if poisson:
+            mean = float(stack.double().mean())
+            lam = (stack / max(mean, 1e-12) * 20.0).clamp_(min=0.0)
+            shot = torch.poisson(lam, generator=gen)
+            del lam
+            shot.mul_(mean / 20.0)
+            shot.add_(torch.randn(shot.shape, generator=gen, **f32), alpha=noise_sd * math.sqrt(0.5))
+            stack = shot
+        else:
+            stack.add_(torch.randn(stack.shape, generator=gen, **f32), alpha=noise_sd)
+    return Series(stack=stack, angles=angles, shifts=shifts.astype(np.float32), axis=float(axis),
+                  thickness=int(thickness), nproj=int(nproj), name=name)
+
+
+def config_fast(cfg: int, seed: int | None = None, device="cpu", scale: float = 1.0) -> Series:
+    """config()'s series drawn with make_series_fast (same parameters)."""
+    s = seed if seed is not None else 1000 + cfg
+    if cfg == 2:
+        n = int(2048 * scale) // 2 * 2
+        return make_series_fast(nx=n, ny=n, vol_z=max(8, int(300 * scale)),
+                                n_blobs=max(30, int(3000 * scale * scale)), sigma=(1.5, 5.0),
+                                tilt_step=2.0, axis=84.7, shift_sd=8.0, drift=0.3, snr=0.05,
+                                poisson=True, background=True, seed=s,
+                                thickness=max(8, int(300 * scale)) // 2 * 2, name="cfg2",
+                                device=device)
+    raise ValueError(f"no fast form of configuration {cfg}")
