@@ -212,6 +212,11 @@ MF_API void* mf_context_stream(mf_context* ctx);
  * count).  Read when a pass or a group is set up or a single re-projection is
  * queued. */
 MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows);
+/* The tile-row choices the autotuner made in this context: up to max_rows rows
+ * of 8 doubles each, {xb, yb, series per launch, precision, chosen rows, median
+ * ms per launch with 256, 128 and 64 rows}; *n receives the number of rows
+ * recorded (which may exceed max_rows). */
+MF_API int mf_context_tc_tuning(mf_context* ctx, double* out, int max_rows, int* n);
 
 /* ---- groups: many series in lockstep ---------------------------------------
  * Not in the reference, which aligns one series per process.  A group runs the

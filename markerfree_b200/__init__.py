@@ -104,6 +104,8 @@ SIGNATURES = [
     ("mf_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("mf_device_cos_sin", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int, _f32p, _f32p]),
     ("mf_context_set_tc_rows", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("mf_context_tc_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.c_int, _c_int_p]),
     ("mf_group_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                        ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_void_p)]),
@@ -249,6 +251,19 @@ class Context:
     def set_tc_rows(self, rows: int):
         """Image rows per tensor-core tile (64, 128, 256; 0 = automatic)."""
         _check(lib().mf_context_set_tc_rows(self.h, int(rows)))
+
+    def tc_tuning(self) -> list:
+        """The autotuner's choices: one dict per (shape, series per launch, precision)."""
+        n = ctypes.c_int()
+        buf = (ctypes.c_double * (8 * 64))()
+        _check(lib().mf_context_tc_tuning(self.h, buf, 64, ctypes.byref(n)))
+        rows = []
+        for i in range(min(n.value, 64)):
+            r = buf[8 * i:8 * i + 8]
+            rows.append({"xb": int(r[0]), "yb": int(r[1]), "series": int(r[2]),
+                         "precision": int(r[3]), "rows": int(r[4]),
+                         "ms_per_launch": {"256": r[5], "128": r[6], "64": r[7]}})
+        return rows
 
     def stream_ptr(self) -> int:
         return int(lib().mf_context_stream(self.h) or 0)

@@ -191,38 +191,81 @@ __device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsi
 // samples never fires and every sample counts.
 // An in-range coordinate (0 <= X < 2^23) is truncated by a round-toward-zero add
 // of 2^23: the low bits of the sum are (int)X, and the index is formed from the
-// biased bits in 32-bit modular arithmetic, the bias removed once.
-template <bool kByColumn, bool kNonNeg>
+// biased bits in 32-bit modular arithmetic.  kFold (stride a multiple of 256):
+// 2^23's bits times the stride vanish mod 2^32, so the biased index is the true
+// index plus 0x4B000000 without wrapping, and that constant moves into the base
+// address instead of being subtracted per sample.
+// Two consecutive samples are stepped together: each packed f32x2 operation
+// evaluates one coordinate of samples x and x + 1 (lane for lane the scalar IEEE
+// operation), and the samples are added to the sum in order, x first.
+template <bool kByColumn, bool kNonNeg, bool kFold>
 __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, int stride,
                                               const RadonLine& ln, int lo, int hi, float* sum_out,
                                               int* cnt_out) {
   constexpr unsigned kBias = 0x4B000000u;  // bits of 2^23
-  const unsigned bias_idx = kBias * (unsigned)stride + kBias;  // mod 2^32
-  const unsigned long long cs2 = pack2(ln.c, ln.s), y2 = pack2(ln.ys, ln.yc);
-  const unsigned long long o2 = pack2(ln.ox, ln.oy), big2 = pack2(8388608.0f, 8388608.0f);
-  const unsigned long long one2 = pack2(1.0f, 1.0f);
-  unsigned long long fx2 = pack2((float)lo, (float)lo);
+  const unsigned bias_idx = kFold ? 0u : kBias * (unsigned)stride + kBias;  // mod 2^32
+  const uintptr_t base = (uintptr_t)proj - (kFold ? 4ull * kBias : 0ull);
+  const unsigned long long c2 = pack2(ln.c, ln.c), s2 = pack2(ln.s, ln.s);
+  const unsigned long long ys2 = pack2(ln.ys, ln.ys), yc2 = pack2(ln.yc, ln.yc);
+  const unsigned long long ox2 = pack2(ln.ox, ln.ox), oy2 = pack2(ln.oy, ln.oy);
+  const unsigned long long big2 = pack2(8388608.0f, 8388608.0f), two2 = pack2(2.0f, 2.0f);
+  auto index = [&](float tx, float ty) -> unsigned {
+    const unsigned bx = __float_as_uint(tx), by = __float_as_uint(ty);
+    return (kByColumn ? bx * (unsigned)stride + by : by * (unsigned)stride + bx) - bias_idx;
+  };
+  auto load = [&](unsigned idx) -> float {
+    return __ldg(reinterpret_cast<const float*>(base + ((uintptr_t)idx << 2)));
+  };
+  unsigned long long fx2 = pack2((float)lo, (float)(lo + 1));
   float sum = 0.0f;
   int cnt = 0;
-#pragma unroll 4
-  for (int x = lo; x < hi; ++x) {
-    // X = fma(x, cos, -(y sin)) + ox, Y = fma(x, sin, y cos) + oy, as lin2()
-    const unsigned long long t = add2_rz(add2_rn(fma2_rn(fx2, cs2, y2), o2), big2);
-    fx2 = add2_rn(fx2, one2);
-    float tx, ty;
-    unpack2(t, &tx, &ty);
-    const unsigned bx = __float_as_uint(tx), by = __float_as_uint(ty);
-    const unsigned idx = (kByColumn ? bx * (unsigned)stride + by : by * (unsigned)stride + bx) -
-                         bias_idx;
-    const float v = __ldg(proj + idx);
-    if (!kNonNeg) {
-      if (v < 0) continue;
-      cnt++;
+  int x = lo;
+#pragma unroll 2
+  for (; x + 1 < hi; x += 2) {
+    // X = fma(x, cos, -(y sin)) + ox, Y = fma(x, sin, y cos) + oy, as lin2(), for x, x + 1
+    const unsigned long long tx = add2_rz(add2_rn(fma2_rn(fx2, c2, ys2), ox2), big2);
+    const unsigned long long ty = add2_rz(add2_rn(fma2_rn(fx2, s2, yc2), oy2), big2);
+    fx2 = add2_rn(fx2, two2);
+    float x0, x1, y0, y1;
+    unpack2(tx, &x0, &x1);
+    unpack2(ty, &y0, &y1);
+    const float v0 = load(index(x0, y0));
+    const float v1 = load(index(x1, y1));
+    if (kNonNeg) {
+      sum = __fadd_rn(sum, v0);
+      sum = __fadd_rn(sum, v1);
+    } else {
+      if (!(v0 < 0)) {
+        cnt++;
+        sum = __fadd_rn(sum, v0);
+      }
+      if (!(v1 < 0)) {
+        cnt++;
+        sum = __fadd_rn(sum, v1);
+      }
     }
-    sum = __fadd_rn(sum, v);
+  }
+  if (x < hi) {
+    const float fx = (float)x;
+    const float tx = __fadd_rz(ln.X(fx), 8388608.0f), ty = __fadd_rz(ln.Y(fx), 8388608.0f);
+    const float v = load(index(tx, ty));
+    if (kNonNeg || !(v < 0)) {
+      cnt++;
+      sum = __fadd_rn(sum, v);
+    }
   }
   *sum_out = sum;
   *cnt_out = kNonNeg ? max(hi - lo, 0) : cnt;
+}
+
+template <bool kByColumn, bool kNonNeg>
+__device__ __forceinline__ void radon_line(const float* __restrict__ proj, int stride,
+                                           const RadonLine& ln, int lo, int hi, float* sum,
+                                           int* cnt) {
+  if ((stride & 255) == 0)
+    radon_samples<kByColumn, kNonNeg, true>(proj, stride, ln, lo, hi, sum, cnt);
+  else
+    radon_samples<kByColumn, kNonNeg, false>(proj, stride, ln, lo, hi, sum, cnt);
 }
 
 // GRadon (Rotate.cu:42-95) for every tilt z = blockIdx.z.  The samples that fall
@@ -268,14 +311,14 @@ __global__ void k_radon(const float* __restrict__ stack, const float* __restrict
   const bool nonneg = neg != nullptr && neg[z] == 0;
   if (stack_t != nullptr && fabsf(ln.c) > fabsf(ln.s)) {  // uniform over the block
     if (nonneg)
-      radon_samples<true, true>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
+      radon_line<true, true>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
     else
-      radon_samples<true, false>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
+      radon_line<true, false>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
   } else {
     if (nonneg)
-      radon_samples<false, true>(stack + off, width, ln, lo, hi, &sum, &cnt);
+      radon_line<false, true>(stack + off, width, ln, lo, hi, &sum, &cnt);
     else
-      radon_samples<false, false>(stack + off, width, ln, lo, hi, &sum, &cnt);
+      radon_line<false, false>(stack + off, width, ln, lo, hi, &sum, &cnt);
   }
   lines[((size_t)z * num + b) * (L + 2) + y] = (cnt == 0) ? kSentinel : __fdiv_rn(sum, (float)cnt);
   if (samples) {  // stage timing: samples taken (one atomic per warp)
@@ -425,86 +468,99 @@ __global__ void k_axis_score(const float* __restrict__ cc, int nz, int num,
   score[b] = __fdiv_rn(s, (float)nz);
 }
 
-struct AxisBuffers {
-  DevBuf rot, cs, tcos, sx, sy, region, lines, sum, cc, score;
-};
+AxisJob::~AxisJob() {
+  if (ev[0]) cudaEventDestroy(ev[0]);
+  if (ev[1]) cudaEventDestroy(ev[1]);
+}
 
-int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, const float* stack_t,
-                     const int* d_neg, int nx, int ny, int nz, const float* angles,
-                     const float* sx, const float* sy, int zt, const float* rot_cand, int num,
-                     int L, std::vector<float>* scores, cudaStream_t st) {
+int tilt_axis_scores_enqueue(Context* c, cufftHandle plan, const float* stack,
+                             const float* stack_t, const int* d_neg, int nx, int ny, int nz,
+                             const float* angles, const float* sx, const float* sy, int zt,
+                             const float* rot_cand, int num, int L, int slot, AxisJob* J,
+                             cudaStream_t st) {
   const int cmp = L / 2 + 1;
-  AxisBuffers B;
-  std::vector<float> tc(nz);
-  for (int z = 0; z < nz; ++z) tc[z] = (float)std::cos(angles[z] * kD2R);
-  MF_TRY(B.cs.alloc(sizeof(float2) * num));
-  MF_TRY(B.tcos.alloc(sizeof(float) * nz));
-  MF_TRY(B.sx.alloc(sizeof(float) * nz));
-  MF_TRY(B.sy.alloc(sizeof(float) * nz));
-  MF_TRY(B.region.alloc(sizeof(int) * 2 * (size_t)num * L));
-  MF_TRY(B.lines.alloc(sizeof(float) * (size_t)nz * num * (L + 2)));
-  MF_TRY(B.sum.alloc(sizeof(cufftComplex) * (size_t)num * cmp));
-  MF_TRY(B.cc.alloc(sizeof(float) * (size_t)num * nz));
-  MF_TRY(B.score.alloc(sizeof(float) * num));
-  MF_TRY(B.rot.alloc(sizeof(float) * num));
-  MF_CHECK_CUDA(cudaMemcpyAsync(B.rot.p, rot_cand, sizeof(float) * num, cudaMemcpyHostToDevice, st));
-  k_axis_cs<<<(num + 127) / 128, 128, 0, st>>>(B.rot.as<float>(), num, B.cs.as<float2>());
-  c->launches++;
-  MF_CHECK_CUDA(cudaMemcpyAsync(B.tcos.p, tc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(B.sx.p, sx, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(B.sy.p, sy, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
-  k_common_region<<<dim3(num, (L + 127) / 128), dim3(1, 128), 0, st>>>(
-      nx, ny, L, B.cs.as<float2>(), sx[zt], sy[zt], B.region.as<int>());
-  // with stage timing on, the Radon kernel is timed on its own and counts its samples
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  DevBuf count;
-  if (c->profiling) {
-    MF_TRY(count.alloc(sizeof(unsigned long long)));
-    MF_CHECK_CUDA(cudaMemsetAsync(count.p, 0, sizeof(unsigned long long), st));
-    MF_CHECK_CUDA(cudaEventCreate(&ev[0]));
-    MF_CHECK_CUDA(cudaEventCreate(&ev[1]));
-    MF_CHECK_CUDA(cudaEventRecord(ev[0], st));
-  }
-  k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
-      stack, stack_t, d_neg, nx, ny, L, num, B.cs.as<float2>(), B.tcos.as<float>(),
-      B.sx.as<float>(), B.sy.as<float>(), B.region.as<int>(), B.lines.as<float>(),
-      count.as<unsigned long long>());
-  if (c->profiling) {
-    MF_CHECK_CUDA(cudaEventRecord(ev[1], st));
-    unsigned long long n = 0;
-    MF_CHECK_CUDA(cudaMemcpyAsync(&n, count.p, sizeof(n), cudaMemcpyDeviceToHost, st));
-    MF_CHECK_CUDA(cudaStreamSynchronize(st));
-    float ms = 0.0f;
-    MF_CHECK_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    c->breakdown[kStageRadonMs] += ms;
-    c->breakdown[kStageRadonSamples] += (double)n;
-    c->breakdown[kStageRadonLaunches] += 1.0;
-    // compulsory bytes: every tilt image once, the line values written once
-    c->breakdown[kStageRadonBytes] +=
-        4.0 * (double)nx * ny * nz + 4.0 * (double)nz * num * (L + 2);
-  }
-  k_line_prep<<<nz * num, 512, 0, st>>>(B.lines.as<float>(), L);
-  c->launches += 3;
-  MF_CHECK_CUDA(cudaGetLastError());
-  MF_CHECK_CUFFT(cufftExecR2C(plan, B.lines.as<cufftReal>(), B.lines.as<cufftComplex>()));
-  const cufftComplex* spec = B.lines.as<cufftComplex>();
-  k_axis_sum<<<dim3((cmp + 127) / 128, num), 128, 0, st>>>(spec, nz, num, cmp,
-                                                            B.sum.as<cufftComplex>());
   const int bs = calc_warps(cmp, 32) * 32;
   const int nblk = cmp / bs + 1;
   if (nblk > 64) return set_error(MF_ERR_ARG, "tilt axis: line of %d bins too long", L);
   const int gs = calc_warps(nblk, 32) * 32;
-  k_axis_cc<<<dim3(num, nz), bs, 0, st>>>(spec, B.sum.as<cufftComplex>(), nz, num, cmp, gs,
-                                          B.cc.as<float>());
-  k_axis_score<<<(num + 127) / 128, 128, 0, st>>>(B.cc.as<float>(), nz, num, B.score.as<float>());
+  J->num = num;
+  J->L = L;
+  J->nx = nx;
+  J->ny = ny;
+  J->nz = nz;
+  char* host = (char*)c->pinned.get(slot, sizeof(float) * num + sizeof(unsigned long long));
+  if (!host) return MF_ERR_NOMEM;
+  J->h_count = (unsigned long long*)host;
+  J->h_scores = (float*)(host + sizeof(unsigned long long));
+  // device buffers are released stream-ordered when this function returns, after
+  // the work queued here; only the page-locked results outlive it
+  DevBuf rot, cs, tcos, d_sx, d_sy, region, lines, sum, cc, score, count;
+  std::vector<float> tc(nz);
+  for (int z = 0; z < nz; ++z) tc[z] = (float)std::cos(angles[z] * kD2R);
+  MF_TRY(cs.alloc(sizeof(float2) * num));
+  MF_TRY(tcos.alloc(sizeof(float) * nz));
+  MF_TRY(d_sx.alloc(sizeof(float) * nz));
+  MF_TRY(d_sy.alloc(sizeof(float) * nz));
+  MF_TRY(region.alloc(sizeof(int) * 2 * (size_t)num * L));
+  MF_TRY(lines.alloc(sizeof(float) * (size_t)nz * num * (L + 2)));
+  MF_TRY(sum.alloc(sizeof(cufftComplex) * (size_t)num * cmp));
+  MF_TRY(cc.alloc(sizeof(float) * (size_t)num * nz));
+  MF_TRY(score.alloc(sizeof(float) * num));
+  MF_TRY(rot.alloc(sizeof(float) * num));
+  MF_CHECK_CUDA(cudaMemcpyAsync(rot.p, rot_cand, sizeof(float) * num, cudaMemcpyHostToDevice, st));
+  k_axis_cs<<<(num + 127) / 128, 128, 0, st>>>(rot.as<float>(), num, cs.as<float2>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaMemcpyAsync(tcos.p, tc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_sx.p, sx, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_sy.p, sy, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  k_common_region<<<dim3(num, (L + 127) / 128), dim3(1, 128), 0, st>>>(
+      nx, ny, L, cs.as<float2>(), sx[zt], sy[zt], region.as<int>());
+  // with stage timing on, the Radon kernel is timed on its own and counts its samples
+  if (c->profiling) {
+    MF_TRY(count.alloc(sizeof(unsigned long long)));
+    MF_CHECK_CUDA(cudaMemsetAsync(count.p, 0, sizeof(unsigned long long), st));
+    MF_CHECK_CUDA(cudaEventCreate(&J->ev[0]));
+    MF_CHECK_CUDA(cudaEventCreate(&J->ev[1]));
+    MF_CHECK_CUDA(cudaEventRecord(J->ev[0], st));
+  }
+  k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
+      stack, stack_t, d_neg, nx, ny, L, num, cs.as<float2>(), tcos.as<float>(),
+      d_sx.as<float>(), d_sy.as<float>(), region.as<int>(), lines.as<float>(),
+      count.as<unsigned long long>());
+  if (c->profiling) {
+    MF_CHECK_CUDA(cudaEventRecord(J->ev[1], st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(J->h_count, count.p, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, st));
+  }
+  k_line_prep<<<nz * num, 512, 0, st>>>(lines.as<float>(), L);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
-  scores->resize(num);
-  MF_CHECK_CUDA(cudaMemcpyAsync(scores->data(), B.score.p, sizeof(float) * num,
+  MF_CHECK_CUFFT(cufftExecR2C(plan, lines.as<cufftReal>(), lines.as<cufftComplex>()));
+  const cufftComplex* spec = lines.as<cufftComplex>();
+  k_axis_sum<<<dim3((cmp + 127) / 128, num), 128, 0, st>>>(spec, nz, num, cmp,
+                                                            sum.as<cufftComplex>());
+  k_axis_cc<<<dim3(num, nz), bs, 0, st>>>(spec, sum.as<cufftComplex>(), nz, num, cmp, gs,
+                                          cc.as<float>());
+  k_axis_score<<<(num + 127) / 128, 128, 0, st>>>(cc.as<float>(), nz, num, score.as<float>());
+  c->launches += 3;
+  MF_CHECK_CUDA(cudaGetLastError());
+  MF_CHECK_CUDA(cudaMemcpyAsync(J->h_scores, score.p, sizeof(float) * num,
                                 cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+int tilt_axis_scores_finish(Context* c, AxisJob* J, std::vector<float>* scores) {
+  if (J->ev[0]) {
+    float ms = 0.0f;
+    MF_CHECK_CUDA(cudaEventElapsedTime(&ms, J->ev[0], J->ev[1]));
+    c->breakdown[kStageRadonMs] += ms;
+    c->breakdown[kStageRadonSamples] += (double)*J->h_count;
+    c->breakdown[kStageRadonLaunches] += 1.0;
+    // compulsory bytes: every tilt image once, the line values written once
+    c->breakdown[kStageRadonBytes] +=
+        4.0 * (double)J->nx * J->ny * J->nz + 4.0 * (double)J->nz * J->num * (J->L + 2);
+  }
+  scores->assign(J->h_scores, J->h_scores + J->num);
   return MF_OK;
 }
 

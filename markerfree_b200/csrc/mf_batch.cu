@@ -198,6 +198,8 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     d.stack_t = s->stack_t.as<float>();
     d.sx = s->d_sx.as<float>();
     d.sy = s->d_sy.as<float>();
+    d.sx64 = s->dev_sx64();
+    d.sy64 = s->dev_sy64();
     d.rot = s->d_rot.as<float>();
     d.angles = s->d_angles.as<float>();
     d.z0 = g->d_z0.as<float>() + b;
@@ -233,8 +235,10 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
         g->tcjobs[(size_t)k * B + b] =
             TcJob{v.xt, v.colvalid, g->reproj.as<float>() + (size_t)b * g->bpix, b * nz, 0};
       }
-    // tile rows: timed on the first step of this group's shape (the launches
-    // only write the re-projection buffers, which every pass overwrites)
+    // tile rows: timed on the first step of this group's shape, on a zeroed
+    // 16-bit stack (the launches only write the re-projection buffers, which
+    // every pass overwrites)
+    MF_CHECK_CUDA(cudaMemsetAsync(g->corr16.p, 0, g->corr16.bytes, st));
     MF_TRY(tc_autotune_rows(
         c, xb, yb, B, g->prec,
         [&](int nb) -> int {
@@ -243,7 +247,7 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
           return launch_reproject_tc_group(c, g->tcops, g->tcjobs.data(), B, nullptr, xb, yb, m,
                                            nb, g->d_tcerr.as<int>(), st);
         },
-        &g->tc_nb, st));
+        g->d_tcerr.as<int>(), &g->tc_nb, st));
     MF_TRY(tc_prepare(c, g->tc_nb));
     MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, g->tc_nb, &g->imgmap));
     MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
@@ -428,13 +432,7 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
                                 cudaMemcpyDeviceToHost, st));
   if (g->prec != MF_PREC_FP32)
     MF_CHECK_CUDA(cudaMemcpyAsync(&tcerr, g->d_tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  for (int b = 0; b < B; ++b) {
-    mf_series* s = g->ser[b];
-    MF_CHECK_CUDA(cudaMemcpyAsync(s->sx.data(), s->d_sx.p, sizeof(float) * g->nz,
-                                  cudaMemcpyDeviceToHost, st));
-    MF_CHECK_CUDA(cudaMemcpyAsync(s->sy.data(), s->d_sy.p, sizeof(float) * g->nz,
-                                  cudaMemcpyDeviceToHost, st));
-  }
+  for (int b = 0; b < B; ++b) MF_TRY(g->ser[b]->queue_download_shifts());
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   if (tcerr != 0)
     return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", tcerr);
@@ -498,10 +496,7 @@ int group_proj_align(mf_group* g, int* passes) {
   };
   MF_TRY(once());
   for (int i = 1; i <= 4; ++i) {
-    for (int b = 0; b < B; ++b) {
-      float ax;
-      MF_TRY(tilt_axis(g->ser[b], 20.0f / i, 100, &ax, nullptr));
-    }
+    MF_TRY(tilt_axis_many(g->ser.data(), B, 20.0f / i, 100));
     if (i == 1) MF_TRY(once());
   }
   MF_TRY(once());
@@ -595,8 +590,9 @@ MF_API int mf_group_proj_align(mf_group* g, int* passes) {
 }
 
 // Process::DoIt minus file I/O (Process.cpp:34-92) for n series of one shape:
-// every series is uploaded, pre-processed and coarse-aligned on its own, then
-// projection-matched in groups of up to kMaxGroup, then corrected into d_out[i].
+// every series is uploaded and pre-processed, coarse-aligned stage by stage with
+// the others of its group of up to kMaxGroup, projection-matched with them in
+// lockstep, then corrected into d_out[i].
 MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_raw, int nx, int ny,
                                 int nz, const float* const* file_angles, const mf_options* opt,
                                 mf_align_param* params, float* const* d_out, int* passes) {
@@ -615,11 +611,12 @@ MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_ra
   int rc = MF_OK;
   for (int i = 0; i < n && rc == MF_OK; ++i) {
     rc = mf_series_create_device(ctx, d_raw[i], nx, ny, nz, file_angles[i], &ser[i]);
-    if (rc == MF_OK) {
-      ser[i]->precision = (mf_precision)opt->precision;
-      if (opt->align_z != 0) rc = coarse_align(ser[i], opt->pitch_angle, opt->offset);
-    }
+    if (rc == MF_OK) ser[i]->precision = (mf_precision)opt->precision;
   }
+  // the coarse stages stage by stage over groups of series (one host wait per stage)
+  for (int g0 = 0; g0 < n && rc == MF_OK && opt->align_z != 0; g0 += kMaxGroup)
+    rc = coarse_align_many(ser.data() + g0, std::min(kMaxGroup, n - g0), opt->pitch_angle,
+                           opt->offset);
   for (int g0 = 0; g0 < n && rc == MF_OK && opt->align_z != 0; g0 += kMaxGroup) {
     const int m = std::min(kMaxGroup, n - g0);
     mf_group* g = nullptr;

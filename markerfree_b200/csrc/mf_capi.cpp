@@ -135,6 +135,19 @@ MF_API int mf_context_set_tc_rows(mf_context* ctx, int rows) {
   return MF_OK;
 }
 
+MF_API int mf_context_tc_tuning(mf_context* ctx, double* out, int max_rows, int* n) {
+  if (!ctx || !n || max_rows < 0 || (max_rows > 0 && !out))
+    return set_error(MF_ERR_ARG, "bad argument");
+  const auto& t = ctx->c.tc_tuned;
+  const auto& ms = ctx->c.tc_tuned_ms;
+  *n = (int)t.size();
+  for (int i = 0; i < (int)t.size() && i < max_rows; ++i) {
+    for (int k = 0; k < 5; ++k) out[8 * i + k] = t[i][k];
+    for (int k = 0; k < 3; ++k) out[8 * i + 5 + k] = i < (int)ms.size() ? ms[i][k] : 0.0;
+  }
+  return MF_OK;
+}
+
 // ---------------------------------------------------------------------------
 static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_device, int nx,
                                 int ny, int nz, const float* file_angles, mf_series** out) {

@@ -60,6 +60,30 @@ void DevBuf::release() {
   st = nullptr;
 }
 
+void* PinnedSlots::get(int i, size_t bytes) {
+  if (i < 0) return nullptr;
+  if ((int)slot.size() <= i) slot.resize(i + 1, {nullptr, 0});
+  auto& e = slot[i];
+  if (e.first && e.second >= bytes) return e.first;
+  if (e.first) cudaFreeHost(e.first);
+  e = {nullptr, 0};
+  size_t n = bytes < 4096 ? 4096 : bytes;
+  if (cudaHostAlloc(&e.first, n, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    e.first = nullptr;
+    set_error(MF_ERR_NOMEM, "page-locked host allocation of %zu bytes failed", n);
+    return nullptr;
+  }
+  e.second = n;
+  return e.first;
+}
+
+PinnedSlots::~PinnedSlots() {
+  for (auto& e : slot)
+    if (e.first) cudaFreeHost(e.first);
+  cudaGetLastError();
+}
+
 FftPlan::~FftPlan() { release(); }
 
 void FftPlan::release() {

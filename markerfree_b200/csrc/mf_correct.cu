@@ -308,11 +308,30 @@ __global__ void k_block_min(const float* __restrict__ p, size_t n, float* __rest
   if (threadIdx.x == 0) part[blockIdx.x] = s[0];
 }
 
-// One block per slice: FP64 sum and count of (v - min) over the central box.
-__global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny, float sub,
-                           int subtract, double* __restrict__ sums, int* __restrict__ counts) {
+// SetPositive's stack minimum (fStackMin starts at 1e30, slice minima at 1e20)
+// from the block minima: mm[0] = min(1e30, minima...) capped at 1e20.
+__global__ void k_min_final(const float* __restrict__ part, int nb, float* __restrict__ mm) {
+  __shared__ float s[256];
+  float m = 1e30f;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fminf(m, part[i]);
+  s[threadIdx.x] = m;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) s[threadIdx.x] = fminf(s[threadIdx.x], s[threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) mm[0] = s[0] > 1e20f ? 1e20f : s[0];
+}
+
+// One block per slice: FP64 sum and count of (v - min) over the central box; the
+// minimum is subtracted only when it is below zero (Preprocess.cu:103-160).
+__global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny,
+                           const float* __restrict__ mm, double* __restrict__ sums,
+                           int* __restrict__ counts) {
   __shared__ double s_sum[256];
   __shared__ int s_cnt[256];
+  const float sub = mm[0];
+  const bool subtract = !(sub >= 0);
   const int z = blockIdx.x;
   const int x0 = nx * 1 / 6, y0 = ny * 1 / 6, w = nx * 4 / 6, h = ny * 4 / 6;
   const float* f = stack + (size_t)z * nx * ny;
@@ -342,9 +361,23 @@ __global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny, floa
   }
 }
 
+// MassNormalization's factors (Preprocess.cu:162-250): every slice is scaled to the
+// mean of the zero tilt (file order index `zero`), capped at 1000.
+__global__ void k_mass_scale(const double* __restrict__ sums, const int* __restrict__ counts,
+                             int nz, int zero, float* __restrict__ scale) {
+  const float ref0 = counts[zero] == 0 ? 0.0f : (float)(sums[zero] / counts[zero]);
+  const float ref = ref0 > 1000.0f ? 1000.0f : ref0;
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) {
+    const float mean = counts[i] == 0 ? 0.0f : (float)(sums[i] / counts[i]);
+    scale[i] = __fdiv_rn(ref, __fadd_rn(mean, 0.00001f));
+  }
+}
+
 // out = (v - min) * scale[z], skipping sentinels as Subtract and mScale do.
-__global__ void k_positive_scale(float* __restrict__ stack, size_t pix, int nz, float sub,
-                                 int subtract, const float* __restrict__ scale) {
+__global__ void k_positive_scale(float* __restrict__ stack, size_t pix, int nz,
+                                 const float* __restrict__ mm, const float* __restrict__ scale) {
+  const float sub = mm[0];
+  const bool subtract = !(sub >= 0);
   size_t n = pix * nz;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -355,48 +388,31 @@ __global__ void k_positive_scale(float* __restrict__ stack, size_t pix, int nz, 
   }
 }
 
+// The whole pre-processing is queued on st with no host round trip: the minimum,
+// the slice means and the scale factors stay in device memory.
 int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
                       const float* file_angles, cudaStream_t st) {
   size_t pix = (size_t)nx * ny;
   size_t n = pix * nz;
   const int nb = 1024;
-  DevBuf part, sums, counts, scale;
+  DevBuf part, sums, counts, scale, mm;
   MF_TRY(part.alloc(sizeof(float) * nb));
   MF_TRY(sums.alloc(sizeof(double) * nz));
   MF_TRY(counts.alloc(sizeof(int) * nz));
   MF_TRY(scale.alloc(sizeof(float) * nz));
+  MF_TRY(mm.alloc(sizeof(float)));
   k_block_min<<<nb, 256, 0, st>>>(d_stack, n, part.as<float>());
-  c->launches++;
-  MF_CHECK_CUDA(cudaGetLastError());
-  std::vector<float> hp(nb);
-  MF_CHECK_CUDA(cudaMemcpyAsync(hp.data(), part.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  float mn = 1e30f;  // SetPositive: fStackMin starts at 1e30, slice minima start at 1e20
-  for (float v : hp) mn = std::fmin(mn, v);
-  if (mn > 1e20f) mn = 1e20f;
-  int subtract = !(mn >= 0);
-  k_box_mean<<<nz, 256, 0, st>>>(d_stack, nx, ny, mn, subtract, sums.as<double>(),
+  k_min_final<<<1, 256, 0, st>>>(part.as<float>(), nb, mm.as<float>());
+  k_box_mean<<<nz, 256, 0, st>>>(d_stack, nx, ny, mm.as<float>(), sums.as<double>(),
                                   counts.as<int>());
-  c->launches++;
-  MF_CHECK_CUDA(cudaGetLastError());
-  std::vector<double> hs(nz);
-  std::vector<int> hc(nz);
-  MF_CHECK_CUDA(cudaMemcpyAsync(hs.data(), sums.p, sizeof(double) * nz, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int) * nz, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  std::vector<float> mean(nz), sc(nz);
-  for (int i = 0; i < nz; ++i) mean[i] = hc[i] == 0 ? 0.0f : (float)(hs[i] / hc[i]);
   // the zero tilt is looked up in the file-order angles (Preprocess.cu:168)
-  int zero = frame_idx_from_tilt(nz, file_angles, 0.0f);
-  float ref = mean[zero];
-  if (ref > 1000.0f) ref = 1000.0f;
-  for (int i = 0; i < nz; ++i) sc[i] = ref / (mean[i] + 0.00001f);
-  MF_CHECK_CUDA(cudaMemcpyAsync(scale.p, sc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
-  k_positive_scale<<<c->sm_count * 8, 256, 0, st>>>(d_stack, pix, nz, mn, subtract,
+  const int zero = frame_idx_from_tilt(nz, file_angles, 0.0f);
+  k_mass_scale<<<1, 256, 0, st>>>(sums.as<double>(), counts.as<int>(), nz, zero,
+                                  scale.as<float>());
+  k_positive_scale<<<c->sm_count * 8, 256, 0, st>>>(d_stack, pix, nz, mm.as<float>(),
                                                      scale.as<float>());
-  c->launches++;
+  c->launches += 5;
   MF_CHECK_CUDA(cudaGetLastError());
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;
 }
 

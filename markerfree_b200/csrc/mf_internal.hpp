@@ -86,6 +86,20 @@ struct DevBuf {
   }
 };
 
+// Page-locked host slots for results that kernels deliver to the host: a copy into
+// pageable memory would make the host wait for the stream at the copy, so the
+// stages that queue work for many series before waiting once copy their results
+// here instead.  Slot i grows (cudaHostAlloc) the first time it is asked for more
+// bytes and is kept for the context's lifetime.
+struct PinnedSlots {
+  std::vector<std::pair<void*, size_t>> slot;
+  void* get(int i, size_t bytes);  // nullptr (error set) when the allocation fails
+  PinnedSlots() = default;
+  PinnedSlots(const PinnedSlots&) = delete;
+  PinnedSlots& operator=(const PinnedSlots&) = delete;
+  ~PinnedSlots();
+};
+
 // cuFFT plan wrapper; plans are created on first use and bound to a stream.
 struct FftPlan {
   cufftHandle h = 0;
@@ -113,6 +127,9 @@ struct Context {
   int tc_rows = 0;  // tensor-core tile rows (64/128/256); 0 = chosen per shape
   // tile rows the autotuner chose, per (xb, yb, jobs, precision)
   std::vector<std::array<int, 5>> tc_tuned;
+  // median ms per launch the autotuner measured for 256/128/64 rows, per entry of tc_tuned
+  std::vector<std::array<float, 3>> tc_tuned_ms;
+  PinnedSlots pinned;  // host result slots of the queued stages
   double stage[6] = {0, 0, 0, 0, 0, 0};  // see mf_context_stage_times
   double breakdown[kStages] = {};        // ms per stage, see mf_context_stage_breakdown
 };
@@ -289,12 +306,16 @@ int tc_image_map(const void* base, int half_kind, int xb, int xpitch, int yb, in
 // override if set, else the widest of 256/128/64 that still gives most SMs a tile.
 int tc_pick_rows(const Context* c, int xb, int yb);
 // Autotuner of the tile rows: times `launch(nb)` (one re-projection step with
-// tiles of nb rows, queued on st) for nb = 64, 128, 256, keeps the fastest for
-// the shape (xb, yb, jobs, precision) in the context and returns it in *nb_out.
-// A shape seen before, or tile rows fixed with mf_context_set_tc_rows, is not
-// timed again.
+// tiles of nb rows, queued on st) for nb = 64, 128, 256 -- one untimed launch,
+// then the median of five timed ones -- keeps the fastest for the shape (xb, yb,
+// jobs, precision) in the context and returns it in *nb_out.  The kernel's
+// pipeline error word d_err is cleared before each variant and read after it: a
+// variant whose bounded waits gave up fails the call with MF_ERR_CUDA instead of
+// looking fast.  A shape seen before, or tile rows fixed with
+// mf_context_set_tc_rows, is not timed again.
 int tc_autotune_rows(Context* c, int xb, int yb, int jobs, int prec,
-                     const std::function<int(int)>& launch, int* nb_out, cudaStream_t st);
+                     const std::function<int(int)>& launch, int* d_err, int* nb_out,
+                     cudaStream_t st);
 // Sets the kernel attributes of the tile-rows variant `nb` on the current device
 // (done outside any stream capture).
 int tc_prepare(Context* c, int nb);
@@ -330,6 +351,10 @@ struct GroupSeriesDev {
   const float* stack_t;  // the same, column-major per tilt (nz x nx x ny)
   float* sx;
   float* sy;
+  // FP16/BF16 modes: the FP64 accumulators of the shifts (sx/sy hold their float
+  // values); null in FP32 mode, where shifts accumulate in float as in the reference
+  double* sx64;
+  double* sy64;
   const float* rot;
   const float* angles;
   float* z0;

@@ -121,10 +121,14 @@ int series_init(mf_series* s, mf_context* ctx, int nx, int ny, int nz, const flo
   if (nz > 1 && s->angles[0] > s->angles[1]) std::reverse(s->angles.begin(), s->angles.end());
   s->sx.assign(nz, 0.0f);
   s->sy.assign(nz, 0.0f);
+  s->sx64.assign(nz, 0.0);
+  s->sy64.assign(nz, 0.0);
   s->rot.assign(nz, 0.0f);
   s->angle_offset = 0.0f;
   MF_TRY(s->d_sx.alloc(sizeof(float) * nz));
   MF_TRY(s->d_sy.alloc(sizeof(float) * nz));
+  MF_TRY(s->d_sx64.alloc(sizeof(double) * nz));
+  MF_TRY(s->d_sy64.alloc(sizeof(double) * nz));
   MF_TRY(s->d_rot.alloc(sizeof(float) * nz));
   MF_TRY(s->d_angles.alloc(sizeof(float) * nz));
   return MF_OK;
@@ -136,26 +140,49 @@ int mf_series::upload_params() {
   cudaStream_t st = ctx->c.stream;
   MF_CHECK_CUDA(cudaMemcpyAsync(d_sx.p, sx.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_sy.p, sy.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+  if (shift64()) {
+    for (int i = 0; i < nz; ++i) {
+      if ((float)sx64[i] != sx[i]) sx64[i] = sx[i];
+      if ((float)sy64[i] != sy[i]) sy64[i] = sy[i];
+    }
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_sx64.p, sx64.data(), sizeof(double) * nz,
+                                  cudaMemcpyHostToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(d_sy64.p, sy64.data(), sizeof(double) * nz,
+                                  cudaMemcpyHostToDevice, st));
+  }
   MF_CHECK_CUDA(cudaMemcpyAsync(d_rot.p, rot.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_angles.p, angles.data(), sizeof(float) * nz,
                                 cudaMemcpyHostToDevice, st));
   return MF_OK;
 }
 
-int mf_series::download_shifts() {
+int mf_series::queue_download_shifts() {
   cudaStream_t st = ctx->c.stream;
   MF_CHECK_CUDA(cudaMemcpyAsync(sx.data(), d_sx.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(sy.data(), d_sy.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (shift64()) {
+    MF_CHECK_CUDA(cudaMemcpyAsync(sx64.data(), d_sx64.p, sizeof(double) * nz,
+                                  cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(sy64.data(), d_sy64.p, sizeof(double) * nz,
+                                  cudaMemcpyDeviceToHost, st));
+  }
+  return MF_OK;
+}
+
+int mf_series::download_shifts() {
+  MF_TRY(queue_download_shifts());
+  MF_CHECK_CUDA(cudaStreamSynchronize(ctx->c.stream));
   return MF_OK;
 }
 
 namespace mf {
 
 // ---------------------------------------------------------------------------
-// Transform::DoIt + Measure (Transform.cpp:60-97), all tilt pairs batched.
-int transform_doit(mf_series* s, float* max_err_out) {
-  StageTimer timer(&s->ctx->c, kStageCoarse);
+// Transform::DoIt + Measure (Transform.cpp:60-97), all tilt pairs batched.  The
+// pass is queued by transform_enqueue (its measured shifts land in page-locked
+// slot `slot` of the context) and applied by transform_finish once the stream
+// has been synchronised.
+int transform_enqueue(mf_series* s, int slot, TransformJob* J) {
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   const int nx = s->nx, ny = s->ny, nz = s->nz;
@@ -172,6 +199,7 @@ int transform_doit(mf_series* s, float* max_err_out) {
   const int xb = T.xb, yb = T.yb, pad = xb + 2, cmp = xb / 2 + 1;
   const size_t bpix = (size_t)xb * yb, ppix = (size_t)pad * yb;
   MF_TRY(s->upload_params());
+  // device buffers are released stream-ordered on return, after the queued work
   DevBuf corr, pbuf, refs, imgs, part, stats, d_idx, d_refidx, d_mats, d_shifts, d_peakpart;
   MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
   MF_TRY(pbuf.alloc(sizeof(float) * ppix * nz));
@@ -184,8 +212,10 @@ int transform_doit(mf_series* s, float* max_err_out) {
       corr.as<float>(), xb, yb, pad, pbuf.as<float>());
   c->launches++;
   // pairs
-  std::vector<int> img_idx, ref_idx;
+  std::vector<int>& img_idx = J->img_idx;
+  std::vector<int> ref_idx;
   std::vector<float> mats;
+  img_idx.clear();
   for (int z = 0; z < nz; ++z) {
     int r = find_ref_index(nz, s->angles.data(), z);
     if (r == z) continue;
@@ -197,57 +227,66 @@ int transform_doit(mf_series* s, float* max_err_out) {
     mats.insert(mats.end(), m, m + 3);
   }
   const int np = (int)img_idx.size();
+  J->np = np;
+  J->h_sh = nullptr;
+  if (np == 0) return MF_OK;
+  J->h_sh = (float2*)c->pinned.get(slot, sizeof(float2) * np);
+  if (!J->h_sh) return MF_ERR_NOMEM;
+  MF_TRY(imgs.alloc(sizeof(float) * ppix * np));
+  MF_TRY(part.alloc(sizeof(double2) * moment_parts(yb) * std::max(nz, np)));
+  MF_TRY(stats.alloc(sizeof(float2) * std::max(nz, np)));
+  MF_TRY(d_idx.alloc(sizeof(int) * np));
+  MF_TRY(d_refidx.alloc(sizeof(int) * np));
+  MF_TRY(d_mats.alloc(sizeof(float) * 3 * np));
+  MF_TRY(d_shifts.alloc(sizeof(float2) * np));
+  MF_TRY(d_peakpart.alloc(sizeof(float2) * 32 * np));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, img_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_refidx.p, ref_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(d_mats.p, mats.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
+  const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
+  if (!T.mask.p) {  // one geometry for every stretch correlation of the series
+    MF_TRY(T.mask.alloc(sizeof(float) * bpix));
+    MF_TRY(make_round_mask(c, xb, yb, cx, cy, msx, msy, 4.0f, T.mask.as<float>(), st));
+  }
+  // references: normalise (mean, std) + round edge, all tilts
+  MF_TRY(norm_mask_pad(c, pbuf.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy,
+                       msx, msy, 4.0f, T.mask.as<float>(), refs.as<float>(), part.as<double2>(),
+                       stats.as<float2>(), st));
+  // images: stretch the padded raw copy, then normalise + round edge
+  MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
+                      np, 1, imgs.as<float>(), ppix, st));
+  MF_TRY(norm_mask_pad(c, imgs.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy,
+                       msx, msy, 4.0f, T.mask.as<float>(), imgs.as<float>(), part.as<double2>(),
+                       stats.as<float2>(), st));
+  cufftHandle fr, fi, inv;
+  MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));
+  MF_TRY(s->ctx->plan({2, xb, yb, np}, &fi));
+  MF_TRY(s->ctx->plan({3, xb, yb, np}, &inv));
+  MF_CHECK_CUFFT(cufftExecR2C(fr, refs.as<cufftReal>(), refs.as<cufftComplex>()));
+  MF_CHECK_CUFFT(cufftExecR2C(fi, imgs.as<cufftReal>(), imgs.as<cufftComplex>()));
+  float scale = (float)(1.0 / ((cmp - 1) * 2) / yb);
+  MF_TRY(xcorr_filter(c, refs.as<cufftComplex>(), ppix / 2, d_refidx.as<int>(),
+                      imgs.as<cufftComplex>(), ppix / 2, np, cmp, yb, 400.0f, scale, st));
+  MF_CHECK_CUFFT(cufftExecC2R(inv, imgs.as<cufftComplex>(), imgs.as<cufftReal>()));
+  MF_TRY(cc_peaks(c, imgs.as<float>(), ppix, pad, xb, yb, np, d_peakpart.as<float2>(),
+                  d_shifts.as<float2>(), st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(J->h_sh, d_shifts.p, sizeof(float2) * np, cudaMemcpyDeviceToHost,
+                                st));
+  return MF_OK;
+}
+
+int transform_finish(mf_series* s, TransformJob* J, float* max_err_out) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  TransformState& T = s->tr;
+  const int xb = T.xb, yb = T.yb;
   float maxerr = 0.0f;
-  if (np > 0) {
-    MF_TRY(imgs.alloc(sizeof(float) * ppix * np));
-    MF_TRY(part.alloc(sizeof(double2) * moment_parts(yb) * std::max(nz, np)));
-    MF_TRY(stats.alloc(sizeof(float2) * std::max(nz, np)));
-    MF_TRY(d_idx.alloc(sizeof(int) * np));
-    MF_TRY(d_refidx.alloc(sizeof(int) * np));
-    MF_TRY(d_mats.alloc(sizeof(float) * 3 * np));
-    MF_TRY(d_shifts.alloc(sizeof(float2) * np));
-    MF_TRY(d_peakpart.alloc(sizeof(float2) * 32 * np));
-    MF_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, img_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
-    MF_CHECK_CUDA(cudaMemcpyAsync(d_refidx.p, ref_idx.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
-    MF_CHECK_CUDA(cudaMemcpyAsync(d_mats.p, mats.data(), sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
-    const float cx = xb * 0.5f, cy = yb * 0.5f, msx = xb * 1.0f, msy = yb * 1.0f;
-    if (!T.mask.p) {  // one geometry for every stretch correlation of the series
-      MF_TRY(T.mask.alloc(sizeof(float) * bpix));
-      MF_TRY(make_round_mask(c, xb, yb, cx, cy, msx, msy, 4.0f, T.mask.as<float>(), st));
-    }
-    // references: normalise (mean, std) + round edge, all tilts
-    MF_TRY(norm_mask_pad(c, pbuf.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, nz, 1, cx, cy,
-                         msx, msy, 4.0f, T.mask.as<float>(), refs.as<float>(), part.as<double2>(),
-                         stats.as<float2>(), st));
-    // images: stretch the padded raw copy, then normalise + round edge
-    MF_TRY(stretch_many(c, pbuf.as<float>(), ppix, d_idx.as<int>(), xb, yb, pad, d_mats.as<float>(),
-                        np, 1, imgs.as<float>(), ppix, st));
-    MF_TRY(norm_mask_pad(c, imgs.as<float>(), nullptr, pad, ppix, xb, yb, pad, ppix, np, 1, cx, cy,
-                         msx, msy, 4.0f, T.mask.as<float>(), imgs.as<float>(), part.as<double2>(),
-                         stats.as<float2>(), st));
-    cufftHandle fr, fi, inv;
-    MF_TRY(s->ctx->plan({2, xb, yb, nz}, &fr));
-    MF_TRY(s->ctx->plan({2, xb, yb, np}, &fi));
-    MF_TRY(s->ctx->plan({3, xb, yb, np}, &inv));
-    MF_CHECK_CUFFT(cufftExecR2C(fr, refs.as<cufftReal>(), refs.as<cufftComplex>()));
-    MF_CHECK_CUFFT(cufftExecR2C(fi, imgs.as<cufftReal>(), imgs.as<cufftComplex>()));
-    float scale = (float)(1.0 / ((cmp - 1) * 2) / yb);
-    MF_TRY(xcorr_filter(c, refs.as<cufftComplex>(), ppix / 2, d_refidx.as<int>(),
-                        imgs.as<cufftComplex>(), ppix / 2, np, cmp, yb, 400.0f, scale, st));
-    MF_CHECK_CUFFT(cufftExecC2R(inv, imgs.as<cufftComplex>(), imgs.as<cufftReal>()));
-    MF_TRY(cc_peaks(c, imgs.as<float>(), ppix, pad, xb, yb, np, d_peakpart.as<float2>(),
-                    d_shifts.as<float2>(), st));
-    std::vector<float2> sh(np);
-    MF_CHECK_CUDA(cudaMemcpyAsync(sh.data(), d_shifts.p, sizeof(float2) * np, cudaMemcpyDeviceToHost, st));
-    MF_CHECK_CUDA(cudaStreamSynchronize(st));
-    float binx = nx * 1.0f / xb, biny = ny * 1.0f / yb;
-    for (int p = 0; p < np; ++p) {
-      int z = img_idx[p];
-      T.pshx[z] = sh[p].x * binx;
-      T.pshy[z] = sh[p].y * biny;
-      float e = (float)std::sqrt(T.pshx[z] * T.pshx[z] + T.pshy[z] * T.pshy[z]);
-      if (e > maxerr) maxerr = e;
-    }
+  float binx = nx * 1.0f / xb, biny = ny * 1.0f / yb;
+  for (int p = 0; p < J->np; ++p) {
+    int z = J->img_idx[p];
+    T.pshx[z] = J->h_sh[p].x * binx;
+    T.pshy[z] = J->h_sh[p].y * biny;
+    float e = (float)std::sqrt(T.pshx[z] * T.pshx[z] + T.pshy[z] * T.pshy[z]);
+    if (e > maxerr) maxerr = e;
   }
   // UpdateShift + UnStretch (Transform.cpp:99-157)
   int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
@@ -287,17 +326,27 @@ int transform_doit(mf_series* s, float* max_err_out) {
   return MF_OK;
 }
 
+int transform_doit(mf_series* s, float* max_err_out) {
+  StageTimer timer(&s->ctx->c, kStageCoarse);
+  TransformJob J;
+  MF_TRY(transform_enqueue(s, 0, &J));
+  MF_CHECK_CUDA(cudaStreamSynchronize(s->ctx->c.stream));
+  return transform_finish(s, &J, max_err_out);
+}
+
 // ---------------------------------------------------------------------------
-// CalcTIltAxis::DoIt + CLsetup (Rotate.cu:292-374)
-int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores_out) {
-  StageTimer timer(&s->ctx->c, kStageAxis);
+// CalcTIltAxis::DoIt + CLsetup (Rotate.cu:292-374): axis_enqueue queues one search
+// (scores to the context's page-locked slot `slot`), axis_finish applies the
+// arg-max rule once the stream has been synchronised.
+int axis_enqueue(mf_series* s, float range, int num, int slot, AxisSearch* A) {
   if (num < 2) return set_error(MF_ERR_ARG, "tilt axis: need at least 2 candidates");
   Context* c = &s->ctx->c;
   const int nz = s->nz;
   int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
   float axis0 = s->rot[zt];
   float step = range / (num - 1);
-  std::vector<float> cand(num);
+  std::vector<float>& cand = A->cand;
+  cand.assign(num, 0.0f);
   cand[0] = axis0 - step * num / 2;
   for (int i = 1; i < num; ++i) cand[i] = cand[i - 1] + step;
   float fmin_size = 1e20f;
@@ -312,13 +361,18 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores
   int L = (int)fmin_size;
   L = L / 2 * 2 - 100;
   if (L < 4) return set_error(MF_ERR_ARG, "tilt axis: image too small (line length %d)", L);
-  std::vector<float> scores;
   cufftHandle plan;
   MF_TRY(s->ctx->plan({4, L, 0, (long long)nz * num}, &plan));
-  MF_TRY(tilt_axis_scores(c, plan, s->stack.as<float>(), s->stack_t.as<float>(),
-                          s->d_neg.as<int>(), s->nx, s->ny, nz, s->angles.data(),
-                          s->sx.data(), s->sy.data(), zt, cand.data(), num, L, &scores,
-                          c->stream));
+  return tilt_axis_scores_enqueue(c, plan, s->stack.as<float>(), s->stack_t.as<float>(),
+                                  s->d_neg.as<int>(), s->nx, s->ny, nz, s->angles.data(),
+                                  s->sx.data(), s->sy.data(), zt, cand.data(), num, L, slot,
+                                  &A->job, c->stream);
+}
+
+int axis_finish(mf_series* s, AxisSearch* A, float* axis_out, float* scores_out) {
+  std::vector<float> scores;
+  MF_TRY(tilt_axis_scores_finish(&s->ctx->c, &A->job, &scores));
+  const int num = (int)A->cand.size(), nz = s->nz;
   if (scores_out) std::copy(scores.begin(), scores.end(), scores_out);
   int best = 0;
   float bs = 0.0f;
@@ -327,7 +381,7 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores
       bs = scores[i];
       best = i;
     }
-  float axis = cand[best];
+  float axis = A->cand[best];
   if (axis < -45 && s->rot[0] == 0) axis += 180.0f;
   if (axis > 135) axis -= 180.0f;
   for (int i = 0; i < nz; ++i) s->rot[i] = axis;
@@ -335,10 +389,19 @@ int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores
   return MF_OK;
 }
 
+int tilt_axis(mf_series* s, float range, int num, float* axis_out, float* scores_out) {
+  StageTimer timer(&s->ctx->c, kStageAxis);
+  AxisSearch A;
+  MF_TRY(axis_enqueue(s, range, num, 0, &A));
+  MF_CHECK_CUDA(cudaStreamSynchronize(s->ctx->c.stream));
+  return axis_finish(s, &A, axis_out, scores_out);
+}
+
 // ---------------------------------------------------------------------------
-// FindOffset::DoIt (FindOffset.cu:85-238)
-int find_offset(mf_series* s, float* offset_out) {
-  StageTimer timer(&s->ctx->c, kStageCoarse);
+// FindOffset::DoIt (FindOffset.cu:85-238): offset_enqueue queues the moments of
+// every (offset, tilt pair) (to the context's page-locked slot `slot`),
+// offset_finish picks the offset once the stream has been synchronised.
+int offset_enqueue(mf_series* s, int slot, OffsetJob* J) {
   Context* c = &s->ctx->c;
   cudaStream_t st = c->stream;
   const int nx = s->nx, ny = s->ny, nz = s->nz, bin = 4;
@@ -346,16 +409,18 @@ int find_offset(mf_series* s, float* offset_out) {
   if (xb < 2 || yb < 2) return set_error(MF_ERR_ARG, "find offset: image too small");
   const size_t bpix = (size_t)xb * yb;
   MF_TRY(s->upload_params());
+  // device buffers are released stream-ordered on return, after the queued work
   DevBuf corr, d_pairs, d_out;
   MF_TRY(corr.alloc(sizeof(float) * bpix * nz));
   MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
                             nx, ny, nullptr, nz, s->d_sx.as<float>(),
                             s->d_sy.as<float>(), s->d_rot.as<float>(), 0, bin, 0,
                             corr.as<float>(), xb, bpix, st));
-  const int num = 31;
+  const int num = kOffsetCount;
   std::vector<float> a = s->angles;
   std::vector<OffsetPair> pairs;
-  std::vector<int> first(num + 1, 0);
+  std::vector<int>& first = J->first;
+  first.assign(num + 1, 0);
   for (int n = 0; n < num; ++n) {
     float off = 0.0f + (n - num / 2) * 1.0f;
     for (int z = 0; z < nz; ++z) a[z] += off;
@@ -373,16 +438,23 @@ int find_offset(mf_series* s, float* offset_out) {
   }
   first[num] = (int)pairs.size();
   const int np = (int)pairs.size();
+  J->h_mom = (double*)c->pinned.get(slot, sizeof(double) * 6 * std::max(np, 1));
+  if (!J->h_mom) return MF_ERR_NOMEM;
   MF_TRY(d_pairs.alloc(sizeof(OffsetPair) * np));
   MF_TRY(d_out.alloc(sizeof(double) * 6 * np));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_pairs.p, pairs.data(), sizeof(OffsetPair) * np,
                                 cudaMemcpyHostToDevice, st));
   MF_TRY(offset_moments(c, corr.as<float>(), xb, yb, d_pairs.as<OffsetPair>(), np,
                         d_out.as<double>(), st));
-  std::vector<double> mom((size_t)6 * np);
-  MF_CHECK_CUDA(cudaMemcpyAsync(mom.data(), d_out.p, sizeof(double) * 6 * np,
+  MF_CHECK_CUDA(cudaMemcpyAsync(J->h_mom, d_out.p, sizeof(double) * 6 * np,
                                 cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+int offset_finish(mf_series* s, OffsetJob* J, float* offset_out) {
+  const int num = kOffsetCount;
+  const std::vector<int>& first = J->first;
+  const double* mom = J->h_mom;
   float maxcc = 0.0f, best = 0.0f;
   for (int n = 0; n < num; ++n) {
     float off = 0.0f + (n - num / 2) * 1.0f;
@@ -416,6 +488,14 @@ int find_offset(mf_series* s, float* offset_out) {
   s->angle_offset += best;
   if (offset_out) *offset_out = best;
   return MF_OK;
+}
+
+int find_offset(mf_series* s, float* offset_out) {
+  StageTimer timer(&s->ctx->c, kStageCoarse);
+  OffsetJob J;
+  MF_TRY(offset_enqueue(s, 0, &J));
+  MF_CHECK_CUDA(cudaStreamSynchronize(s->ctx->c.stream));
+  return offset_finish(s, &J, offset_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -569,7 +649,7 @@ static int pa_enqueue(mf_series* s) {
                           P.tflags.as<int>(), st));
   // FitRotCenterZ + RemoveOffsetZ(-1)
   MF_TRY(fit_z0(c, nz, P.zt, s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
-                s->d_rot.as<float>(), P.d_z0.as<float>(), st));
+                s->dev_sx64(), s->dev_sy64(), s->d_rot.as<float>(), P.d_z0.as<float>(), st));
   const bool prof = c->profiling && (int)P.events.size() >= 3 * n;
   for (int k = 0; k < n; ++k) {
     const int ip = P.order[k];
@@ -605,7 +685,8 @@ static int pa_enqueue(mf_series* s) {
     MF_CHECK_CUFFT(cufftExecC2R(P.cc_inv, (cufftComplex*)(cc + ppix), cc + ppix));
     MF_TRY(pa_peak_update(c, cc + ppix, pad, xb, yb, ppart, ip, s->nx, s->ny,
                           s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
-                          s->d_rot.as<float>(), P.d_z0.as<float>(), P.d_err.as<float>(),
+                          s->dev_sx64(), s->dev_sy64(), s->d_rot.as<float>(), P.d_z0.as<float>(),
+                          P.d_err.as<float>(),
                           P.d_meas.as<float>(), st));
     // re-correct the aligned tilt (mCorrectProj)
     MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
@@ -719,6 +800,56 @@ int coarse_align(mf_series* s, float pitch_angle, float offset) {
     s->angle_offset = offset;
   }
   for (int z = 0; z < s->nz; ++z) s->angles[z] += s->angle_offset;
+  return MF_OK;
+}
+
+// The same for n series of one context, stage by stage: every stage is queued for
+// all series (results to page-locked slots 0..n-1) before one wait, so the GPU
+// runs the series' work back to back instead of idling at a host round trip per
+// series.  Each series' arithmetic and decisions are those of coarse_align.
+int transform_many(mf_series* const* ser, int n) {
+  StageTimer timer(&ser[0]->ctx->c, kStageCoarse);
+  std::vector<TransformJob> J(n);
+  for (int i = 0; i < n; ++i) MF_TRY(transform_enqueue(ser[i], i, &J[i]));
+  MF_CHECK_CUDA(cudaStreamSynchronize(ser[0]->ctx->c.stream));
+  for (int i = 0; i < n; ++i) MF_TRY(transform_finish(ser[i], &J[i], nullptr));
+  return MF_OK;
+}
+
+int tilt_axis_many(mf_series* const* ser, int n, float range, int num) {
+  StageTimer timer(&ser[0]->ctx->c, kStageAxis);
+  std::vector<AxisSearch> A(n);
+  for (int i = 0; i < n; ++i) MF_TRY(axis_enqueue(ser[i], range, num, i, &A[i]));
+  MF_CHECK_CUDA(cudaStreamSynchronize(ser[0]->ctx->c.stream));
+  for (int i = 0; i < n; ++i) MF_TRY(axis_finish(ser[i], &A[i], nullptr, nullptr));
+  return MF_OK;
+}
+
+int coarse_align_many(mf_series* const* ser, int n, float pitch_angle, float offset) {
+  if (n < 1) return MF_OK;
+  for (int i = 1; i < n; ++i)
+    if (ser[i]->ctx != ser[0]->ctx) return set_error(MF_ERR_ARG, "series of different contexts");
+  if (pitch_angle == 0) {
+    for (int i = 0; i < n; ++i) ser[i]->tr.ready = false;
+    for (int k = 1; k <= 3; ++k) {
+      MF_TRY(transform_many(ser, n));
+      MF_TRY(tilt_axis_many(ser, n, 180.0f / k, 100));
+    }
+  } else {
+    for (int i = 0; i < n; ++i)
+      for (int z = 0; z < ser[i]->nz; ++z) ser[i]->rot[z] = pitch_angle;
+  }
+  if (offset == 0) {
+    StageTimer timer(&ser[0]->ctx->c, kStageCoarse);
+    std::vector<OffsetJob> J(n);
+    for (int i = 0; i < n; ++i) MF_TRY(offset_enqueue(ser[i], i, &J[i]));
+    MF_CHECK_CUDA(cudaStreamSynchronize(ser[0]->ctx->c.stream));
+    for (int i = 0; i < n; ++i) MF_TRY(offset_finish(ser[i], &J[i], nullptr));
+  } else {
+    for (int i = 0; i < n; ++i) ser[i]->angle_offset = offset;
+  }
+  for (int i = 0; i < n; ++i)
+    for (int z = 0; z < ser[i]->nz; ++z) ser[i]->angles[z] += ser[i]->angle_offset;
   return MF_OK;
 }
 

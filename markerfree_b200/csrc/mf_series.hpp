@@ -4,6 +4,7 @@
 #include <memory>
 
 #include "mf_internal.hpp"
+#include "mf_xcorr.hpp"
 
 struct mf_context {
   mf::Context c;
@@ -76,16 +77,53 @@ struct mf_series {
   std::vector<float> file_angles;
   std::vector<float> angles;
   std::vector<float> sx, sy, rot;
+  // FP16/BF16 modes: the shifts' FP64 accumulators (sx/sy hold their float values).
+  // A float value the host changed replaces its accumulator at the next upload.
+  std::vector<double> sx64, sy64;
   float angle_offset = 0.0f;
-  mf::DevBuf d_sx, d_sy, d_rot, d_angles;
+  mf::DevBuf d_sx, d_sy, d_rot, d_angles, d_sx64, d_sy64;
   mf_precision precision = MF_PREC_FP32;
   mf::TransformState tr;
   mf::ProjAlignState pa;
+  bool shift64() const { return precision != MF_PREC_FP32; }
+  double* dev_sx64() { return shift64() ? d_sx64.as<double>() : nullptr; }
+  double* dev_sy64() { return shift64() ? d_sy64.as<double>() : nullptr; }
   int upload_params();
+  // queues the shifts' copies to the host (and their accumulators in FP16/BF16
+  // modes) without waiting
+  int queue_download_shifts();
   int download_shifts();
 };
 
 namespace mf {
+// Queued forms of the coarse stages (mf_series.cu): *_enqueue queues one series'
+// work, its host results to the context's page-locked slot `slot`; *_finish reads
+// them after the stream has been synchronised and updates the series.
+struct TransformJob {
+  std::vector<int> img_idx;  // tilt of each measured pair
+  int np = 0;
+  float2* h_sh = nullptr;    // page-locked: measured binned shift of each pair
+};
+struct AxisSearch {
+  std::vector<float> cand;   // candidate axes
+  AxisJob job;
+};
+constexpr int kOffsetCount = 31;  // tilt-angle offsets -15..15 degrees (FindOffset.cu:103-110)
+struct OffsetJob {
+  std::vector<int> first;    // first pair of each offset
+  double* h_mom = nullptr;   // page-locked: 6 moments per (offset, pair)
+};
+int transform_enqueue(mf_series* s, int slot, TransformJob* job);
+int transform_finish(mf_series* s, TransformJob* job, float* max_err);
+int axis_enqueue(mf_series* s, float range, int num, int slot, AxisSearch* search);
+int axis_finish(mf_series* s, AxisSearch* search, float* axis_out, float* scores_out);
+int offset_enqueue(mf_series* s, int slot, OffsetJob* job);
+int offset_finish(mf_series* s, OffsetJob* job, float* offset_out);
+// Stage by stage over n series of one context, one wait per stage.
+int transform_many(mf_series* const* ser, int n);
+int tilt_axis_many(mf_series* const* ser, int n, float range, int num);
+int coarse_align_many(mf_series* const* ser, int n, float pitch_angle, float offset);
+
 int series_init(mf_series* s, mf_context* ctx, int nx, int ny, int nz, const float* file_angles);
 int transform_doit(mf_series* s, float* max_err);
 // scores_out (num floats, may be null): the score of every candidate

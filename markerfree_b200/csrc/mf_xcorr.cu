@@ -396,21 +396,53 @@ __device__ __forceinline__ void z_induced(float z0, float angle, float rot, floa
   rot_shift(a, 0.0f, rot, s0, s1);
 }
 
-// Final peak + ClacAlignProj update (ProjAlign.cpp:181-241) for held-out tilt ip.
-__global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int xb, int yb,
-                                 const float2* __restrict__ part, int nparts, int ip, int nx,
-                                 int ny, const float* __restrict__ angles, float* __restrict__ sx,
-                                 float* __restrict__ sy, const float* __restrict__ rot,
-                                 const float* __restrict__ z0p, float* __restrict__ err,
-                                 float* __restrict__ meas) {
-  float bv;
-  int bi;
-  reduce_partials(part, nparts, &bv, &bi);
-  if (threadIdx.x != 0) return;
-  int px = 0, py = 0;
-  pa_window_peak(bi, stride, xb, yb, &px, &py);
+// Rotation of a shift and the z-induced shift in FP64 (the forms below, for the
+// FP64 accumulation of the FP16/BF16 modes).
+__device__ __forceinline__ void rot_shift64(double in0, double in1, float angle_deg, double* o0,
+                                            double* o1) {
+  const double c = cos((double)angle_deg * kD2R), s = sin((double)angle_deg * kD2R);
+  *o0 = in0 * c - in1 * s;
+  *o1 = in0 * s + in1 * c;
+}
+__device__ __forceinline__ void z_induced64(float z0, float angle, float rot, double* s0,
+                                            double* s1) {
+  *s0 = 0.0;
+  *s1 = 0.0;
+  if (z0 == 0.0f) return;
+  rot_shift64(-(double)z0 * sin((double)angle * kD2R), 0.0, rot, s0, s1);
+}
+
+// ClacAlignProj (ProjAlign.cpp:181-241) for held-out tilt ip from the integer peak
+// (px, py) of the correlation map: sub-pixel fit, binned -> un-binned shift, the
+// measured shift printed by the reference, its rotation by the tilt axis plus the
+// z-induced shift added to the tilt's shift, and |shift| as the tilt's error.
+// With sx64 (FP16/BF16 modes) the update is formed from the FP64 fit in FP64 and
+// accumulated there, sx receiving the float value; otherwise every step is the
+// reference's float arithmetic.
+__device__ void pa_update(const float* map, int stride, int xb, int yb, int px, int py, int ip,
+                          int nx, int ny, const float* angles, float* sx, float* sy,
+                          double* sx64, double* sy64, const float* rot, float z0, float* err,
+                          float* meas) {
   double dx, dy, pk;
   pa_fit(map, stride, px, py, &dx, &dy, &pk);
+  const float r = rot[ip];
+  if (sx64 != nullptr) {
+    const double a0 = ((double)px + dx - (double)(xb / 2)) * ((double)nx / (double)xb);
+    const double a1 = ((double)py + dy - (double)(yb / 2)) * ((double)ny / (double)yb);
+    if (meas) {
+      meas[2 * ip] = (float)a0;
+      meas[2 * ip + 1] = (float)a1;
+    }
+    double b0, b1, i0, i1;
+    rot_shift64(a0, a1, r, &b0, &b1);
+    z_induced64(z0, angles[ip], r, &i0, &i1);
+    sx64[ip] += b0 + i0;
+    sy64[ip] += b1 + i1;
+    sx[ip] = (float)sx64[ip];
+    sy[ip] = (float)sy64[ip];
+    err[ip] = (float)sqrt(a0 * a0 + a1 * a1);
+    return;
+  }
   float pkx = (float)(px + dx), pky = (float)(py + dy);
   float shx = __fsub_rn(pkx, (float)(xb / 2));
   float shy = __fsub_rn(pky, (float)(yb / 2));
@@ -422,15 +454,32 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
     meas[2 * ip] = a0;
     meas[2 * ip + 1] = a1;
   }
-  float r = rot[ip];
   rot_shift(a0, a1, r, &a0, &a1);
   float i0, i1;
-  z_induced(*z0p, angles[ip], r, &i0, &i1);
+  z_induced(z0, angles[ip], r, &i0, &i1);
   a0 = __fadd_rn(a0, i0);
   a1 = __fadd_rn(a1, i1);
   sx[ip] = __fadd_rn(sx[ip], a0);
   sy[ip] = __fadd_rn(sy[ip], a1);
   err[ip] = fs;
+}
+
+// Final peak + ClacAlignProj update for held-out tilt ip.
+__global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int xb, int yb,
+                                 const float2* __restrict__ part, int nparts, int ip, int nx,
+                                 int ny, const float* __restrict__ angles, float* __restrict__ sx,
+                                 float* __restrict__ sy, double* __restrict__ sx64,
+                                 double* __restrict__ sy64, const float* __restrict__ rot,
+                                 const float* __restrict__ z0p, float* __restrict__ err,
+                                 float* __restrict__ meas) {
+  float bv;
+  int bi;
+  reduce_partials(part, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
+  int px = 0, py = 0;
+  pa_window_peak(bi, stride, xb, yb, &px, &py);
+  pa_update(map, stride, xb, yb, px, py, ip, nx, ny, angles, sx, sy, sx64, sy64, rot, *z0p, err,
+            meas);
 }
 
 // Group form: blockIdx.x = series b, map b at maps + b * map_stride, partials
@@ -452,26 +501,8 @@ __global__ void k_pa_peak_update_group(const float* __restrict__ maps, size_t ma
   const int ip = steps[b].ip;
   int px = 0, py = 0;
   pa_window_peak(bi, stride, xb, yb, &px, &py);
-  double dx, dy, pk;
-  pa_fit(map, stride, px, py, &dx, &dy, &pk);
-  float pkx = (float)(px + dx), pky = (float)(py + dy);
-  float shx = __fsub_rn(pkx, (float)(xb / 2));
-  float shy = __fsub_rn(pky, (float)(yb / 2));
-  float binx = __fdiv_rn((float)nx, (float)xb), biny = __fdiv_rn((float)ny, (float)yb);
-  float a0 = __fmul_rn(shx, binx), a1 = __fmul_rn(shy, biny);
-  float fs = __fadd_rn(__fmul_rn(a0, a0), __fmul_rn(a1, a1));
-  fs = sqrtf(fs);
-  S.meas[2 * ip] = a0;  // the shift the reference prints (ProjAlign.cpp:203)
-  S.meas[2 * ip + 1] = a1;
-  float r = S.rot[ip];
-  rot_shift(a0, a1, r, &a0, &a1);
-  float i0, i1;
-  z_induced(*S.z0, S.angles[ip], r, &i0, &i1);
-  a0 = __fadd_rn(a0, i0);
-  a1 = __fadd_rn(a1, i1);
-  S.sx[ip] = __fadd_rn(S.sx[ip], a0);
-  S.sy[ip] = __fadd_rn(S.sy[ip], a1);
-  S.err[ip] = fs;
+  pa_update(map, stride, xb, yb, px, py, ip, nx, ny, S.angles, S.sx, S.sy, S.sx64, S.sy64, S.rot,
+            *S.z0, S.err, S.meas);
 }
 
 int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,
@@ -493,8 +524,8 @@ int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int s
 
 int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
                    int ip, int nx, int ny, const float* d_angles, float* d_sx, float* d_sy,
-                   const float* d_rot, const float* d_z0, float* d_err, float* d_meas,
-                   cudaStream_t st) {
+                   double* d_sx64, double* d_sy64, const float* d_rot, const float* d_z0,
+                   float* d_err, float* d_meas, cudaStream_t st) {
   int sx = xb / 20, sy = yb / 20;
   if (sx < 3) sx = 3;
   if (sy < 3) sy = 3;
@@ -502,7 +533,7 @@ int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, flo
   const int nb = kPeakParts;
   k_peak_partial<<<dim3(nb, 1), 256, 0, st>>>(map, 0, stride, sx, ex, sy, ey, d_part);
   k_pa_peak_update<<<1, 32, 0, st>>>(map, stride, xb, yb, d_part, nb, ip, nx, ny, d_angles, d_sx,
-                                     d_sy, d_rot, d_z0, d_err, d_meas);
+                                     d_sy, d_sx64, d_sy64, d_rot, d_z0, d_err, d_meas);
   c->launches += 2;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -588,14 +619,16 @@ int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w
 
 // ---------------------------------------------------------------------------
 // FitRotCenterZ + RemoveOffsetZ(-1) (ProjAlign.cpp:459-501, 553-579); the
-// reference's uninitialised accumulator dA is taken as 0.
+// reference's uninitialised accumulator dA is taken as 0.  With sx64/sy64 (FP16/BF16
+// modes) the shifts are read from and the z-induced shifts removed in FP64.
 __device__ void fit_z0_one(int nz, int zt, const float* __restrict__ angles, float* sx,
-                           float* sy, const float* __restrict__ rot, float* z0p);
+                           float* sy, double* sx64, double* sy64, const float* __restrict__ rot,
+                           float* z0p);
 
 __global__ void k_fit_z0(int nz, int zt, const float* __restrict__ angles, float* sx, float* sy,
-                         const float* __restrict__ rot, float* z0p) {
+                         double* sx64, double* sy64, const float* __restrict__ rot, float* z0p) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  fit_z0_one(nz, zt, angles, sx, sy, rot, z0p);
+  fit_z0_one(nz, zt, angles, sx, sy, sx64, sy64, rot, z0p);
 }
 
 __global__ void k_fit_z0_group(const GroupSeriesDev* __restrict__ ser,
@@ -603,7 +636,7 @@ __global__ void k_fit_z0_group(const GroupSeriesDev* __restrict__ ser,
   const int b = blockIdx.x;
   if (threadIdx.x != 0 || (active && active[b] == 0)) return;
   const GroupSeriesDev& S = ser[b];
-  fit_z0_one(nz, S.zt, S.angles, S.sx, S.sy, S.rot, S.z0);
+  fit_z0_one(nz, S.zt, S.angles, S.sx, S.sy, S.sx64, S.sy64, S.rot, S.z0);
 }
 
 // max over err[order[i]] (the DoIt return value), initial -1e20, per series
@@ -636,7 +669,34 @@ int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int 
 }
 
 __device__ void fit_z0_one(int nz, int zt, const float* __restrict__ angles, float* sx,
-                           float* sy, const float* __restrict__ rot, float* z0p) {
+                           float* sy, double* sx64, double* sy64, const float* __restrict__ rot,
+                           float* z0p) {
+  if (sx64 != nullptr) {
+    double s0x, s0y;
+    rot_shift64(sx64[zt], sy64[zt], -rot[zt], &s0x, &s0y);
+    const double cent0 = s0x / cos((double)angles[zt] * kD2R);
+    double dA = 0.0, dB = 0.0;
+    for (int i = 0; i < nz; ++i) {
+      double r0, r1;
+      rot_shift64(sx64[i], sy64[i], -rot[i], &r0, &r1);
+      const double ds = sin((double)angles[i] * kD2R), dc = cos((double)angles[i] * kD2R);
+      dA += (cent0 * dc - r0) * ds;
+      dB += ds * ds;
+    }
+    const float z0 = (float)(dA / (dB + 1e-30));
+    *z0p = z0;
+    if (z0 == 0.0f) return;
+    for (int i = 0; i < nz; ++i) {
+      if (i == zt) continue;
+      double a, b;
+      z_induced64(z0, angles[i], rot[i], &a, &b);
+      sx64[i] -= a;
+      sy64[i] -= b;
+      sx[i] = (float)sx64[i];
+      sy[i] = (float)sy64[i];
+    }
+    return;
+  }
   float s0x, s0y;
   rot_shift(sx[zt], sy[zt], -rot[zt], &s0x, &s0y);
   float cent0 = (float)((double)s0x / cos((double)angles[zt] * kD2R));
@@ -661,8 +721,8 @@ __device__ void fit_z0_one(int nz, int zt, const float* __restrict__ angles, flo
 }
 
 int fit_z0(Context* c, int nz, int zt, const float* d_angles, float* d_sx, float* d_sy,
-           const float* d_rot, float* d_z0, cudaStream_t st) {
-  k_fit_z0<<<1, 32, 0, st>>>(nz, zt, d_angles, d_sx, d_sy, d_rot, d_z0);
+           double* d_sx64, double* d_sy64, const float* d_rot, float* d_z0, cudaStream_t st) {
+  k_fit_z0<<<1, 32, 0, st>>>(nz, zt, d_angles, d_sx, d_sy, d_sx64, d_sy64, d_rot, d_z0);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

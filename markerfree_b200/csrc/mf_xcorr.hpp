@@ -38,17 +38,19 @@ int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int 
 int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,
                  cufftComplex* img, size_t img_stride, int npairs, int cmp, int ny, float bfactor,
                  float scale, cudaStream_t st);
+// d_sx64/d_sy64 (FP16/BF16 modes; null in FP32 mode): FP64 accumulators of the
+// shifts, of which d_sx/d_sy receive the float values.
 int pa_peak_update(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
                    int ip, int nx, int ny, const float* d_angles, float* d_sx, float* d_sy,
-                   const float* d_rot, const float* d_z0, float* d_err, float* d_meas,
-                   cudaStream_t st);
+                   double* d_sx64, double* d_sy64, const float* d_rot, const float* d_z0,
+                   float* d_err, float* d_meas, cudaStream_t st);
 int pa_peak_only(Context* c, const float* map, int stride, int xb, int yb, float2* d_part,
                  float* d_out, cudaStream_t st);
 int cc_peaks(Context* c, const float* maps, size_t map_stride, int stride, int w, int h, int nmaps,
              float2* d_part, float2* d_shifts, cudaStream_t st);
 constexpr int kPeakParts = 256;  // partial blocks of the single-map peak search
 int fit_z0(Context* c, int nz, int zt, const float* d_angles, float* d_sx, float* d_sy,
-           const float* d_rot, float* d_z0, cudaStream_t st);
+           double* d_sx64, double* d_sy64, const float* d_rot, float* d_z0, cudaStream_t st);
 int max_err(Context* c, const float* d_err, const int* d_order, int n, float* d_out,
             cudaStream_t st);
 int stretch_many(Context* c, const float* src, size_t src_img_stride, const int* d_src_idx,
@@ -59,15 +61,30 @@ void stretch_matrix(float dstretch, float tilt_axis, float* m);
 int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
                       const float* file_angles, cudaStream_t st);
 
-// Common-line tilt-axis search over all tilts (Rotate.cu).  Scores (num floats)
-// are returned to the host; the caller applies the arg-max rule.
-struct AxisPlanCache;
+// Common-line tilt-axis search over all tilts (Rotate.cu), queued without a host
+// wait: tilt_axis_scores_enqueue launches every kernel of one search and copies the
+// candidates' scores into a page-locked slot of the context; once the stream has
+// been synchronised, tilt_axis_scores_finish returns them (num floats) and books
+// the Radon kernel's stage timing.  The caller applies the arg-max rule.
+struct AxisJob {
+  float* h_scores = nullptr;              // page-locked, num floats
+  unsigned long long* h_count = nullptr;  // page-locked, samples taken (stage timing)
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int num = 0, L = 0, nx = 0, ny = 0, nz = 0;
+  AxisJob() = default;
+  AxisJob(const AxisJob&) = delete;
+  AxisJob& operator=(const AxisJob&) = delete;
+  ~AxisJob();
+};
 // stack_t: the same stack column-major per tilt (transpose_stack); d_neg[z]: image
-// z holds a value below zero (null: assume it may).
-int tilt_axis_scores(Context* c, cufftHandle plan, const float* stack, const float* stack_t,
-                     const int* d_neg, int nx, int ny, int nz, const float* angles,
-                     const float* sx, const float* sy, int zt, const float* rot_cand, int num,
-                     int line_len, std::vector<float>* scores, cudaStream_t st);
+// z holds a value below zero (null: assume it may); slot: the context's pinned
+// slot the scores go to (unique among the searches queued before one wait).
+int tilt_axis_scores_enqueue(Context* c, cufftHandle plan, const float* stack,
+                             const float* stack_t, const int* d_neg, int nx, int ny, int nz,
+                             const float* angles, const float* sx, const float* sy, int zt,
+                             const float* rot_cand, int num, int line_len, int slot, AxisJob* job,
+                             cudaStream_t st);
+int tilt_axis_scores_finish(Context* c, AxisJob* job, std::vector<float>* scores);
 // d_c[i] = cosf(d_x[i]), d_s[i] = sinf(d_x[i]) on the device.
 int device_cos_sin(Context* ctx, const float* d_x, int n, float* d_c, float* d_s,
                    cudaStream_t st);

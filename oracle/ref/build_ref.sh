@@ -6,11 +6,12 @@
 # cuFFT, and given oracle/ref/mpi.h in place of an MPI installation.  The binary
 # is used to produce the reference's own outputs on synthetic inputs.
 #
-# usage: oracle/ref/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# usage: oracle/ref/build_ref.sh [REFERENCE_ROOT]
+# (default: $MF_REFERENCE_ROOT, else a checkout named `reference` beside this repository)
 set -euo pipefail
-REF=${1:-/root/reference}
-SRC="$REF/Markerfree/src"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF=${1:-${MF_REFERENCE_ROOT:-$HERE/../../../reference}}
+SRC="$REF/Markerfree/src"
 OUT="$HERE/../_ref"
 OBJ="$OUT/obj"
 mkdir -p "$OBJ"

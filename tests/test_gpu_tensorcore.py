@@ -214,3 +214,37 @@ def test_pass_shift_errors_against_fp64_oracle(ctx, mflib, prec):
                     float(np.abs(g.shift_y - po.shift_y).max()))
     print(f"precision {prec}: largest per-tilt shift error against FP64 {worst:.4f} px")
     assert worst < SHIFT_TOL_MIXED, worst
+
+
+@pytest.mark.parametrize("prec", [0, 2, 1])
+def test_tilt_axis_error_against_fp64_oracle(ctx, mflib, prec):
+    """The tilt axis, in degrees, that each precision (mf_precision 0 = FP32, 2 = FP16,
+    1 = BF16 operands) finds after two projection-matching passes (the 20-degree
+    refinement of Process::mProjAlign, Process.cpp:283-296), against the oracle
+    whose re-projection accumulates in FP64 and whose search sees the FP64 path's
+    shifts: within 0.01 degrees, and stated."""
+    s0 = synth.make_series(nx=192, ny=192, vol_z=48, n_blobs=90, tilt_min=-45, tilt_max=45,
+                           tilt_step=3.0, axis=87.0, shift_sd=3.0, snr=4.0, seed=21,
+                           thickness=40)
+    nz = s0.stack.shape[0]
+    st = O.preprocess(s0.stack, s0.angles)
+    s = mflib.Series(ctx, s0.stack, s0.angles)
+    s.set_precision(prec)
+    p = mflib.Param(nz)
+    p.rotate[:] = 86.0
+    s.set_param(p)
+    po = O.Param(nz)
+    po.rotate[:] = 86.0
+    pa = O.ProjAlign(st, s0.angles, po, 0.0, 40, 10)
+    pa.set_f64(True)
+    s.projalign_setup(0.0, 40, 10)
+    for _ in range(2):
+        pa.doit()
+        s.projalign_doit()
+    ax_o, sc_o = O.tilt_axis_scores(st, s0.angles, po, 20.0)
+    ax_g = s.tilt_axis(20.0)
+    top = np.sort(sc_o)[-2:]
+    err = abs(ax_g - ax_o)
+    print(f"precision {prec}: tilt axis {ax_g:.4f} against FP64 {ax_o:.4f}: error {err:.4f} deg "
+          f"(oracle's best two candidate scores {top[1]:.6f}, {top[0]:.6f})")
+    assert err <= 0.01, err
