@@ -617,7 +617,8 @@ def run_kernel_case(args):
     """One stage of the workload on its own, for profilers (ncu -k ...): `reproject`
     re-projects one held-out tilt (full size, 10 neighbours) with the banded
     operator; `xcorr` measures one cross-correlation shift; `axis` runs one
-    tilt-axis search (100 candidates over 20 degrees)."""
+    tilt-axis search (100 candidates over 20 degrees); `pass` runs projection-
+    matching passes of a group of --batch series in --precision."""
     import torch
     import markerfree_b200 as mf
     s = make_batch(1, "cuda:0", args.scale)[0]
@@ -633,6 +634,24 @@ def run_kernel_case(args):
     g = torch.Generator(device="cuda").manual_seed(7)
     corr = torch.randn((nz, ny, nx), generator=g, device="cuda", dtype=torch.float32)
     out = torch.empty((ny, nx), device="cuda", dtype=torch.float32)
+    if args.kernel_case == "pass":
+        # one projection-matching pass of a group of --batch series (every pass kernel)
+        batch = make_batch(args.batch, "cuda:0", args.scale)
+        sers = []
+        for b in batch:
+            ser = mf.Series(ctx, b.stack.cpu().numpy(), b.angles)
+            ser.set_precision(PRECISIONS[args.precision])
+            p = ser.get_param()
+            p.rotate[:] = b.axis
+            ser.set_param(p)
+            sers.append(ser)
+        grp = mf.Group(sers, 0.0, batch[0].thickness, 10)
+        for _ in range(args.steps):
+            grp.doit()
+        ctx.sync()
+        grp.close()
+        print(json.dumps({"kernel_case": "pass", "series": len(sers), "tilts": nz}))
+        return 0
     if args.kernel_case == "axis":
         ser = mf.Series(ctx, s.stack, ang)
         p = ser.get_param()
@@ -656,7 +675,7 @@ def run_kernel_case(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr", "axis"],
+    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr", "axis", "pass"],
                     help="run one stage alone (profiling)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)

@@ -105,6 +105,14 @@ MF_API int mf_series_create(mf_context* ctx, const float* raw_stack, int nx, int
 /* Same, from a device buffer already holding the raw stack (file order). */
 MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw_stack, int nx, int ny,
                                    int nz, const float* file_angles, mf_series** out);
+/* A stack that PreProcess has already treated (Markerfree/src/method/Preprocess.cu:
+ * 103-177, the contents of the reference's buf.mrc that Process::mCoarseAlign and
+ * mProjAlign read, Process.cpp:161-236): ascending angle order, made positive and
+ * mass-normalised.  It is uploaded as it is, with `angles` in the same (ascending)
+ * order; no pre-processing runs, so a caller that has run the reference's own
+ * pre-processing hands over exactly the stack its later stages would read. */
+MF_API int mf_series_create_preprocessed(mf_context* ctx, const float* stack, int nx, int ny,
+                                         int nz, const float* angles, mf_series** out);
 /* Destroy every series of a context before the context itself. */
 MF_API void mf_series_destroy(mf_series* s);
 /* Takes effect at the next mf_projalign_setup (a set-up pass of another

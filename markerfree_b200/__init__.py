@@ -65,6 +65,9 @@ SIGNATURES = [
     ("mf_series_create_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                                ctypes.c_int, ctypes.c_int, _f32p,
                                                ctypes.POINTER(ctypes.c_void_p)]),
+    ("mf_series_create_preprocessed", ctypes.c_int, [ctypes.c_void_p, _f32p, ctypes.c_int,
+                                                     ctypes.c_int, ctypes.c_int, _f32p,
+                                                     ctypes.POINTER(ctypes.c_void_p)]),
     ("mf_series_destroy", None, [ctypes.c_void_p]),
     ("mf_series_set_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mf_series_get_stack", ctypes.c_int, [ctypes.c_void_p, _f32p]),
@@ -283,15 +286,18 @@ class Context:
 class Series:
     """A pre-processed tilt series kept in HBM (replaces buf.mrc)."""
 
-    def __init__(self, ctx: Context, raw_stack, file_angles):
+    def __init__(self, ctx: Context, raw_stack, file_angles, preprocessed=False):
+        """raw_stack in file order (pre-processed on the GPU), or with
+        preprocessed=True a stack the reference's PreProcess already treated, in
+        ascending angle order (mf_series_create_preprocessed)."""
         import weakref
         raw = _f32(raw_stack)
         self.nz, self.ny, self.nx = raw.shape
         self.ctx = ctx
         self.file_angles = _f32(file_angles)[: self.nz]
         h = ctypes.c_void_p()
-        _check(lib().mf_series_create(ctx.h, raw, self.nx, self.ny, self.nz, self.file_angles,
-                                      ctypes.byref(h)))
+        create = lib().mf_series_create_preprocessed if preprocessed else lib().mf_series_create
+        _check(create(ctx.h, raw, self.nx, self.ny, self.nz, self.file_angles, ctypes.byref(h)))
         self.h = h
         if not hasattr(ctx, "_series"):
             ctx._series = weakref.WeakSet()

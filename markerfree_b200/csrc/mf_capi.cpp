@@ -150,7 +150,8 @@ MF_API int mf_context_tc_tuning(mf_context* ctx, double* out, int max_rows, int*
 
 // ---------------------------------------------------------------------------
 static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_device, int nx,
-                                int ny, int nz, const float* file_angles, mf_series** out) {
+                                int ny, int nz, const float* file_angles, mf_series** out,
+                                bool preprocess = true) {
   if (!out) return set_error(MF_ERR_ARG, "null output pointer");
   *out = nullptr;
   MF_TRY(use_device(ctx));
@@ -164,7 +165,7 @@ static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_d
   if (rc == MF_OK) rc = s->stack.alloc(sizeof(float) * pix * nz);
   if (rc == MF_OK) {
     // SetPositive writes slice a to index nz-1-a when the angles descend
-    bool rev = file_angles[0] > file_angles[1];
+    bool rev = preprocess && file_angles[0] > file_angles[1];
     cudaStream_t st = ctx->c.stream;
     for (int a = 0; a < nz && rc == MF_OK; ++a) {
       int i = rev ? nz - 1 - a : a;
@@ -175,7 +176,7 @@ static int series_create_common(mf_context* ctx, const float* raw, bool raw_on_d
       if (e != cudaSuccess) rc = set_error(MF_ERR_CUDA, "stack upload: %s", cudaGetErrorString(e));
     }
   }
-  if (rc == MF_OK)
+  if (rc == MF_OK && preprocess)
     rc = preprocess_device(&ctx->c, s->stack.as<float>(), nx, ny, nz, file_angles, ctx->c.stream);
   // the column-major copy read by the resampling and the tilt-axis search
   if (rc == MF_OK) rc = s->stack_t.alloc(sizeof(float) * pix * nz);
@@ -202,6 +203,18 @@ MF_API int mf_series_create_device(mf_context* ctx, const float* d_raw, int nx, 
                                    const float* file_angles, mf_series** out) {
   MF_GUARD_BEGIN
   return series_create_common(ctx, d_raw, true, nx, ny, nz, file_angles, out);
+  MF_GUARD_END
+}
+
+MF_API int mf_series_create_preprocessed(mf_context* ctx, const float* stack, int nx, int ny,
+                                         int nz, const float* angles, mf_series** out) {
+  MF_GUARD_BEGIN
+  if (angles)
+    for (int z = 1; z < nz; ++z)
+      if (!(angles[z] > angles[z - 1]))
+        return set_error(MF_ERR_ARG, "a pre-processed stack is in ascending angle order "
+                                     "(angle %d is %.2f after %.2f)", z, angles[z], angles[z - 1]);
+  return series_create_common(ctx, stack, false, nx, ny, nz, angles, out, false);
   MF_GUARD_END
 }
 

@@ -46,6 +46,10 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "Markerfree")
 # A case name ending in "_p<k>" runs the base case with its stack multiplied by
 # 1 + 1e-6 * U(-1, 1) (seed k): the spread of the reference's own results over
 # such perturbations bounds how closely any other implementation can follow it.
+# A name ending in "_s1" runs the base case with -s 1, so the reference writes its
+# parameters as an IMOD .xf file (SaveParam.cpp:15-120) instead of the .txt.
+# "cfg2" is the realistic single-series configuration (synth.config(2): 2048^2 x 61
+# tilts, T = 300, SNR 0.05), generated by the config function rather than kwargs.
 CASES = {
     # name: (generator kwargs, thickness, nproj, timeout s)
     "c1s256": (dict(nx=256, ny=256, vol_z=64, n_blobs=80, seed=1101, snr=0.5,
@@ -58,14 +62,29 @@ CASES = {
     # a well-conditioned series: high SNR, the alignment settles in few passes
     "hi384": (dict(nx=384, ny=384, vol_z=96, n_blobs=160, seed=1201, snr=4.0, shift_sd=3.0,
                    axis=87.0), 80, 10, 1200),
+    "cfg2": (dict(config=2), 300, 10, 1800),
+    # wide enough that the reference bins the projection matching by 2
+    # (ProjAlign.cpp:57-61: round(3072 / 2048) = 2; slab 100 / 2 = 50)
+    "bin2": (dict(nx=3072, ny=320, vol_z=64, n_blobs=240, seed=1301, snr=4.0, shift_sd=3.0,
+                  axis=87.0, tilt_min=-40, tilt_max=40, tilt_step=4.0), 100, 10, 1200),
 }
 
 
 def case_spec(name):
-    """(generator kwargs, thickness, nproj, timeout, perturbation seed or None)."""
+    """(generator kwargs, thickness, nproj, timeout, perturbation seed or None, save mode)."""
+    save = 0
+    if name.endswith("_s1"):
+        name, save = name[:-3], 1
     base, _, tag = name.partition("_p")
     kw, thick, nproj, tmo = CASES[base]
-    return kw, thick, nproj, tmo, (int(tag) if tag else None)
+    return kw, thick, nproj, tmo, (int(tag) if tag else None), save
+
+
+def make_case_series(kw, thick, nproj):
+    """The case's series: synth.config(n) for {"config": n}, else make_series(**kw)."""
+    if "config" in kw:
+        return synth.config(kw["config"])
+    return synth.make_series(thickness=thick, nproj=nproj, **kw)
 
 
 def perturbed(stack, seed):
@@ -103,8 +122,8 @@ def read_mrc_float(path):
 
 
 def run_case(outdir, name):
-    kw, thick, nproj, tmo, pert = case_spec(name)
-    s = synth.make_series(thickness=thick, nproj=nproj, **kw)
+    kw, thick, nproj, tmo, pert, save = case_spec(name)
+    s = make_case_series(kw, thick, nproj)
     d = os.path.join(outdir, name)
     os.makedirs(d, exist_ok=True)
     mrc = os.path.join(d, "in.mrc")
@@ -115,7 +134,7 @@ def run_case(outdir, name):
             fh.write(f"{a:.2f}\n")
     out = os.path.join(d, "out.mrc")
     cmd = [REF_BIN, "-i", mrc, "-o", out, "-a", tlt, "-g", f"0.0001,0,0,0,{thick},1,0",
-           "-p", str(nproj), "-s", "0"]
+           "-p", str(nproj), "-s", str(save)]
     t0 = time.time()
     with open(os.path.join(d, "ref.log"), "w") as log:
         rc = subprocess.call(cmd, stdout=log, stderr=subprocess.STDOUT, timeout=tmo)
@@ -128,12 +147,16 @@ def run_case(outdir, name):
                             slice_sum=al.astype(np.float64).sum((1, 2)),
                             slice_sq=(al.astype(np.float64) ** 2).sum((1, 2)),
                             crop=al[mid, cy - 32:cy + 32, cx - 32:cx + 32].copy())
-        os.rename(os.path.join(d, "out.txt"), os.path.join(d, "ref.txt"))
+        if save == 1:
+            os.rename(os.path.join(d, "out.xf"), os.path.join(d, "ref.xf"))
+        else:
+            os.rename(os.path.join(d, "out.txt"), os.path.join(d, "ref.txt"))
         os.remove(out)
     os.remove(mrc)
     with open(os.path.join(d, "case.json"), "w") as fh:
         json.dump({"generator": kw, "thickness": thick, "nproj": nproj, "cmd": cmd[1:],
-                   "rc": rc, "wall_s": wall, "perturbation_seed": pert}, fh, indent=1)
+                   "rc": rc, "wall_s": wall, "perturbation_seed": pert, "save_mode": save},
+                  fh, indent=1)
     print(name, "rc", rc, "wall", round(wall, 2), flush=True)
     return rc
 
@@ -184,17 +207,20 @@ def write_fixtures(outdir, name):
     with open(os.path.join(d, "ref.log"), errors="replace") as fh:
         events = parse_log(fh.read())
     al = np.load(os.path.join(d, "aligned.npz"))
+    xf = case.get("save_mode", 0) == 1
     fx = {"case": name, "generator": case["generator"], "thickness": case["thickness"],
           "nproj": case["nproj"], "cmd": case["cmd"],
           "perturbation_seed": case.get("perturbation_seed"), "wall_s": case.get("wall_s"),
+          "save_mode": case.get("save_mode", 0),
           "events": events,
-          "params": parse_txt(os.path.join(d, "ref.txt")),
+          "params": [] if xf else parse_txt(os.path.join(d, "ref.txt")),
           "aligned_slice_sum": al["slice_sum"].tolist(),
           "aligned_slice_sq": al["slice_sq"].tolist()}
     with open(os.path.join(HERE, f"ref_{name}.json"), "w") as fh:
         json.dump(fx, fh)
-    with open(os.path.join(d, "ref.txt")) as src, open(os.path.join(HERE, f"ref_{name}.txt"),
-                                                       "w") as dst:
+    ext = "xf" if xf else "txt"
+    with open(os.path.join(d, f"ref.{ext}")) as src, \
+            open(os.path.join(HERE, f"ref_{name}.{ext}"), "w") as dst:
         dst.write(src.read())
     np.save(os.path.join(HERE, f"ref_{name}_crop.npy"), al["crop"])
     print(name, len(events), "events", flush=True)

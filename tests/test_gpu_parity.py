@@ -280,3 +280,24 @@ def test_errors_are_reported_not_faulted(ctx, mflib, series):
     with pytest.raises(mflib.MfError) as ei:
         s3.projalign_setup(0.0, 16, 10)
     assert ei.value.code == -8
+
+
+def test_preprocessed_stack_entry_point(ctx, mflib, series):
+    """mf_series_create_preprocessed takes the stack the reference's PreProcess wrote
+    (buf.mrc) as it is: handed the library's own pre-processed stack, it holds the
+    same values and a projection-matching pass gives the same parameters."""
+    nz = series.stack.shape[0]
+    a = mflib.Series(ctx, series.stack, series.angles)
+    st = a.stack()
+    b = mflib.Series(ctx, st, np.sort(series.angles), preprocessed=True)
+    assert np.array_equal(b.stack(), st)
+    for s in (a, b):
+        p = mflib.Param(nz)
+        p.rotate[:] = 86.0
+        s.set_param(p)
+        s.projalign_setup(0.0, 30, 10)
+    assert a.projalign_doit() == b.projalign_doit()
+    pa, pb = a.get_param(), b.get_param()
+    assert np.array_equal(pa.shift_x, pb.shift_x) and np.array_equal(pa.shift_y, pb.shift_y)
+    with pytest.raises(mflib.MfError):
+        mflib.Series(ctx, st, np.sort(series.angles)[::-1].copy(), preprocessed=True)

@@ -41,10 +41,17 @@ SHIFT_TOL = 0.05  # px
 PRINT_TOL = 0.0051 + 0.005  # values printed with 2 decimals, plus float noise
 
 
+def case_series(g):
+    """The series a fixture's run was generated from (make_reference_golden's cases)."""
+    if "config" in g["generator"]:
+        return synth.config(g["generator"]["config"])
+    return synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+
+
 def load(name):
     with open(os.path.join(GOLD, f"ref_{name}.json")) as f:
         g = json.load(f)
-    s = synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+    s = case_series(g)
     angles = np.array([float(f"{a:.2f}") for a in s.angles], np.float32)
     return g, s, angles
 
@@ -197,7 +204,7 @@ def test_aligned_stack_matches_reference_output(ctx, mflib, run):
     from test_oracle_golden import determined_pixels
     with open(os.path.join(GOLD, f"ref_{run}.json")) as f:
         g = json.load(f)
-    s = synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+    s = case_series(g)
     angles = np.array([float(f"{a:.2f}") for a in s.angles], np.float32)
     seed = g.get("perturbation_seed")
     raw = s.stack if seed is None else perturbed(s.stack, seed)
@@ -222,3 +229,48 @@ def test_aligned_stack_matches_reference_output(ctx, mflib, run):
     sums = al.astype(np.float64).sum((1, 2))
     ref_sums = np.array(g["aligned_slice_sum"])
     assert float(np.abs(sums - ref_sums).max() / np.abs(ref_sums).max()) < 2e-4
+
+
+def test_cli_matches_reference_parameter_file(mflib, tmp_path):
+    """The drop-in program, run with the reference's command line on the input the
+    reference was given (hi384, -g 0.0001,0,0,0,80,1,0 -p 10 -s 0; Process.cpp:34-92,
+    SaveParam.cpp:185-262): its .txt has the reference's layout line for line, and
+    every row's axis and shifts agree with one of the reference's runs within
+    max(0.01 deg, their axis spread) and max(0.05 px, their shift spread)."""
+    import subprocess
+    import sys as _sys
+    _sys.path.insert(0, GOLD)
+    from make_reference_golden import parse_txt, write_mrc
+    g, s, angles = load("hi384")
+    runs = reference_runs("hi384")
+    mrc = str(tmp_path / "in.mrc")
+    tlt = str(tmp_path / "in.rawtlt")
+    out = str(tmp_path / "out.mrc")
+    write_mrc(mrc, s.stack)
+    with open(tlt, "w") as fh:
+        for a in s.angles:
+            fh.write(f"{a:.2f}\n")
+    cli = os.path.join(os.path.dirname(HERE), "markerfree_b200", "_build", "Markerfree")
+    r = subprocess.run([cli, "-i", mrc, "-o", out, "-a", tlt, "-g",
+                        f"0.0001,0,0,0,{g['thickness']},1,0", "-p", str(g["nproj"]), "-s", "0"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    mine = open(str(tmp_path / "out.txt")).read().splitlines()
+    ref = open(os.path.join(GOLD, "ref_hi384.txt")).read().splitlines()
+    assert len(mine) == len(ref)
+    for a, b in zip(mine, ref):
+        if a.startswith("Elapsed time"):
+            assert b.startswith("Elapsed time")
+        elif a.startswith("#") or ":" in a:
+            assert a == b
+    rows = np.array(parse_txt(str(tmp_path / "out.txt")), np.float64)
+    assert np.array_equal(rows[:, 0], runs[0][:, 0]) and np.allclose(rows[:, 4], runs[0][:, 4])
+    ax_spread = max(abs(a[0, 1] - b[0, 1]) for a, b in itertools.combinations(runs, 2))
+    sh_spread = max(np.abs(a[:, 2:4] - b[:, 2:4]).max() for a, b in itertools.combinations(runs, 2))
+    score = min(max(np.abs(rows[:, 1] - r[:, 1]).max() / max(AXIS_TOL, ax_spread),
+                    np.abs(rows[:, 2:4] - r[:, 2:4]).max() / max(SHIFT_TOL, sh_spread))
+                for r in runs)
+    assert score <= 1.0, score
+    # the aligned stack it wrote: float32 MRC of the input's size
+    nx, ny, nz, mode = mflib.mrc_info(out)
+    assert (nx, ny, nz, mode) == (s.stack.shape[2], s.stack.shape[1], s.stack.shape[0], 2)

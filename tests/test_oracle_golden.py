@@ -25,10 +25,17 @@ GOLD = os.path.join(HERE, "golden")
 PRINT_TOL = 0.0051 + 0.005
 
 
+def case_series(g):
+    """The series a fixture's run was generated from (make_reference_golden's cases)."""
+    if "config" in g["generator"]:
+        return synth.config(g["generator"]["config"])
+    return synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+
+
 def load(name):
     with open(os.path.join(GOLD, f"ref_{name}.json")) as f:
         g = json.load(f)
-    s = synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+    s = case_series(g)
     angles = np.array([float(f"{a:.2f}") for a in s.angles], np.float32)
     return g, s, angles
 
@@ -239,7 +246,7 @@ def run_input(g):
     import sys as _sys
     _sys.path.insert(0, GOLD)
     from make_reference_golden import perturbed
-    s = synth.make_series(thickness=g["thickness"], nproj=g["nproj"], **g["generator"])
+    s = case_series(g)
     angles = np.array([float(f"{a:.2f}") for a in s.angles], np.float32)
     seed = g.get("perturbation_seed")
     return (s.stack if seed is None else perturbed(s.stack, seed)), angles
