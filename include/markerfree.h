@@ -229,10 +229,11 @@ MF_API int mf_context_tc_tuning(mf_context* ctx, double* out, int max_rows, int*
 /* ---- groups: many series in lockstep ---------------------------------------
  * Not in the reference, which aligns one series per process.  A group runs the
  * projection-matching pass (ProjAlign::DoIt, Markerfree/src/method/ProjAlign.cpp:
- * 127-179) of up to 32 series of one context, shape and precision together: each
- * stage of the pass is one launch over all of them.
- * Per-series results equal those of aligning each series alone.  Destroy a group
- * before its series. */
+ * 127-179) of up to 32 series of one context and precision together: each stage
+ * of the pass is one launch over all of them.  The series may differ in image
+ * size, tilt count and binning; a series with fewer tilts has no work in the last
+ * steps of a pass.  Per-series results equal those of aligning each series alone.
+ * Destroy a group before its series. */
 typedef struct mf_group mf_group;
 /* ProjAlign::Setup for every series (their current angles and parameters). */
 MF_API int mf_group_create(mf_series* const* series, int n, float zshift, int align_z, int nproj,
@@ -253,15 +254,33 @@ MF_API int mf_group_z0(mf_group* g, float* z0);
 MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_raw, int nx, int ny,
                                 int nz, const float* const* file_angles, const mf_options* opt,
                                 mf_align_param* params, float* const* d_out, int* passes);
+/* One series of a batch: raw stack (file order) and aligned output in device
+ * memory, its size, its angles as read (host), its slab thickness. */
+typedef struct {
+  const float* d_raw;        /* nz x ny x nx floats */
+  int nx, ny, nz;
+  const float* file_angles;  /* nz angles, host memory */
+  int align_z;               /* -g A of this series; 0 = the options' align_z */
+  float* d_out;              /* aligned stack (nz x ny/out_bin x nx/out_bin), or NULL */
+} mf_series_desc;
+/* Process::DoIt minus file I/O (Markerfree/src/main/Process.cpp:34-92) for n
+ * series of any sizes, tilt counts and slab thicknesses: each series is
+ * pre-processed, coarse-aligned stage by stage with the others of its group of up
+ * to 32, projection-matched with them in one lockstep group, and corrected into
+ * its d_out.  params[i] must hold nz_i-entry arrays; passes (optional) gets each
+ * series' pass count. */
+MF_API int mf_align_batch_device(mf_context* ctx, int n, const mf_series_desc* series,
+                                 const mf_options* opt, mf_align_param* params, int* passes);
 
 /* ---- serving: continuous batching of requests ------------------------------
  * Not in the reference.  A server keeps `workers` streams busy with requests
  * (tilt series) that arrive at any time: a request is admitted when its
  * estimated device memory fits in `hbm_budget` bytes (0 = 80% of the free
  * memory), prepared on its own (upload, pre-processing, coarse alignment), then
- * projection-matched in a group with other prepared requests of its shape (up to
- * `max_group`).  A worker runs a full group first, then prepares admitted
- * requests (so that same-shape requests join the ready groups), then runs a group
+ * projection-matched in a group with other prepared requests of any shape that
+ * share its precision, -p and z shift (up to `max_group`).  A worker runs a full
+ * group first, then prepares admitted requests (so that more requests join the
+ * ready groups), then runs a group
  * whose oldest request has waited `group_wait_ms` or has no companion on the way;
  * no request waits longer than 20 x `group_wait_ms` once prepared.  A request's
  * result equals the one it gets when aligned alone. */

@@ -44,6 +44,12 @@ class AlignParamC(ctypes.Structure):
                 ("angle_offset", ctypes.c_float)]
 
 
+class SeriesDescC(ctypes.Structure):
+    _fields_ = [("d_raw", ctypes.c_void_p), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("file_angles", ctypes.c_void_p), ("align_z", ctypes.c_int),
+                ("d_out", ctypes.c_void_p)]
+
+
 class OptionsC(ctypes.Structure):
     _fields_ = [("offset", ctypes.c_float), ("pitch_angle", ctypes.c_float),
                 ("zshift", ctypes.c_float), ("thickness", ctypes.c_int),
@@ -116,6 +122,9 @@ SIGNATURES = [
     ("mf_group_doit", ctypes.c_int, [ctypes.c_void_p, _i32p, _f32p]),
     ("mf_group_proj_align", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("mf_group_z0", ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    ("mf_align_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.POINTER(SeriesDescC), ctypes.POINTER(OptionsC),
+                                             ctypes.POINTER(AlignParamC), ctypes.c_void_p]),
     ("mf_align_many_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int,
@@ -523,6 +532,33 @@ def align_many_device(ctx: Context, d_raws, nx, ny, nz, file_angles, d_outs=None
     passes = np.zeros(n, np.int32)
     _check(lib().mf_align_many_device(ctx.h, n, raws, nx, ny, nz, angp, ctypes.byref(o), cs, outs,
                                       passes.ctypes.data_as(ctypes.c_void_p)))
+    for p, c in zip(params, cs):
+        p.angle_offset = c.angle_offset
+    return params, passes
+
+
+def align_batch_device(ctx: Context, d_raws, file_angles, align_z, d_outs=None, offset=0.0,
+                       pitch_angle=0.0, zshift=0.0, out_bin=1, nproj=10, precision=PREC_FP32):
+    """mf_align_batch_device: n raw stacks (device tensors, shapes (nz, ny, nx) that
+    may differ), per-series angles and slab thicknesses (a sequence, or one value
+    for all).  Returns (list of Param, passes array)."""
+    n = len(d_raws)
+    if not hasattr(align_z, "__len__"):
+        align_z = [align_z] * n
+    angs = [_f32(a)[:d.shape[0]].copy() for a, d in zip(file_angles, d_raws)]
+    descs = (SeriesDescC * n)()
+    for i, d in enumerate(d_raws):
+        nz, ny, nx = d.shape
+        descs[i] = SeriesDescC(_ptr(d).value, nx, ny, nz, angs[i].ctypes.data, int(align_z[i]),
+                               _ptr(d_outs[i]).value if d_outs is not None else None)
+    params = [Param(d.shape[0]) for d in d_raws]
+    cs = (AlignParamC * n)(*[p.c() for p in params])
+    # the options' align_z only switches alignment on; each series has its own
+    o = OptionsC(offset, pitch_angle, zshift, 0, int(max(align_z)), out_bin, 0, nproj, 0,
+                 precision)
+    passes = np.zeros(n, np.int32)
+    _check(lib().mf_align_batch_device(ctx.h, n, descs, ctypes.byref(o), cs,
+                                       passes.ctypes.data_as(ctypes.c_void_p)))
     for p, c in zip(params, cs):
         p.angle_offset = c.angle_offset
     return params, passes

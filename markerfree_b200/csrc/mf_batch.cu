@@ -4,114 +4,150 @@
 // Markerfree/src/main/Process.cpp:272-319 (mProjAlign, ProjAlignOnce), which align
 // one series at a time.  Within a pass the held-out tilts of one series are
 // sequential, so one series cannot fill a B200; series, however, are
-// independent.  A group takes up to kMaxGroup series of the same shape and
-// precision and runs the i-th held-out tilt of every series together: each stage
-// of the pass (correction, R-weight FFTs, re-projection, normalisation,
-// cross-correlation FFTs, filter, peak and parameter update, re-correction) is
-// one launch over the whole group.  A per-series `active` flag in device memory
-// lets the same launches serve every iteration of ProjAlignOnce even though each
-// series leaves that loop after its own number of passes (the pass can also be
-// captured once into a CUDA graph; `use_graph` below says why it is not by
-// default).  Results per series are the same as when the series is
-// aligned alone: the per-series arithmetic and its order are unchanged.
+// independent.  A group takes up to kMaxGroup series of one precision -- of any
+// image size, tilt count and slab thickness -- and runs the k-th held-out tilt of
+// every series together: each stage of the pass (correction, R-weight,
+// re-projection, normalisation, filter, peak and parameter update,
+// re-correction) is one launch over the whole group, every kernel reading its
+// series' geometry and buffers from the series' GroupSeriesDev record.  cuFFT
+// runs per series with the plan shapes of that series aligned alone.  A series
+// with fewer tilts has no work in the last steps of a pass, and a per-series
+// `active` flag lets each series leave ProjAlignOnce after its own number of
+// passes.  Results per series are the same as when the series is aligned alone:
+// the per-series arithmetic and its order are unchanged.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <memory>
 
 #include "mf_series.hpp"
 #include "mf_xcorr.hpp"
 
 using namespace mf;
 
+namespace {
+
+// Host-side state of one series of a group: its geometry, its work buffers of the
+// pass and its cuFFT plans.
+struct GroupMember {
+  int nx = 0, ny = 0, nz = 0, n = 0, zt = 0;
+  int bin = 1, xb = 0, yb = 0, pad = 0, cmp = 0, thick = 0, ytiles = 0, xpitch = 0;
+  int out_x = 0, binx = 1, biny = 1;
+  size_t bpix = 0, ppix = 0;
+  DevBuf corr, scratch, reproj, cc, recorr, recorr_out, mpart, stats, ppart, corr16, tflags;
+  const float* mask = nullptr;
+  TmaDesc imgmap;
+  std::vector<int> order;
+  int op0 = 0;  // index of this series' first operator in the group's operator set
+  cufftHandle rows_fwd_all = 0, rows_inv_all = 0, rows_fwd_one = 0, rows_inv_one = 0;
+  cufftHandle cc_fwd = 0, cc_inv = 0;
+};
+
+}  // namespace
+
 struct mf_group {
   mf_context* ctx = nullptr;
   std::vector<mf_series*> ser;
-  int B = 0, nx = 0, ny = 0, nz = 0, n = 0;
-  int bin = 1, xb = 0, yb = 0, pad = 0, cmp = 0, thick = 0, nproj = 10, prec = MF_PREC_FP32;
-  int ytiles = 0, xpitch = 0, tc_nb = 256;
-  size_t bpix = 0, ppix = 0;
-  std::vector<std::vector<int>> order;
+  int B = 0, prec = MF_PREC_FP32, nproj = 10;
+  int nmax = 0;  // steps of a pass: the most held-out tilts of any series
+  int nz_max = 0, xb_max = 0, yb_max = 0, pad_max = 0, cmp_max = 0, ytiles_max = 0;
+  int ntiles_max = 0, rows_max = 0, tc_nb = 256;
+  std::vector<std::unique_ptr<GroupMember>> m;
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> masks;  // per (xb, yb)
   std::vector<int> active;
   std::vector<float> z0;
   // device tables
-  DevBuf d_ser, d_steps, d_active, d_order, d_bp, d_normptr, d_applyjobs, d_tiltidx;
-  DevBuf d_maxerr, d_z0, d_err, d_meas, d_tcerr;
-  // device buffers (series-major, contiguous over the group)
-  DevBuf corr, scratch, corr16, tflags, rowflags, reproj, cc, recorr, recorr_out;
-  DevBuf mpart, stats, ppart, mask;
+  DevBuf d_ser, d_steps, d_active, d_bp, d_applyjobs, d_maxerr, d_z0, d_err, d_meas, d_tcerr;
+  DevBuf d_order, rowflags;
   ReprojOpSet ops;
   TcOpSet tcops;
-  TmaDesc imgmap;
-  std::vector<TcJob> tcjobs;  // [n][B]
-  cufftHandle rows_fwd_all = 0, rows_inv_all = 0, rows_fwd_one = 0, rows_inv_one = 0;
-  cufftHandle cc_fwd = 0, cc_inv = 0;
-  cudaGraphExec_t graph = nullptr;
-  int64_t graph_kernels = 0;
-  // Group passes launch eagerly: capturing and instantiating the graph of a group
-  // pass (thousands of nodes, 8 series) cost more than its six replays saved
-  // (bench step 2058 ms with the graph, 1564 ms without).
-  bool use_graph = false;
-  std::vector<cudaEvent_t> events;  // 3 per step when the context profiles
+  std::vector<TmaDesc> maps;               // per series
+  std::vector<std::vector<TcJob>> tcjobs;  // per step: the series with a tilt at that step
+  std::vector<cudaEvent_t> events;         // 3 per step when the context profiles
   double op_bytes = 0, op_fma = 0;  // mean compulsory bytes / MACs of one operator apply
   ~mf_group() {
-    if (graph) cudaGraphExecDestroy(graph);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
   }
 };
 
 namespace mf {
 
-// corr[b][ip_b] = recorr_out[b] for the active series of a step
-__global__ void k_group_scatter(const float* __restrict__ src, const GroupSeriesDev* __restrict__ ser,
+// corr[b][ip_b] = recorr_out[b] for the series with a held-out tilt at the step
+__global__ void k_group_scatter(const GroupSeriesDev* __restrict__ ser,
                                 const GroupStepDev* __restrict__ steps,
-                                const int* __restrict__ active, size_t bpix) {
+                                const int* __restrict__ active) {
   const int b = blockIdx.y;
-  if (active[b] == 0) return;
-  const float4* s = reinterpret_cast<const float4*>(src + (size_t)b * bpix);
-  float4* d = reinterpret_cast<float4*>(ser[b].corr + (size_t)steps[b].ip * bpix);
-  const size_t n4 = bpix / 4;
+  if (active[b] == 0 || steps[b].ip < 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const float4* s = reinterpret_cast<const float4*>(S.recorr_out);
+  float4* d = reinterpret_cast<float4*>(S.corr + (size_t)steps[b].ip * S.bpix);
+  const size_t n4 = S.bpix / 4;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4;
        i += (size_t)gridDim.x * blockDim.x)
     d[i] = s[i];
 }
 
-static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
+// ProjAlign::Setsize (ProjAlign.cpp:48-125) and CorrTomoStack's sizes
+// (CorrStack.cu:65-100) of one series.
+static void member_geometry(GroupMember* M, const mf_series* s, int align_z) {
+  M->nx = s->nx;
+  M->ny = s->ny;
+  M->nz = s->nz;
+  M->n = s->nz - 1;
+  const int bx = (int)((float)s->nx / 2048.0f + 0.5f), by = (int)((float)s->ny / 2048.0f + 0.5f);
+  M->bin = std::max(1, std::max(bx, by));
+  M->xb = s->nx / M->bin / 2 * 2;
+  M->yb = s->ny / M->bin / 2 * 2;
+  M->pad = (M->xb / 2 + 1) * 2;
+  M->cmp = M->pad / 2;
+  M->thick = align_z / M->bin / 2 * 2;
+  const int pad_x = (s->nx / 2 + 1) * 2;
+  M->out_x = (pad_x / 2 - 1) * 2;
+  M->binx = M->out_x / M->xb;
+  M->biny = s->ny / M->yb;
+  M->bpix = (size_t)M->xb * M->yb;
+  M->ppix = (size_t)M->pad * M->yb;
+  M->ytiles = (M->yb + kApplyTileY - 1) / kApplyTileY;
+  M->xpitch = (M->xb + 7) / 8 * 8;
+}
+
+static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj) {
   StageTimer timer(&g->ctx->c, kStageSetup);
   Context* c = &g->ctx->c;
   cudaStream_t st = c->stream;
-  const int B = g->B, nx = g->nx, ny = g->ny, nz = g->nz;
-  int bx = (int)((float)nx / 2048.0f + 0.5f), by = (int)((float)ny / 2048.0f + 0.5f);
-  g->bin = std::max(1, std::max(bx, by));
-  g->xb = nx / g->bin / 2 * 2;
-  g->yb = ny / g->bin / 2 * 2;
-  g->pad = (g->xb / 2 + 1) * 2;
-  g->cmp = g->pad / 2;
-  g->thick = align_z / g->bin / 2 * 2;
-  g->nproj = nproj;
+  const int B = g->B;
   if (nproj <= 0) return set_error(MF_ERR_ARG, "nproj must be > 0");
-  if (g->thick < 2) return set_error(MF_ERR_ARG, "slab thickness %d too small", g->thick);
-  const int xb = g->xb, yb = g->yb, pad = g->pad;
-  g->bpix = (size_t)xb * yb;
-  g->ppix = (size_t)pad * yb;
-  g->ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
-  g->n = nz - 1;
-  const int n = g->n;
-  // geometry of every series: outward order and neighbour ranges (ProjAlign.cpp:151-176)
+  g->nproj = nproj;
+  g->m.clear();
   std::vector<ReprojGeom> geoms;
-  std::vector<GroupStepDev> steps((size_t)n * B);
   std::vector<float> bp;
   std::vector<int> orders;
-  std::vector<int> zts(B);
-  g->order.assign(B, {});
+  std::vector<std::vector<GroupStepDev>> steps_b(B);
   for (int b = 0; b < B; ++b) {
     mf_series* s = g->ser[b];
-    const int zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
-    zts[b] = zt;
+    g->m.emplace_back(new GroupMember());
+    GroupMember& M = *g->m.back();
+    member_geometry(&M, s, align_z[b]);
+    if (M.thick < 2)
+      return set_error(MF_ERR_ARG, "series %d: slab thickness %d too small", b, M.thick);
+    g->nz_max = std::max(g->nz_max, M.nz);
+    g->nmax = std::max(g->nmax, M.n);
+    g->xb_max = std::max(g->xb_max, M.xb);
+    g->yb_max = std::max(g->yb_max, M.yb);
+    g->pad_max = std::max(g->pad_max, M.pad);
+    g->cmp_max = std::max(g->cmp_max, M.cmp);
+    g->ytiles_max = std::max(g->ytiles_max, M.ytiles);
+    g->ntiles_max = std::max(g->ntiles_max, (M.xb + kOpTileX - 1) / kOpTileX);
+    g->rows_max = std::max(g->rows_max, M.nz * M.yb);
+    // outward order and neighbour ranges (ProjAlign.cpp:151-176)
+    const int nz = M.nz;
+    M.zt = frame_idx_from_tilt(nz, s->angles.data(), 0.0f);
     std::vector<unsigned char> skip(nz, 1);
-    skip[zt] = 0;
+    skip[M.zt] = 0;
     std::vector<ReprojGeom> gb;
     for (int i = 1; i < nz; ++i) {
       for (int side = 0; side < 2; ++side) {
-        int ip = side == 0 ? zt + i : zt - i;
+        int ip = side == 0 ? M.zt + i : M.zt - i;
         if (ip < 0 || ip >= nz) continue;
         int rg[2];
         find_proj_range(s->angles.data(), nz, skip.data(), ip, nproj, rg);
@@ -121,16 +157,18 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
                            "(%.2f)",
                            b, ip, s->angles[ip]);
         ReprojGeom gm;
-        reproj_geometry(s->angles.data(), ip, rg[0], rg[1], xb, yb, g->thick, &gm);
+        reproj_geometry(s->angles.data(), ip, rg[0], rg[1], M.xb, M.yb, M.thick, &gm);
         gb.push_back(gm);
         skip[ip] = 0;
       }
     }
+    if ((int)gb.size() != M.n)
+      return set_error(MF_ERR_GEOMETRY, "series %d: %d held-out tilts instead of %d", b,
+                       (int)gb.size(), M.n);
     MF_TRY(fill_bp_device(c, s->angles.data(), &gb, st));
+    M.op0 = (int)geoms.size();
     for (const ReprojGeom& gm : gb) {
-      const int k = (int)g->order[b].size();
-      if (k >= n) break;
-      GroupStepDev& sd = steps[(size_t)k * B + b];
+      GroupStepDev sd;
       sd.ip = gm.ip;
       sd.i0 = gm.i0;
       sd.nk = gm.nk;
@@ -140,40 +178,60 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
       sd.fcos = gm.fcos;
       sd.fsin = gm.fsin;
       bp.insert(bp.end(), gm.bp.begin(), gm.bp.end());
-      g->order[b].push_back(gm.ip);
+      steps_b[b].push_back(sd);
+      M.order.push_back(gm.ip);
       geoms.push_back(gm);
     }
-    if ((int)g->order[b].size() != n)
-      return set_error(MF_ERR_GEOMETRY, "series %d: %d held-out tilts instead of %d", b,
-                       (int)g->order[b].size(), n);
-    orders.insert(orders.end(), g->order[b].begin(), g->order[b].end());
   }
-  // buffers
-  MF_TRY(g->corr.alloc(sizeof(float) * g->bpix * nz * B));
-  MF_TRY(g->scratch.alloc(sizeof(float) * g->ppix * nz * B));
-  MF_TRY(g->reproj.alloc(sizeof(float) * g->bpix * B));
-  MF_TRY(g->cc.alloc(sizeof(float) * g->ppix * 2 * B));
-  MF_TRY(g->recorr.alloc(sizeof(float) * g->ppix * B));
-  MF_TRY(g->recorr_out.alloc(sizeof(float) * g->bpix * B));
-  MF_TRY(g->mpart.alloc(sizeof(double2) * moment_parts(yb) * 2 * B));
-  MF_TRY(g->stats.alloc(sizeof(float2) * 2 * B));
-  MF_TRY(g->mask.alloc(sizeof(float) * g->bpix));
-  MF_TRY(make_round_mask(c, xb, yb, (float)((pad / 2 - 1) * 2) * 0.5f, (float)yb * 0.5f,
-                         (float)pad, (float)yb, 4.0f, g->mask.as<float>(), st));
-  MF_TRY(g->ppart.alloc(sizeof(float2) * kPeakParts * B));
-  MF_TRY(g->rowflags.alloc(sizeof(int) * g->ytiles * B));
+  const int nmax = g->nmax;
+  // steps table [k][b]; a series without a tilt at step k gets ip = -1
+  std::vector<GroupStepDev> steps((size_t)nmax * B);
+  for (int k = 0; k < nmax; ++k)
+    for (int b = 0; b < B; ++b) {
+      GroupStepDev sd{};
+      sd.ip = -1;
+      if (k < (int)steps_b[b].size()) sd = steps_b[b][k];
+      steps[(size_t)k * B + b] = sd;
+    }
+  // per-series buffers
+  for (int b = 0; b < B; ++b) {
+    GroupMember& M = *g->m[b];
+    MF_TRY(M.corr.alloc(sizeof(float) * M.bpix * M.nz));
+    MF_TRY(M.scratch.alloc(sizeof(float) * M.ppix * M.nz));
+    MF_TRY(M.reproj.alloc(sizeof(float) * M.bpix));
+    MF_TRY(M.cc.alloc(sizeof(float) * M.ppix * 2));
+    MF_TRY(M.recorr.alloc(sizeof(float) * M.ppix));
+    MF_TRY(M.recorr_out.alloc(sizeof(float) * M.bpix));
+    MF_TRY(M.mpart.alloc(sizeof(double2) * moment_parts(M.yb) * 2));
+    MF_TRY(M.stats.alloc(sizeof(float2) * 2));
+    MF_TRY(M.ppart.alloc(sizeof(float2) * kPeakParts));
+    auto key = std::make_pair(M.xb, M.yb);
+    auto it = g->masks.find(key);
+    if (it == g->masks.end()) {
+      std::unique_ptr<DevBuf> mk(new DevBuf());
+      MF_TRY(mk->alloc(sizeof(float) * M.bpix));
+      MF_TRY(make_round_mask(c, M.xb, M.yb, (float)((M.pad / 2 - 1) * 2) * 0.5f,
+                             (float)M.yb * 0.5f, (float)M.pad, (float)M.yb, 4.0f,
+                             mk->as<float>(), st));
+      it = g->masks.emplace(key, std::move(mk)).first;
+    }
+    M.mask = it->second->as<float>();
+    if (g->prec != MF_PREC_FP32) {
+      MF_TRY(M.corr16.alloc((size_t)2 * M.xpitch * M.yb * M.nz));
+      MF_TRY(M.tflags.alloc(sizeof(int) * (size_t)M.nz * M.ytiles * kFlagParts));
+    }
+    for (int z : M.order) orders.push_back(z);
+  }
   MF_TRY(g->d_steps.alloc(sizeof(GroupStepDev) * steps.size()));
   MF_TRY(g->d_order.alloc(sizeof(int) * std::max<size_t>(orders.size(), 1)));
   MF_TRY(g->d_bp.alloc(sizeof(float) * std::max<size_t>(bp.size(), 1)));
   MF_TRY(g->d_active.alloc(sizeof(int) * B));
   MF_TRY(g->d_maxerr.alloc(sizeof(float) * B));
   MF_TRY(g->d_z0.alloc(sizeof(float) * B));
-  MF_TRY(g->d_err.alloc(sizeof(float) * nz * B));
-  MF_TRY(g->d_meas.alloc(sizeof(float) * 2 * nz * B));
+  MF_TRY(g->d_err.alloc(sizeof(float) * g->nz_max * B));
+  MF_TRY(g->d_meas.alloc(sizeof(float) * 2 * g->nz_max * B));
   MF_TRY(g->d_tcerr.alloc(sizeof(int)));
   MF_TRY(g->d_ser.alloc(sizeof(GroupSeriesDev) * B));
-  MF_TRY(g->d_normptr.alloc(sizeof(float*) * 2 * B * (size_t)n));
-  MF_TRY(g->d_tiltidx.alloc(sizeof(int) * B * (size_t)n));
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_steps.p, steps.data(), sizeof(GroupStepDev) * steps.size(),
                                 cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_order.p, orders.data(), sizeof(int) * orders.size(),
@@ -184,16 +242,16 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
   g->z0.assign(B, zshift);
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_z0.p, g->z0.data(), sizeof(float) * B, cudaMemcpyHostToDevice,
                                 st));
-  MF_CHECK_CUDA(cudaMemsetAsync(g->d_err.p, 0, sizeof(float) * nz * B, st));
-  MF_CHECK_CUDA(cudaMemsetAsync(g->d_meas.p, 0, sizeof(float) * 2 * nz * B, st));
+  MF_CHECK_CUDA(cudaMemsetAsync(g->d_err.p, 0, sizeof(float) * g->nz_max * B, st));
+  MF_CHECK_CUDA(cudaMemsetAsync(g->d_meas.p, 0, sizeof(float) * 2 * g->nz_max * B, st));
   MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
   std::vector<GroupSeriesDev> sd(B);
-  std::vector<const float*> normptr((size_t)2 * B * n);
-  std::vector<int> tiltidx((size_t)B * n);
-  float* corr = g->corr.as<float>();
+  size_t order_off = 0;
   for (int b = 0; b < B; ++b) {
     mf_series* s = g->ser[b];
+    GroupMember& M = *g->m[b];
     GroupSeriesDev& d = sd[b];
+    memset(&d, 0, sizeof(d));
     d.stack = s->stack.as<float>();
     d.stack_t = s->stack_t.as<float>();
     d.sx = s->d_sx.as<float>();
@@ -203,182 +261,222 @@ static int group_setup(mf_group* g, float zshift, int align_z, int nproj) {
     d.rot = s->d_rot.as<float>();
     d.angles = s->d_angles.as<float>();
     d.z0 = g->d_z0.as<float>() + b;
-    d.err = g->d_err.as<float>() + (size_t)b * nz;
-    d.meas = g->d_meas.as<float>() + (size_t)b * 2 * nz;
-    d.corr = corr + (size_t)b * nz * g->bpix;
-    d.order = g->d_order.as<int>() + (size_t)b * n;
-    d.zt = zts[b];
-    d.pad0 = 0;
-    for (int k = 0; k < n; ++k) {
-      const int ip = g->order[b][k];
-      normptr[(size_t)k * 2 * B + 2 * b] = g->reproj.as<float>() + (size_t)b * g->bpix;
-      normptr[(size_t)k * 2 * B + 2 * b + 1] = d.corr + (size_t)ip * g->bpix;
-      tiltidx[(size_t)k * B + b] = b * nz + ip;
-    }
+    d.err = g->d_err.as<float>() + (size_t)b * g->nz_max;
+    d.meas = g->d_meas.as<float>() + (size_t)b * 2 * g->nz_max;
+    d.corr = M.corr.as<float>();
+    d.order = g->d_order.as<int>() + order_off;
+    order_off += M.order.size();
+    d.zt = M.zt;
+    d.n = M.n;
+    d.nx = M.nx;
+    d.ny = M.ny;
+    d.nz = M.nz;
+    d.bin = M.bin;
+    d.out_x = M.out_x;
+    d.binx = M.binx;
+    d.biny = M.biny;
+    d.xb = M.xb;
+    d.yb = M.yb;
+    d.pad = M.pad;
+    d.cmp = M.cmp;
+    d.ytiles = M.ytiles;
+    d.xpitch = M.xpitch;
+    d.bpix = M.bpix;
+    d.ppix = M.ppix;
+    d.scratch = M.scratch.as<float>();
+    d.reproj = M.reproj.as<float>();
+    d.cc = M.cc.as<float>();
+    d.recorr = M.recorr.as<float>();
+    d.recorr_out = M.recorr_out.as<float>();
+    d.mask = M.mask;
+    d.mpart = M.mpart.as<double2>();
+    d.stats = M.stats.as<float2>();
+    d.ppart = M.ppart.as<float2>();
+    d.corr16 = M.corr16.p;
+    d.tflags = M.tflags.as<int>();
   }
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_ser.p, sd.data(), sizeof(GroupSeriesDev) * B,
                                 cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(g->d_normptr.p, normptr.data(), sizeof(float*) * normptr.size(),
-                                cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(g->d_tiltidx.p, tiltidx.data(), sizeof(int) * tiltidx.size(),
-                                cudaMemcpyHostToDevice, st));
-  // re-projection operators of every (series, step): geometry index b * n + k
+  // re-projection operators of every (series, step): geometry index op0 + k
+  g->tcjobs.assign(nmax, {});
   if (g->prec != MF_PREC_FP32) {
-    g->xpitch = (xb + 7) / 8 * 8;
-    MF_TRY(g->corr16.alloc((size_t)2 * g->xpitch * yb * nz * B));
-    MF_TRY(g->tflags.alloc(sizeof(int) * (size_t)nz * B * g->ytiles * kFlagParts));
-    MF_TRY(build_reproj_tc_ops(c, geoms, g->prec, &g->tcops, st));
-    g->tcjobs.resize((size_t)n * B);
-    for (int b = 0; b < B; ++b)
-      for (int k = 0; k < n; ++k) {
-        const TcOpView& v = g->tcops.ops[(size_t)b * n + k];
-        g->tcjobs[(size_t)k * B + b] =
-            TcJob{v.xt, v.colvalid, g->reproj.as<float>() + (size_t)b * g->bpix, b * nz, 0};
+    MF_TRY(build_reproj_tc_ops_any(c, geoms, g->prec, &g->tcops, st));
+    g->maps.assign(B, TmaDesc());
+    for (int b = 0; b < B; ++b) {
+      const GroupMember& M = *g->m[b];
+      for (int k = 0; k < M.n; ++k) {
+        const TcOpView& v = g->tcops.ops[M.op0 + k];
+        g->tcjobs[k].push_back(TcJob{v.xt, v.colvalid, M.reproj.as<float>(), b, b, M.xb, M.yb,
+                                     0, 0});
       }
-    // tile rows: timed on the first step of this group's shape, on a zeroed
-    // 16-bit stack (the launches only write the re-projection buffers, which
-    // every pass overwrites)
-    MF_CHECK_CUDA(cudaMemsetAsync(g->corr16.p, 0, g->corr16.bytes, st));
+    }
+    // tile rows: timed on the first step, on zeroed 16-bit stacks (the launches
+    // only write the re-projection buffers, which every pass overwrites)
+    for (int b = 0; b < B; ++b) {
+      GroupMember& M = *g->m[b];
+      MF_CHECK_CUDA(cudaMemsetAsync(M.corr16.p, 0, M.corr16.bytes, st));
+    }
     MF_TRY(tc_autotune_rows(
-        c, xb, yb, B, g->prec,
+        c, g->xb_max, g->yb_max, B, g->prec,
         [&](int nb) -> int {
-          TmaDesc m;
-          MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, nb, &m));
-          return launch_reproject_tc_group(c, g->tcops, g->tcjobs.data(), B, nullptr, xb, yb, m,
+          for (int b = 0; b < B; ++b) {
+            GroupMember& M = *g->m[b];
+            MF_TRY(tc_image_map(M.corr16.p, g->prec, M.xb, M.xpitch, M.yb, M.nz, nb, &g->maps[b]));
+          }
+          return launch_reproject_tc_group(c, g->tcops, g->tcjobs[0].data(),
+                                           (int)g->tcjobs[0].size(), nullptr, g->maps.data(), B,
                                            nb, g->d_tcerr.as<int>(), st);
         },
         g->d_tcerr.as<int>(), &g->tc_nb, st));
     MF_TRY(tc_prepare(c, g->tc_nb));
-    MF_TRY(tc_image_map(g->corr16.p, g->prec, xb, g->xpitch, yb, nz * B, g->tc_nb, &g->imgmap));
+    for (int b = 0; b < B; ++b) {
+      GroupMember& M = *g->m[b];
+      MF_TRY(tc_image_map(M.corr16.p, g->prec, M.xb, M.xpitch, M.yb, M.nz, g->tc_nb, &g->maps[b]));
+    }
     MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
   } else {
-    MF_TRY(build_reproj_ops(c, geoms, &g->ops, st));
-    std::vector<ApplyJob> jobs((size_t)n * B);
-    for (int b = 0; b < B; ++b)
-      for (int k = 0; k < n; ++k) {
-        const ReprojOpView& v = g->ops.ops[(size_t)b * n + k];
-        jobs[(size_t)k * B + b] =
-            ApplyJob{v.tiles, v.colvalid, sd[b].corr, g->reproj.as<float>() + (size_t)b * g->bpix,
-                     g->rowflags.as<int>() + (size_t)b * g->ytiles};
+    MF_TRY(build_reproj_ops_any(c, geoms, &g->ops, st));
+    MF_TRY(g->rowflags.alloc(sizeof(int) * (size_t)nmax * B * g->ytiles_max));
+    std::vector<ApplyJob> jobs((size_t)nmax * B);
+    for (int k = 0; k < nmax; ++k)
+      for (int b = 0; b < B; ++b) {
+        const GroupMember& M = *g->m[b];
+        ApplyJob J{};
+        J.rowflags = g->rowflags.as<int>() + ((size_t)k * B + b) * g->ytiles_max;
+        if (k < M.n) {
+          const ReprojOpView& v = g->ops.ops[M.op0 + k];
+          J.tiles = v.tiles;
+          J.colvalid = v.colvalid;
+          J.corr = M.corr.as<float>();
+          J.out = M.reproj.as<float>();
+          J.xb = M.xb;
+          J.yb = M.yb;
+          J.ntiles = v.ntiles;
+        }
+        jobs[(size_t)k * B + b] = J;
       }
     MF_TRY(g->d_applyjobs.alloc(sizeof(ApplyJob) * jobs.size()));
     MF_CHECK_CUDA(cudaMemcpyAsync(g->d_applyjobs.p, jobs.data(), sizeof(ApplyJob) * jobs.size(),
                                   cudaMemcpyHostToDevice, st));
   }
-  const double nops = (double)B * n;
+  const double nops = std::max<double>(1.0, (double)geoms.size());
   g->op_bytes = (g->prec != MF_PREC_FP32 ? g->tcops.bytes : g->ops.bytes) / nops;
   g->op_fma = (g->prec != MF_PREC_FP32 ? g->tcops.fma : g->ops.fma) / nops;
-  // FFT plans (cached per context)
+  // FFT plans (cached per context).  The same plan shapes as the series' own pass,
+  // executed once per series: a plan batched over the group may round
+  // differently, and a different rounding can flip a near-tied decision later
+  // (tilt-axis candidates, nearest-neighbour re-correction), so per-series
+  // execution keeps each result identical to the series aligned alone.
   mf_context* ctx = g->ctx;
-  // The same plan shapes as a single series' pass, executed once per series: a
-  // plan batched over the group may round differently, and a different rounding
-  // can flip a near-tied decision later (tilt-axis candidates, nearest-neighbour
-  // re-correction), so per-series execution keeps each result identical to the
-  // series aligned alone.
-  MF_TRY(ctx->plan({0, xb, yb, (long long)nz * yb}, &g->rows_fwd_all));
-  MF_TRY(ctx->plan({1, xb, yb, (long long)nz * yb}, &g->rows_inv_all));
-  MF_TRY(ctx->plan({0, xb, yb, (long long)yb}, &g->rows_fwd_one));
-  MF_TRY(ctx->plan({1, xb, yb, (long long)yb}, &g->rows_inv_one));
-  MF_TRY(ctx->plan({2, xb, yb, 2}, &g->cc_fwd));
-  MF_TRY(ctx->plan({3, xb, yb, 1}, &g->cc_inv));
+  for (int b = 0; b < B; ++b) {
+    GroupMember& M = *g->m[b];
+    MF_TRY(ctx->plan({0, M.xb, M.yb, (long long)M.nz * M.yb}, &M.rows_fwd_all));
+    MF_TRY(ctx->plan({1, M.xb, M.yb, (long long)M.nz * M.yb}, &M.rows_inv_all));
+    MF_TRY(ctx->plan({0, M.xb, M.yb, (long long)M.yb}, &M.rows_fwd_one));
+    MF_TRY(ctx->plan({1, M.xb, M.yb, (long long)M.yb}, &M.rows_inv_one));
+    MF_TRY(ctx->plan({2, M.xb, M.yb, 2}, &M.cc_fwd));
+    MF_TRY(ctx->plan({3, M.xb, M.yb, 1}, &M.cc_inv));
+  }
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;
 }
 
 // One projection-matching pass over the active series (the group form of
-// pa_enqueue in mf_series.cu).
+// pa_enqueue in mf_series.cu).  cuFFT runs only for the series that take part in
+// a stage (active, and with a held-out tilt at the step).
 static int group_enqueue(mf_group* g) {
   Context* c = &g->ctx->c;
   cudaStream_t st = c->stream;
-  const int B = g->B, nz = g->nz, n = g->n, xb = g->xb, yb = g->yb, pad = g->pad, cmp = g->cmp;
-  const size_t bpix = g->bpix, ppix = g->ppix;
+  const int B = g->B, nmax = g->nmax;
   const bool tc = g->prec != MF_PREC_FP32;
   const GroupSeriesDev* ser = g->d_ser.as<GroupSeriesDev>();
   const GroupStepDev* steps = g->d_steps.as<GroupStepDev>();
   const int* active = g->d_active.as<int>();
-  float* corr = g->corr.as<float>();
-  float* scratch = g->scratch.as<float>();
-  float* cc = g->cc.as<float>();
-  if (!tc) MF_CHECK_CUDA(cudaMemsetAsync(g->rowflags.p, 0, sizeof(int) * g->ytiles * B, st));
+  if (!tc)
+    MF_CHECK_CUDA(cudaMemsetAsync(g->rowflags.p, 0,
+                                  sizeof(int) * (size_t)nmax * B * g->ytiles_max, st));
   // CorrTomoStack::DoIt for every tilt of every active series
-  GroupCorrArgs ca{ser, nullptr, active, g->nx, g->ny, nz, g->bin, 1, scratch, pad, ppix};
-  MF_TRY(launch_correct_group(c, ca, B * nz, st));
-  for (int b = 0; b < B; ++b) {
-    float* sb = scratch + (size_t)b * nz * ppix;
-    MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_all, sb, (cufftComplex*)sb));
-  }
-  MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, B * nz * yb, st));
+  GroupCorrArgs ca{ser, nullptr, active, g->nz_max, 1};
+  MF_TRY(launch_correct_group(c, ca, B, g->xb_max, g->yb_max, st));
   for (int b = 0; b < B; ++b)
-    MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_all, (cufftComplex*)(scratch + (size_t)b * nz * ppix),
-                                corr + (size_t)b * nz * bpix));
+    if (g->active[b]) {
+      float* sb = g->m[b]->scratch.as<float>();
+      MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->rows_fwd_all, sb, (cufftComplex*)sb));
+    }
+  MF_TRY(launch_rweight_group(c, ser, nullptr, active, B, g->cmp_max, g->rows_max, st));
+  for (int b = 0; b < B; ++b)
+    if (g->active[b])
+      MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->rows_inv_all,
+                                  (cufftComplex*)g->m[b]->scratch.as<float>(),
+                                  g->m[b]->corr.as<float>()));
   if (tc)
-    MF_TRY(launch_to_half(c, corr, xb, yb, nullptr, 0, B * nz, g->prec, g->corr16.p, g->xpitch,
-                          g->tflags.as<int>(), st));
-  MF_TRY(fit_z0_group(c, ser, active, B, nz, st));
-  const float mcx = (float)((pad / 2 - 1) * 2) * 0.5f, mcy = (float)yb * 0.5f;
-  const bool prof = c->profiling && (int)g->events.size() >= 3 * n;
-  for (int k = 0; k < n; ++k) {
+    MF_TRY(launch_to_half_group(c, ser, nullptr, active, B, g->nz_max, g->ytiles_max, g->prec,
+                                st));
+  MF_TRY(fit_z0_group(c, ser, active, B, st));
+  const bool prof = c->profiling && (int)g->events.size() >= 3 * nmax;
+  std::vector<TcJob> jobs;
+  for (int k = 0; k < nmax; ++k) {
     const GroupStepDev* sk = steps + (size_t)k * B;
+    auto takes_part = [&](int b) { return g->active[b] && k < g->m[b]->n; };
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k], st));
     if (tc) {
-      MF_TRY(launch_reproject_tc_group(c, g->tcops, g->tcjobs.data() + (size_t)k * B, B, active,
-                                       xb, yb, g->imgmap, g->tc_nb, g->d_tcerr.as<int>(), st));
-      MF_TRY(launch_reproject_exact_group(c, ser, sk, active, B, nz, xb, yb, g->d_bp.as<float>(),
-                                          g->tflags.as<int>(), nullptr, g->reproj.as<float>(),
-                                          st));
+      jobs.clear();
+      for (const TcJob& J : g->tcjobs[k])
+        if (g->active[J.series]) jobs.push_back(J);
+      MF_TRY(launch_reproject_tc_group(c, g->tcops, jobs.data(), (int)jobs.size(), active,
+                                       g->maps.data(), B, g->tc_nb, g->d_tcerr.as<int>(), st));
+      MF_TRY(launch_reproject_exact_group(c, ser, sk, active, B, g->xb_max, g->ytiles_max,
+                                          g->d_bp.as<float>(), true, nullptr, st));
     } else {
-      const int ntiles = (xb + kOpTileX - 1) / kOpTileX;
       MF_TRY(launch_reproject_apply_group(c, g->ops, g->d_applyjobs.as<ApplyJob>() + (size_t)k * B,
-                                          active, B, xb, yb, ntiles, st));
-      MF_TRY(launch_reproject_exact_group(c, ser, sk, active, B, nz, xb, yb, g->d_bp.as<float>(),
-                                          nullptr, g->rowflags.as<int>(), g->reproj.as<float>(),
-                                          st));
+                                          active, B, g->ntiles_max, g->yb_max, st));
+      MF_TRY(launch_reproject_exact_group(
+          c, ser, sk, active, B, g->xb_max, g->ytiles_max, g->d_bp.as<float>(), false,
+          g->rowflags.as<int>() + (size_t)k * B * g->ytiles_max, st));
     }
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 1], st));
     // MeaAlignProj for every series: PANorm both images, FFT, filter, inverse, peak
-    MF_TRY(norm_mask_pad_group(c, g->d_normptr.as<const float*>() + (size_t)k * 2 * B, active,
-                               2 * B, xb, yb, pad, ppix, mcx, mcy, (float)pad, (float)yb, 4.0f,
-                               g->mask.as<float>(), cc, g->mpart.as<double2>(),
-                               g->stats.as<float2>(), st));
-    for (int b = 0; b < B; ++b) {
-      float* cb = cc + (size_t)b * 2 * ppix;
-      MF_CHECK_CUFFT(cufftExecR2C(g->cc_fwd, cb, (cufftComplex*)cb));
-    }
-    MF_TRY(xcorr_filter(c, (cufftComplex*)cc, ppix, nullptr, (cufftComplex*)(cc + ppix), ppix, B,
-                        cmp, yb, 500.0f, 1.0f, st));
-    for (int b = 0; b < B; ++b) {
-      float* mb = cc + (size_t)(2 * b + 1) * ppix;
-      MF_CHECK_CUFFT(cufftExecC2R(g->cc_inv, (cufftComplex*)mb, mb));
-    }
-    MF_TRY(pa_peak_update_group(c, cc + ppix, 2 * ppix, pad, xb, yb, g->ppart.as<float2>(), ser,
-                                sk, active, B, g->nx, g->ny, st));
-    // re-correct the aligned tilt of every series (mCorrectProj)
-    GroupCorrArgs rc{ser, sk, active, g->nx, g->ny, nz, g->bin, 1, g->recorr.as<float>(), pad,
-                     ppix};
-    MF_TRY(launch_correct_group(c, rc, B, st));
-    for (int b = 0; b < B; ++b) {
-      float* rb = g->recorr.as<float>() + (size_t)b * ppix;
-      MF_CHECK_CUFFT(cufftExecR2C(g->rows_fwd_one, rb, (cufftComplex*)rb));
-    }
-    MF_TRY(launch_rweight(c, (cufftComplex*)g->recorr.as<float>(), cmp, B * yb, st));
+    MF_TRY(norm_mask_pad_group(c, ser, sk, active, B, g->xb_max, g->yb_max, g->pad_max, st));
     for (int b = 0; b < B; ++b)
-      MF_CHECK_CUFFT(cufftExecC2R(g->rows_inv_one,
-                                  (cufftComplex*)(g->recorr.as<float>() + (size_t)b * ppix),
-                                  g->recorr_out.as<float>() + (size_t)b * bpix));
-    k_group_scatter<<<dim3(64, B), 256, 0, st>>>(g->recorr_out.as<float>(), ser, sk, active, bpix);
+      if (takes_part(b)) {
+        float* cb = g->m[b]->cc.as<float>();
+        MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->cc_fwd, cb, (cufftComplex*)cb));
+      }
+    MF_TRY(xcorr_filter_group(c, ser, sk, active, B, g->cmp_max, g->yb_max, 500.0f, st));
+    for (int b = 0; b < B; ++b)
+      if (takes_part(b)) {
+        float* mb = g->m[b]->cc.as<float>() + g->m[b]->ppix;
+        MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->cc_inv, (cufftComplex*)mb, mb));
+      }
+    MF_TRY(pa_peak_update_group(c, ser, sk, active, B, st));
+    // re-correct the aligned tilt of every series (mCorrectProj)
+    GroupCorrArgs rc{ser, sk, active, g->nz_max, 1};
+    MF_TRY(launch_correct_group(c, rc, B, g->xb_max, g->yb_max, st));
+    for (int b = 0; b < B; ++b)
+      if (takes_part(b)) {
+        float* rb = g->m[b]->recorr.as<float>();
+        MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->rows_fwd_one, rb, (cufftComplex*)rb));
+      }
+    MF_TRY(launch_rweight_group(c, ser, sk, active, B, g->cmp_max, g->yb_max, st));
+    for (int b = 0; b < B; ++b)
+      if (takes_part(b))
+        MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->rows_inv_one,
+                                    (cufftComplex*)g->m[b]->recorr.as<float>(),
+                                    g->m[b]->recorr_out.as<float>()));
+    k_group_scatter<<<dim3(64, B), 256, 0, st>>>(ser, sk, active);
     c->launches++;
     MF_CHECK_CUDA(cudaGetLastError());
     if (tc)
-      MF_TRY(launch_to_half(c, corr, xb, yb, g->d_tiltidx.as<int>() + (size_t)k * B, 0, B, g->prec,
-                            g->corr16.p, g->xpitch, g->tflags.as<int>(), st));
+      MF_TRY(launch_to_half_group(c, ser, sk, active, B, g->nz_max, g->ytiles_max, g->prec, st));
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 2], st));
   }
-  MF_TRY(max_err_group(c, ser, active, B, n, g->d_maxerr.as<float>(), st));
+  MF_TRY(max_err_group(c, ser, active, B, g->d_maxerr.as<float>(), st));
   return MF_OK;
 }
 
 // One pass over the series with active[b] != 0; max_err[b] receives each active
-// series' largest measured shift (inactive entries are left as they are).
+// series' largest measured shift (inactive entries are left as they are).  The
+// pass is launched eagerly: its cuFFT calls depend on which series take part.
 static int group_doit(mf_group* g, const int* active, float* max_err) {
   StageTimer timer(&g->ctx->c, kStagePass);
   Context* c = &g->ctx->c;
@@ -388,42 +486,12 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   for (int b = 0; b < B; ++b) MF_TRY(g->ser[b]->upload_params());
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_active.p, g->active.data(), sizeof(int) * B,
                                 cudaMemcpyHostToDevice, st));
-  // Profiled passes run eagerly: events recorded by graph nodes cannot be timed.
-  while (c->profiling && (int)g->events.size() < 3 * g->n) {
+  while (c->profiling && (int)g->events.size() < 3 * g->nmax) {
     cudaEvent_t e;
     MF_CHECK_CUDA(cudaEventCreate(&e));
     g->events.push_back(e);
   }
-  if (g->use_graph && !g->graph && !c->profiling) {
-    int64_t l0 = c->launches;
-    cudaGraph_t gr = nullptr;
-    std::unique_lock<std::recursive_mutex> fft_lock(fft_mutex());
-    MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int rc = group_enqueue(g);
-    cudaError_t ec = cudaStreamEndCapture(st, &gr);
-    fft_lock.unlock();
-    g->graph_kernels = c->launches - l0;
-    c->launches = l0;
-    if (rc != MF_OK || ec != cudaSuccess) {
-      if (gr) cudaGraphDestroy(gr);
-      cudaGetLastError();
-      g->use_graph = false;
-    } else {
-      cudaError_t ei = cudaGraphInstantiate(&g->graph, gr, 0);
-      cudaGraphDestroy(gr);
-      if (ei != cudaSuccess) {
-        cudaGetLastError();
-        g->graph = nullptr;
-        g->use_graph = false;
-      }
-    }
-  }
-  if (g->graph && !c->profiling) {
-    MF_CHECK_CUDA(cudaGraphLaunch(g->graph, st));
-    c->launches += g->graph_kernels;
-  } else {
-    MF_TRY(group_enqueue(g));
-  }
+  MF_TRY(group_enqueue(g));
   std::vector<float> me(B);
   int tcerr = 0;
   MF_CHECK_CUDA(cudaMemcpyAsync(me.data(), g->d_maxerr.p, sizeof(float) * B,
@@ -436,27 +504,27 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   if (tcerr != 0)
     return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", tcerr);
-  int nact = 0;
+  double steps_run = 0;
   for (int b = 0; b < B; ++b)
     if (active[b]) {
       max_err[b] = me[b];
       g->ser[b]->pa.z0 = g->z0[b];
-      nact++;
+      steps_run += g->m[b]->n;
     }
-  if (c->profiling && (int)g->events.size() >= 3 * g->n) {
+  if (c->profiling && (int)g->events.size() >= 3 * g->nmax) {
     // stage times of this pass: [0] re-projection launches (one per step for the
     // whole group), [2] the rest of each step; bytes and MACs of the active series
-    for (int k = 0; k < g->n; ++k) {
+    for (int k = 0; k < g->nmax; ++k) {
       float a = 0.0f, b2 = 0.0f;
       MF_CHECK_CUDA(cudaEventElapsedTime(&a, g->events[3 * k], g->events[3 * k + 1]));
       MF_CHECK_CUDA(cudaEventElapsedTime(&b2, g->events[3 * k + 1], g->events[3 * k + 2]));
       c->stage[0] += a;
       c->stage[2] += b2;
     }
-    c->stage[1] += g->n;
+    c->stage[1] += g->nmax;
     c->stage[3] += 1;
-    c->stage[4] += g->op_bytes * g->n * nact;
-    c->stage[5] += g->op_fma * g->n * nact;
+    c->stage[4] += g->op_bytes * steps_run;
+    c->stage[5] += g->op_fma * steps_run;
   }
   return MF_OK;
 }
@@ -505,30 +573,24 @@ int group_proj_align(mf_group* g, int* passes) {
   return MF_OK;
 }
 
-int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift, int align_z,
-                 int nproj, mf_group** out) {
+int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift,
+                 const int* align_z, int nproj, mf_group** out) {
   if (!out) return set_error(MF_ERR_ARG, "null output pointer");
   *out = nullptr;
-  if (!ctx || !series || nser < 1 || nser > kMaxGroup)
+  if (!ctx || !series || !align_z || nser < 1 || nser > kMaxGroup)
     return set_error(MF_ERR_ARG, "a group holds 1..%d series (got %d)", kMaxGroup, nser);
   for (int b = 0; b < nser; ++b) {
     const mf_series* s = series[b];
     if (!s) return set_error(MF_ERR_ARG, "null series %d", b);
     if (s->ctx != ctx) return set_error(MF_ERR_ARG, "series %d belongs to another context", b);
     if (s->gpu != ctx->c.gpu) return set_error(MF_ERR_ARG, "series %d is on another GPU", b);
-    if (s->nx != series[0]->nx || s->ny != series[0]->ny || s->nz != series[0]->nz ||
-        s->precision != series[0]->precision)
-      return set_error(MF_ERR_ARG,
-                       "series %d differs in shape or precision from series 0 (%d x %d x %d)", b,
-                       series[0]->nx, series[0]->ny, series[0]->nz);
+    if (s->precision != series[0]->precision)
+      return set_error(MF_ERR_ARG, "series %d differs in precision from series 0", b);
   }
   mf_group* g = new mf_group();
   g->ctx = ctx;
   g->ser.assign(series, series + nser);
   g->B = nser;
-  g->nx = series[0]->nx;
-  g->ny = series[0]->ny;
-  g->nz = series[0]->nz;
   g->prec = series[0]->precision;
   int rc = group_setup(g, zshift, align_z, nproj);
   if (rc != MF_OK) {
@@ -537,6 +599,12 @@ int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshi
   }
   *out = g;
   return MF_OK;
+}
+
+int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift, int align_z,
+                 int nproj, mf_group** out) {
+  std::vector<int> az(std::max(nser, 0), align_z);
+  return group_create(ctx, series, nser, zshift, az.data(), nproj, out);
 }
 
 }  // namespace mf
@@ -551,6 +619,54 @@ int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshi
   catch (...) {                                                           \
     return set_error(MF_ERR_STATE, "unexpected exception in the library"); \
   }
+
+// Process::DoIt minus file I/O (Process.cpp:34-92) for n series given by their
+// device buffers, sizes and slab thicknesses: every series is uploaded and
+// pre-processed, coarse-aligned stage by stage with the others of its group of
+// up to kMaxGroup, projection-matched with them in lockstep, then corrected into
+// its output buffer.
+static int align_batch(mf_context* ctx, int n, const float* const* d_raw, const int* nx,
+                       const int* ny, const int* nz, const float* const* file_angles,
+                       const int* align_z, const mf_options* opt, mf_align_param* params,
+                       float* const* d_out, int* passes) {
+  if (!ctx || n < 1 || !d_raw || !file_angles || !opt || !params)
+    return set_error(MF_ERR_ARG, "null argument");
+  if (opt->nproj <= 0) return set_error(MF_ERR_ARG, "nProj must be > 0.");
+  if (opt->out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
+  if (opt->precision != MF_PREC_FP32 && opt->precision != MF_PREC_BF16 &&
+      opt->precision != MF_PREC_FP16)
+    return set_error(MF_ERR_ARG, "unknown precision %d", opt->precision);
+  std::vector<mf_series*> ser(n, nullptr);
+  auto cleanup = [&]() {
+    for (mf_series* s : ser) mf_series_destroy(s);
+  };
+  int rc = MF_OK;
+  for (int i = 0; i < n && rc == MF_OK; ++i) {
+    rc = mf_series_create_device(ctx, d_raw[i], nx[i], ny[i], nz[i], file_angles[i], &ser[i]);
+    if (rc == MF_OK) ser[i]->precision = (mf_precision)opt->precision;
+  }
+  const bool align = opt->align_z != 0;
+  for (int g0 = 0; g0 < n && rc == MF_OK && align; g0 += kMaxGroup)
+    rc = coarse_align_many(ser.data() + g0, std::min(kMaxGroup, n - g0), opt->pitch_angle,
+                           opt->offset);
+  for (int g0 = 0; g0 < n && rc == MF_OK && align; g0 += kMaxGroup) {
+    const int m = std::min(kMaxGroup, n - g0);
+    mf_group* g = nullptr;
+    rc = group_create(ctx, ser.data() + g0, m, opt->zshift, align_z + g0, opt->nproj, &g);
+    if (rc == MF_OK) rc = group_proj_align(g, passes ? passes + g0 : nullptr);
+    delete g;
+  }
+  if (!align && passes)
+    for (int i = 0; i < n; ++i) passes[i] = 0;
+  for (int i = 0; i < n && rc == MF_OK; ++i) {
+    if (d_out && d_out[i]) rc = correct_stack_device(ser[i], opt->out_bin, d_out[i]);
+    if (rc == MF_OK) rc = mf_series_get_param(ser[i], &params[i]);
+  }
+  if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
+    rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
+  cleanup();
+  return rc;
+}
 
 extern "C" {
 
@@ -589,51 +705,35 @@ MF_API int mf_group_proj_align(mf_group* g, int* passes) {
   MF_GUARD_END
 }
 
-// Process::DoIt minus file I/O (Process.cpp:34-92) for n series of one shape:
-// every series is uploaded and pre-processed, coarse-aligned stage by stage with
-// the others of its group of up to kMaxGroup, projection-matched with them in
-// lockstep, then corrected into d_out[i].
 MF_API int mf_align_many_device(mf_context* ctx, int n, const float* const* d_raw, int nx, int ny,
                                 int nz, const float* const* file_angles, const mf_options* opt,
                                 mf_align_param* params, float* const* d_out, int* passes) {
   MF_GUARD_BEGIN
-  if (!ctx || n < 1 || !d_raw || !file_angles || !opt || !params)
-    return set_error(MF_ERR_ARG, "null argument");
-  if (opt->nproj <= 0) return set_error(MF_ERR_ARG, "nProj must be > 0.");
-  if (opt->out_bin < 1) return set_error(MF_ERR_ARG, "output binning must be >= 1");
-  if (opt->precision != MF_PREC_FP32 && opt->precision != MF_PREC_BF16 &&
-      opt->precision != MF_PREC_FP16)
-    return set_error(MF_ERR_ARG, "unknown precision %d", opt->precision);
-  std::vector<mf_series*> ser(n, nullptr);
-  auto cleanup = [&]() {
-    for (mf_series* s : ser) mf_series_destroy(s);
-  };
-  int rc = MF_OK;
-  for (int i = 0; i < n && rc == MF_OK; ++i) {
-    rc = mf_series_create_device(ctx, d_raw[i], nx, ny, nz, file_angles[i], &ser[i]);
-    if (rc == MF_OK) ser[i]->precision = (mf_precision)opt->precision;
+  if (!ctx || n < 1 || !opt) return set_error(MF_ERR_ARG, "null argument");
+  std::vector<int> vx(n, nx), vy(n, ny), vz(n, nz), az(n, opt->align_z);
+  return align_batch(ctx, n, d_raw, vx.data(), vy.data(), vz.data(), file_angles, az.data(), opt,
+                     params, d_out, passes);
+  MF_GUARD_END
+}
+
+MF_API int mf_align_batch_device(mf_context* ctx, int n, const mf_series_desc* series,
+                                 const mf_options* opt, mf_align_param* params, int* passes) {
+  MF_GUARD_BEGIN
+  if (!ctx || n < 1 || !series || !opt) return set_error(MF_ERR_ARG, "null argument");
+  std::vector<const float*> raw(n), ang(n);
+  std::vector<float*> out(n);
+  std::vector<int> vx(n), vy(n), vz(n), az(n);
+  for (int i = 0; i < n; ++i) {
+    raw[i] = series[i].d_raw;
+    ang[i] = series[i].file_angles;
+    out[i] = series[i].d_out;
+    vx[i] = series[i].nx;
+    vy[i] = series[i].ny;
+    vz[i] = series[i].nz;
+    az[i] = series[i].align_z != 0 ? series[i].align_z : opt->align_z;
   }
-  // the coarse stages stage by stage over groups of series (one host wait per stage)
-  for (int g0 = 0; g0 < n && rc == MF_OK && opt->align_z != 0; g0 += kMaxGroup)
-    rc = coarse_align_many(ser.data() + g0, std::min(kMaxGroup, n - g0), opt->pitch_angle,
-                           opt->offset);
-  for (int g0 = 0; g0 < n && rc == MF_OK && opt->align_z != 0; g0 += kMaxGroup) {
-    const int m = std::min(kMaxGroup, n - g0);
-    mf_group* g = nullptr;
-    rc = group_create(ctx, ser.data() + g0, m, opt->zshift, opt->align_z, opt->nproj, &g);
-    if (rc == MF_OK) rc = group_proj_align(g, passes ? passes + g0 : nullptr);
-    delete g;
-  }
-  if (opt->align_z == 0 && passes)
-    for (int i = 0; i < n; ++i) passes[i] = 0;
-  for (int i = 0; i < n && rc == MF_OK; ++i) {
-    if (d_out && d_out[i]) rc = correct_stack_device(ser[i], opt->out_bin, d_out[i]);
-    if (rc == MF_OK) rc = mf_series_get_param(ser[i], &params[i]);
-  }
-  if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
-    rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
-  cleanup();
-  return rc;
+  return align_batch(ctx, n, raw.data(), vx.data(), vy.data(), vz.data(), ang.data(), az.data(),
+                     opt, params, out.data(), passes);
   MF_GUARD_END
 }
 

@@ -133,13 +133,15 @@ __global__ void k_correct_bin(CorrArgs a) {
 
 // k_correct_bin for a group of series: job j is tilt (j % nz) of series j / nz,
 // or, with a step table, the held-out tilt of series j at that step.
-__global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int binx, int biny) {
+__global__ void k_correct_group(GroupCorrArgs g) {
   __shared__ float s_cs, s_sn, s_sx, s_sy;
   const int j = blockIdx.z;
-  const int b = g.steps ? j : j / g.nz;
+  const int b = g.steps ? j : j / g.nz_max;
   if (g.active && g.active[b] == 0) return;
   const GroupSeriesDev& S = g.ser[b];
-  const int z = g.steps ? g.steps[b].ip : j % g.nz;
+  const int z = g.steps ? g.steps[b].ip : j % g.nz_max;
+  if (z < 0 || z >= S.nz) return;  // no held-out tilt at this step / beyond this series
+  if ((int)(blockIdx.x * blockDim.x) >= S.xb) return;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     const float axis = (float)((double)S.rot[z] * kD2R);  // CorrStack.cu:376-378
     s_cs = cosf(axis);  // CUDA's cosf/sinf, as mGCorrect (CorrStack.cu:160-161)
@@ -149,20 +151,22 @@ __global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int 
   }
   __syncthreads();
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (bx >= xb) return;
-  const Layout L = pick_layout(S.stack_t, g.nx, g.ny, s_cs, s_sn);
-  const float* img = (L.xs == 1 ? S.stack : S.stack_t) + (size_t)z * g.nx * g.ny;
+  if (bx >= S.xb) return;
+  const int nx = S.nx, ny = S.ny, binx = S.binx, biny = S.biny;
+  const Layout L = pick_layout(S.stack_t, nx, ny, s_cs, s_sn);
+  const float* img = (L.xs == 1 ? S.stack : S.stack_t) + (size_t)z * nx * ny;
+  float* out = g.steps ? S.recorr : S.scratch + (size_t)z * S.ppix;
   // rows in a grid-stride loop: the set-up above is paid once per block
-  for (int by = blockIdx.y * blockDim.y + threadIdx.y; by < yb; by += gridDim.y * blockDim.y) {
+  for (int by = blockIdx.y * blockDim.y + threadIdx.y; by < S.yb; by += gridDim.y * blockDim.y) {
     float res;
-    if (g.bin == 1) {
-      res = corr_pixel(img, L, g.nx, g.ny, bx, by, out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
+    if (S.bin == 1) {
+      res = corr_pixel(img, L, nx, ny, bx, by, S.out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
     } else {
       float sum = 0.0f;
       bool bad = false;
       for (int iy = 0; iy < biny && !bad; ++iy) {
         for (int ix = 0; ix < binx; ++ix) {
-          float v = corr_pixel(img, L, g.nx, g.ny, bx * binx + ix, by * biny + iy, out_x, s_sx,
+          float v = corr_pixel(img, L, nx, ny, bx * binx + ix, by * biny + iy, S.out_x, s_sx,
                                s_sy, s_cs, s_sn, g.random_fill);
           if (v < -1e10f) {
             bad = true;
@@ -173,7 +177,7 @@ __global__ void k_correct_group(GroupCorrArgs g, int out_x, int xb, int yb, int 
       }
       res = bad ? kSentinel : sum;
     }
-    g.out[(size_t)j * g.out_tilt_stride + (size_t)by * g.out_row_stride + bx] = res;
+    out[(size_t)by * S.pad + bx] = res;
   }
 }
 
@@ -221,11 +225,11 @@ int launch_correct_bin(Context* c, const float* stack, const float* stack_t, int
   return MF_OK;
 }
 
-int launch_correct_group(Context* c, const GroupCorrArgs& g, int njobs, cudaStream_t st) {
-  CorrArgs a{};
-  fill_sizes(&a, g.nx, g.ny, g.bin);
-  dim3 blk(64, 4), grd((a.xb + 63) / 64, corr_row_blocks(a.yb, 4), njobs);
-  k_correct_group<<<grd, blk, 0, st>>>(g, a.out_x, a.xb, a.yb, a.binx, a.biny);
+int launch_correct_group(Context* c, const GroupCorrArgs& g, int nseries, int xb_max, int yb_max,
+                         cudaStream_t st) {
+  const int njobs = g.steps ? nseries : nseries * g.nz_max;
+  dim3 blk(64, 4), grd((xb_max + 63) / 64, corr_row_blocks(yb_max, 4), njobs);
+  k_correct_group<<<grd, blk, 0, st>>>(g);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -282,6 +286,46 @@ __global__ void k_rweight(cufftComplex* spec, int cmp, int rows) {
 int launch_rweight(Context* c, cufftComplex* spec, int cmp, int rows, cudaStream_t st) {
   dim3 blk(128, 2), grd((cmp + 127) / 128, std::min((rows + 1) / 2, 16384));
   k_rweight<<<grd, blk, 0, st>>>(spec, cmp, rows);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Group form: blockIdx.z = series; the rows of its scratch (all tilts, steps ==
+// null) or of its re-corrected held-out tilt, with its own spectrum width.
+__global__ void k_rweight_group(const GroupSeriesDev* __restrict__ ser,
+                                const GroupStepDev* __restrict__ steps,
+                                const int* __restrict__ active) {
+  const int b = blockIdx.z;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  if (steps && steps[b].ip < 0) return;
+  const int cmp = S.cmp;
+  const int rows = steps ? S.yb : S.nz * S.yb;
+  cufftComplex* spec = reinterpret_cast<cufftComplex*>(steps ? S.recorr : S.scratch);
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= cmp) return;
+  float fN = 2 * ((float)cmp - 1.0f);
+  float r = __fdiv_rn((float)x, fN);
+  float cw = cosf(__fmul_rn(6.2831852f, r));
+  r = __fmul_rn(__fmul_rn(2.0f, r), __fmaf_rn(0.45f, cw, 0.55f));
+  for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < rows;
+       row += gridDim.y * blockDim.y) {
+    size_t i = (size_t)row * cmp + x;
+    cufftComplex v = spec[i];
+    v.x = __fdiv_rn(v.x, fN);
+    v.y = __fdiv_rn(v.y, fN);
+    v.x = __fmul_rn(v.x, r);
+    v.y = __fmul_rn(v.y, r);
+    spec[i] = v;
+  }
+}
+
+int launch_rweight_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                         const int* active, int nseries, int cmp_max, int rows_max,
+                         cudaStream_t st) {
+  dim3 blk(128, 2), grd((cmp_max + 127) / 128, std::min((rows_max + 1) / 2, 16384), nseries);
+  k_rweight_group<<<grd, blk, 0, st>>>(ser, steps, active);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

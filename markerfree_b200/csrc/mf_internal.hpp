@@ -237,6 +237,7 @@ struct TcOpSet {
   DevBuf op16, xt, segs, colvalid;
   std::vector<TcOpView> ops;
   int total_chunks = 0;
+  int nsegs = 0, nxt = 0;  // entries of segs and xt
   int half_kind = 0;  // MF_PREC_BF16 or MF_PREC_FP16
   TmaDesc opmap;      // 2-D tensor map over op16, box 64 x 128
   double bytes = 0;   // compulsory bytes of one apply of every operator
@@ -296,6 +297,12 @@ int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpS
 // Tensor-core operators of all geometries (same xb, yb) in `half_kind` precision.
 int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
                         TcOpSet* set, cudaStream_t st);
+// The same two builders for geometries of any image sizes: one set per size, then
+// concatenated into `set` (ops in the order of `geoms`).
+int build_reproj_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
+                         cudaStream_t st);
+int build_reproj_tc_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
+                            TcOpSet* set, cudaStream_t st);
 // Encodes set->opmap over set->op16 (called by build_reproj_tc_ops).
 int tc_op_map(TcOpSet* set);
 // 3-D tensor map over a 16-bit copy of the corrected stack (nz x yb rows of xb
@@ -338,11 +345,16 @@ int launch_reproject_exact_flagged(Context* c, const float* corr, int xb, int yb
                                    cudaStream_t st);
 
 // ---- multi-series (group) execution ------------------------------------------
-// A group runs the projection-matching pass of up to kMaxGroup series of one
-// shape in lockstep: every stage is one launch over all series of the group
-// (the i-th held-out tilt of every series together).  Per-series state lives in
-// device tables; a per-series `active` flag lets the captured pass skip series
-// that have already left the current ProjAlignOnce loop.
+// A group runs the projection-matching pass of up to kMaxGroup series in
+// lockstep: every stage is one launch over all series of the group (the k-th
+// held-out tilt of every series together).  Series may differ in every size --
+// image, tilt count, slab thickness, matching binning -- so each kernel reads the
+// geometry and the work buffers of its series from the series' GroupSeriesDev
+// record and the grid covers the largest series; blocks beyond a smaller series'
+// extent return at once.  A series with fewer held-out tilts has no work in the
+// last steps (its GroupStepDev::ip is -1 there), and a per-series `active` flag
+// skips series that have already left the current ProjAlignOnce loop.  Every
+// series' arithmetic and its order are those of the series aligned alone.
 constexpr int kMaxGroup = 32;
 constexpr int kFlagParts = 8;  // column parts of a 16-bit copy's per-tile flags
 
@@ -361,50 +373,82 @@ struct GroupSeriesDev {
   float* err;    // nz: |shift| of the last measurement per tilt
   float* meas;   // 2 * nz: shift measured in the last pass (un-binned px, before rotation)
   float* corr;   // corrected stack of this series (nz x yb x xb)
-  const int* order;  // outward processing order (nz - 1 entries)
-  int zt, pad0;
+  const int* order;  // outward processing order (n entries)
+  int zt, n;         // zero-tilt index; held-out tilts per pass (nz - 1)
+  // shape (ProjAlign::Setsize, ProjAlign.cpp:48-125; CorrStack.cu:65-100)
+  int nx, ny, nz, bin;          // raw image, tilts, matching binning
+  int out_x, binx, biny;        // resampling grid before binning, bin factors
+  int xb, yb, pad, cmp;         // binned image, padded FFT row (floats), spectrum width
+  int ytiles, xpitch;           // 128-row tiles; 16-bit row pitch
+  size_t bpix, ppix;            // xb * yb, pad * yb
+  // work buffers of the pass
+  float* scratch;      // nz x yb x pad: rows of the batched R-weight FFT
+  float* reproj;       // yb x xb: re-projection of the step's held-out tilt
+  float* cc;           // 2 x yb x pad: the normalised pair, then spectrum / correlation
+  float* recorr;       // yb x pad: re-corrected held-out tilt before its R-weight
+  float* recorr_out;   // yb x xb
+  const float* mask;   // yb x xb round-edge factors of the correlation mask
+  double2* mpart;      // 2 x moment_parts(yb) moment partials
+  float2* stats;       // 2: (mean, std) of the pair
+  float2* ppart;       // kPeakParts peak partials
+  void* corr16;        // FP16/BF16: nz x yb x xpitch 16-bit copy of corr
+  int* tflags;         // FP16/BF16: nz x ytiles x kFlagParts flags of the copy
 };
 struct GroupStepDev {  // the held-out tilt of one series at one step of the pass
-  int ip, i0, nk, ray_len, thick, bp_off;  // bp_off: float offset in the bp table
+  int ip, i0, nk, ray_len, thick, bp_off;  // ip < 0: the series has no tilt at this step
   float fcos, fsin;
 };
 struct GroupCorrArgs {
   const GroupSeriesDev* ser;
-  const GroupStepDev* steps;  // null: all tilts of every series (job = b * nz + tilt)
+  const GroupStepDev* steps;  // null: all tilts of every series (job = b * nz_max + tilt)
   const int* active;          // null: all series
-  int nx, ny, nz, bin, random_fill;
-  float* out;
-  int out_row_stride;
-  size_t out_tilt_stride;
+  int nz_max, random_fill;
 };
-// resample + bin (k_correct_bin) for a group; one output image per job
-int launch_correct_group(Context* c, const GroupCorrArgs& a, int njobs, cudaStream_t st);
+// resample + bin (k_correct_bin) for a group; all tilts (steps == null) into each
+// series' scratch rows, or each series' held-out tilt of a step into its recorr
+int launch_correct_group(Context* c, const GroupCorrArgs& a, int nseries, int xb_max, int yb_max,
+                         cudaStream_t st);
+// R-weight (k_rweight) of every series' scratch rows (steps == null) or of its
+// re-corrected tilt at a step
+int launch_rweight_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                         const int* active, int nseries, int cmp_max, int rows_max,
+                         cudaStream_t st);
+// FP32 -> 16-bit copy (launch_to_half) of every tilt (steps == null) or of each
+// series' held-out tilt of a step
+int launch_to_half_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                         const int* active, int nseries, int nz_max, int ytiles_max,
+                         int half_kind, cudaStream_t st);
 // exact re-projection of the flagged 128-row tiles of every active series at one
-// step; flags: tflags of the 16-bit copies ([b*nz + tilt][ytiles][kFlagParts])
-// when tc, else the FP32 apply's rowflags ([b][ytiles])
+// step into its reproj buffer; flags: the 16-bit copy's tflags when tc, else the
+// FP32 apply's rowflags of the step (rowflags[b * ytiles_max + tile])
 int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
-                                 const int* active, int nseries, int nz, int xb, int yb,
-                                 const float* d_bp, const int* tflags, const int* rowflags,
-                                 float* out, cudaStream_t st);
-struct ApplyJob {  // one series of a group for the FP32 apply
+                                 const int* active, int nseries, int xb_max, int ytiles_max,
+                                 const float* d_bp, bool tc, const int* rowflags,
+                                 cudaStream_t st);
+struct ApplyJob {  // one series of a group at one step of the FP32 apply
   const OpTile* tiles;
   const int* colvalid;
   const float* corr;
   float* out;
   int* rowflags;
+  int xb, yb, ntiles;  // ntiles 0: no held-out tilt at this step
 };
 int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
-                                 const int* active, int njobs, int xb, int yb, int ntiles,
+                                 const int* active, int njobs, int ntiles_max, int yb_max,
                                  cudaStream_t st);
 struct TcJob {
   const TcXTile* xt;
   const int* colvalid;
   float* out;
-  int zoff;  // first tilt of this series in the group's 16-bit stack
-  int pad;
+  int series;        // index into `active`
+  int map;           // image tensor map of this series
+  int xb, yb, ntx;   // output size and 128-column tiles
+  int tile0;         // first tile of this job in the launch (set when launched)
 };
+// Tensor-core apply for a list of jobs (series of any shapes); maps[j] is the
+// 16-bit image map of job j's series.
 int launch_reproject_tc_group(Context* c, const TcOpSet& set, const TcJob* jobs, int njobs,
-                              const int* active, int xb, int yb, const TmaDesc& imgmap, int nb,
+                              const int* active, const TmaDesc* maps, int nmaps, int nb,
                               int* d_err, cudaStream_t st);
 
 void find_proj_range(const float* angles, int nz, const unsigned char* skip, int iproj,

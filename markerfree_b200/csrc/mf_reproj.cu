@@ -228,42 +228,44 @@ int launch_reproject_exact(Context* c, const float* corr, int xb, int yb, size_t
   return MF_OK;
 }
 
-// Group form: blockIdx.z = series.  A row tile is recomputed when its flags say so
-// (any neighbour's 16-bit tile flag, or the FP32 apply's row flag).
+// Group form: blockIdx.z = series, with its own geometry.  A row tile is recomputed
+// when its flags say so (any neighbour's 16-bit tile flag, or the FP32 apply's row
+// flag of this step).
 __global__ void k_reproject_exact_group(const GroupSeriesDev* __restrict__ ser,
                                         const GroupStepDev* __restrict__ steps,
-                                        const int* __restrict__ active, int nz, int xb, int yb,
-                                        const float* __restrict__ bps,
-                                        const int* __restrict__ tflags,
-                                        const int* __restrict__ rowflags,
-                                        float* __restrict__ out) {
+                                        const int* __restrict__ active,
+                                        const float* __restrict__ bps, int tc,
+                                        const int* __restrict__ rowflags, int ytiles_max) {
   const int b = blockIdx.z;
   if (active && active[b] == 0) return;
   const GroupStepDev S = steps[b];
-  const int ytiles = gridDim.y;
-  if (tflags) {
+  if (S.ip < 0) return;
+  const GroupSeriesDev& G = ser[b];
+  const int yblk = blockIdx.y;
+  if (yblk >= G.ytiles) return;
+  if (tc) {
     int any = 0;
     for (int k = 0; k < S.nk; ++k)
       for (int q = 0; q < kFlagParts; ++q)
-        any |= tflags[((size_t)(b * nz + S.i0 + k) * ytiles + blockIdx.y) * kFlagParts + q];
+        any |= G.tflags[((size_t)(S.i0 + k) * G.ytiles + yblk) * kFlagParts + q];
     if (!any) return;
-  } else if (rowflags[b * ytiles + blockIdx.y] == 0) {
+  } else if (rowflags[b * ytiles_max + yblk] == 0) {
     return;
   }
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (bx >= xb) return;
-  const int ya = blockIdx.y * kApplyTileY, yz = min(yb, ya + kApplyTileY);
-  exact_rows(ser[b].corr, xb, (size_t)xb * yb, bps + S.bp_off, S.i0, S.nk, S.fcos, S.fsin,
-             S.ray_len, S.thick, bx, ya, yz, out + (size_t)b * xb * yb);
+  if (bx >= G.xb) return;
+  const int ya = yblk * kApplyTileY, yz = min(G.yb, ya + kApplyTileY);
+  exact_rows(G.corr, G.xb, G.bpix, bps + S.bp_off, S.i0, S.nk, S.fcos, S.fsin, S.ray_len,
+             S.thick, bx, ya, yz, G.reproj);
 }
 
 int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
-                                 const int* active, int nseries, int nz, int xb, int yb,
-                                 const float* d_bp, const int* tflags, const int* rowflags,
-                                 float* out, cudaStream_t st) {
-  dim3 blk(128, 1), grd((xb + 127) / 128, (yb + kApplyTileY - 1) / kApplyTileY, nseries);
-  k_reproject_exact_group<<<grd, blk, 0, st>>>(ser, steps, active, nz, xb, yb, d_bp, tflags,
-                                               rowflags, out);
+                                 const int* active, int nseries, int xb_max, int ytiles_max,
+                                 const float* d_bp, bool tc, const int* rowflags,
+                                 cudaStream_t st) {
+  dim3 blk(128, 1), grd((xb_max + 127) / 128, ytiles_max, nseries);
+  k_reproject_exact_group<<<grd, blk, 0, st>>>(ser, steps, active, d_bp, tc ? 1 : 0, rowflags,
+                                               ytiles_max);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -692,6 +694,8 @@ int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int ha
   }
   chunk_first[n] = chunks;
   set->total_chunks = chunks;
+  set->nsegs = (int)segs.size();
+  set->nxt = (int)xts.size();
   const size_t chunk_elems = (size_t)kTcM * kTcK;
   MF_TRY(set->op16.alloc(2 * chunk_elems * std::max(chunks, 1)));
   MF_TRY(set->xt.alloc(sizeof(TcXTile) * xts.size()));
@@ -774,6 +778,155 @@ int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int ha
 }
 
 // ---------------------------------------------------------------------------
+// Operators for geometries of several image sizes: one set per size, concatenated.
+static std::vector<std::vector<int>> split_by_shape(const std::vector<ReprojGeom>& geoms) {
+  std::vector<std::vector<int>> parts;
+  std::vector<std::pair<int, int>> shapes;
+  for (int i = 0; i < (int)geoms.size(); ++i) {
+    const std::pair<int, int> sh(geoms[i].xb, geoms[i].yb);
+    size_t k = 0;
+    while (k < shapes.size() && shapes[k] != sh) ++k;
+    if (k == shapes.size()) {
+      shapes.push_back(sh);
+      parts.emplace_back();
+    }
+    parts[k].push_back(i);
+  }
+  return parts;
+}
+
+int build_reproj_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpSet* set,
+                         cudaStream_t st) {
+  const auto parts = split_by_shape(geoms);
+  if (parts.size() <= 1) return build_reproj_ops(c, geoms, set, st);
+  std::vector<ReprojOpSet> sub(parts.size());
+  size_t rows = 0, ntile = 0, ncv = 0;
+  std::vector<size_t> row_off, tile_off, cv_off;
+  for (size_t p = 0; p < parts.size(); ++p) {
+    std::vector<ReprojGeom> g;
+    for (int i : parts[p]) g.push_back(geoms[i]);
+    MF_TRY(build_reproj_ops(c, g, &sub[p], st));
+    row_off.push_back(rows);
+    tile_off.push_back(ntile);
+    cv_off.push_back(ncv);
+    for (const ReprojOpView& v : sub[p].ops) rows += v.total_rows;
+    ntile += (size_t)sub[p].ops.size() * sub[p].ops[0].ntiles;
+    ncv += (size_t)sub[p].ops.size() * sub[p].ops[0].xb;
+  }
+  MF_TRY(set->coef.alloc(sizeof(float) * rows * kOpTileX));
+  MF_TRY(set->rowmap.alloc(sizeof(int2) * rows));
+  MF_TRY(set->tiles.alloc(sizeof(OpTile) * ntile));
+  MF_TRY(set->colvalid.alloc(sizeof(int) * ncv));
+  set->ops.assign(geoms.size(), ReprojOpView());
+  set->bytes = 0;
+  set->fma = 0;
+  for (size_t p = 0; p < parts.size(); ++p) {
+    const ReprojOpSet& q = sub[p];
+    size_t prow = 0;
+    for (const ReprojOpView& v : q.ops) prow += v.total_rows;
+    const int nt = q.ops[0].ntiles, xb = q.ops[0].xb;
+    const size_t pt = q.ops.size() * (size_t)nt;
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->coef.as<float>() + row_off[p] * kOpTileX, q.coef.p,
+                                  sizeof(float) * prow * kOpTileX, cudaMemcpyDeviceToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->rowmap.as<int2>() + row_off[p], q.rowmap.p,
+                                  sizeof(int2) * prow, cudaMemcpyDeviceToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->colvalid.as<int>() + cv_off[p], q.colvalid.p,
+                                  sizeof(int) * q.ops.size() * xb, cudaMemcpyDeviceToDevice, st));
+    std::vector<OpTile> t(pt);
+    MF_CHECK_CUDA(cudaMemcpyAsync(t.data(), q.tiles.p, sizeof(OpTile) * pt,
+                                  cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaStreamSynchronize(st));
+    for (OpTile& x : t) x.row0 += (int)row_off[p];
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->tiles.as<OpTile>() + tile_off[p], t.data(),
+                                  sizeof(OpTile) * pt, cudaMemcpyHostToDevice, st));
+    for (size_t li = 0; li < parts[p].size(); ++li) {
+      ReprojOpView v = q.ops[li];
+      v.coef = set->coef.as<float>();
+      v.rowmap = set->rowmap.as<int2>();
+      v.tiles = set->tiles.as<OpTile>() + tile_off[p] + li * nt;
+      v.colvalid = set->colvalid.as<int>() + cv_off[p] + li * xb;
+      set->ops[parts[p][li]] = v;
+    }
+    set->bytes += q.bytes;
+    set->fma += q.fma;
+  }
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+int build_reproj_tc_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
+                            TcOpSet* set, cudaStream_t st) {
+  const auto parts = split_by_shape(geoms);
+  if (parts.size() <= 1) return build_reproj_tc_ops(c, geoms, half_kind, set, st);
+  std::vector<TcOpSet> sub(parts.size());
+  int chunks = 0, nsegs = 0, nxt = 0;
+  size_t ncv = 0;
+  std::vector<int> chunk_off, seg_off, xt_off;
+  std::vector<size_t> cv_off;
+  for (size_t p = 0; p < parts.size(); ++p) {
+    std::vector<ReprojGeom> g;
+    for (int i : parts[p]) g.push_back(geoms[i]);
+    MF_TRY(build_reproj_tc_ops(c, g, half_kind, &sub[p], st));
+    chunk_off.push_back(chunks);
+    seg_off.push_back(nsegs);
+    xt_off.push_back(nxt);
+    cv_off.push_back(ncv);
+    chunks += sub[p].total_chunks;
+    nsegs += sub[p].nsegs;
+    nxt += sub[p].nxt;
+    ncv += sub[p].ops.size() * (size_t)sub[p].ops[0].xb;
+  }
+  const size_t chunk_bytes = (size_t)kTcM * kTcK * 2;
+  MF_TRY(set->op16.alloc(chunk_bytes * std::max(chunks, 1)));
+  MF_TRY(set->segs.alloc(sizeof(TcSeg) * std::max(nsegs, 1)));
+  MF_TRY(set->xt.alloc(sizeof(TcXTile) * std::max(nxt, 1)));
+  MF_TRY(set->colvalid.alloc(sizeof(int) * ncv));
+  set->ops.assign(geoms.size(), TcOpView());
+  set->total_chunks = chunks;
+  set->nsegs = nsegs;
+  set->nxt = nxt;
+  set->half_kind = half_kind;
+  set->bytes = 0;
+  set->fma = 0;
+  for (size_t p = 0; p < parts.size(); ++p) {
+    const TcOpSet& q = sub[p];
+    const int ntx = q.ops[0].ntx, xb = q.ops[0].xb;
+    if (q.total_chunks > 0)
+      MF_CHECK_CUDA(cudaMemcpyAsync((char*)set->op16.p + chunk_bytes * chunk_off[p], q.op16.p,
+                                    chunk_bytes * q.total_chunks, cudaMemcpyDeviceToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->colvalid.as<int>() + cv_off[p], q.colvalid.p,
+                                  sizeof(int) * q.ops.size() * xb, cudaMemcpyDeviceToDevice, st));
+    std::vector<TcSeg> sg(q.nsegs);
+    std::vector<TcXTile> xt(q.nxt);
+    if (q.nsegs > 0)
+      MF_CHECK_CUDA(cudaMemcpyAsync(sg.data(), q.segs.p, sizeof(TcSeg) * q.nsegs,
+                                    cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(xt.data(), q.xt.p, sizeof(TcXTile) * q.nxt,
+                                  cudaMemcpyDeviceToHost, st));
+    MF_CHECK_CUDA(cudaStreamSynchronize(st));
+    for (TcSeg& x : sg) x.chunk0 += chunk_off[p];
+    for (TcXTile& x : xt) x.seg0 += seg_off[p];
+    if (q.nsegs > 0)
+      MF_CHECK_CUDA(cudaMemcpyAsync(set->segs.as<TcSeg>() + seg_off[p], sg.data(),
+                                    sizeof(TcSeg) * q.nsegs, cudaMemcpyHostToDevice, st));
+    MF_CHECK_CUDA(cudaMemcpyAsync(set->xt.as<TcXTile>() + xt_off[p], xt.data(),
+                                  sizeof(TcXTile) * q.nxt, cudaMemcpyHostToDevice, st));
+    for (size_t li = 0; li < parts[p].size(); ++li) {
+      TcOpView v = q.ops[li];
+      v.xt = set->xt.as<TcXTile>() + xt_off[p] + li * ntx;
+      v.segs = set->segs.as<TcSeg>();
+      v.colvalid = set->colvalid.as<int>() + cv_off[p] + li * xb;
+      set->ops[parts[p][li]] = v;
+    }
+    set->bytes += q.bytes;
+    set->fma += q.fma;
+  }
+  MF_TRY(tc_op_map(set));
+  MF_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Operator apply: out[y][x] = sum_r A[y][r] * B_t[r][x] with A gathered from the
 // neighbour rows through rowmap.  One CTA computes a kApplyTileY x kOpTileX
 // (128 x 64) output tile with 256 threads, each an 8 x 4 register tile.  Operator
@@ -791,14 +944,18 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
                int* __restrict__ rowflags, float* __restrict__ out,
                const ApplyJob* __restrict__ jobs, const int* __restrict__ active) {
   if (jobs) {
-    // group form: blockIdx.z selects the series
+    // group form: blockIdx.z selects the series, with its own size
     if (active && active[blockIdx.z] == 0) return;
     const ApplyJob J = jobs[blockIdx.z];
+    if ((int)blockIdx.x >= J.ntiles || (int)blockIdx.y * kApplyTileY >= J.yb) return;
     corr = J.corr;
     tiles = J.tiles;
     colvalid = J.colvalid;
     rowflags = J.rowflags;
     out = J.out;
+    xb = J.xb;
+    yb = J.yb;
+    pix = (size_t)J.xb * J.yb;
   }
   __shared__ __align__(16) float As[2][kOpChunk][kApplyTileY];
   __shared__ __align__(16) float Bs[2][kOpChunk][kOpTileX];
@@ -897,12 +1054,11 @@ int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr
 }
 
 int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
-                                 const int* active, int njobs, int xb, int yb, int ntiles,
+                                 const int* active, int njobs, int ntiles_max, int yb_max,
                                  cudaStream_t st) {
-  dim3 grd(ntiles, (yb + kApplyTileY - 1) / kApplyTileY, njobs);
-  k_op_apply<<<grd, 256, 0, st>>>(nullptr, xb, yb, (size_t)xb * yb, set.coef.as<float>(),
-                                  set.rowmap.as<int2>(), nullptr, nullptr, nullptr, nullptr,
-                                  d_jobs, active);
+  dim3 grd(ntiles_max, (yb_max + kApplyTileY - 1) / kApplyTileY, njobs);
+  k_op_apply<<<grd, 256, 0, st>>>(nullptr, 0, 0, 0, set.coef.as<float>(), set.rowmap.as<int2>(),
+                                  nullptr, nullptr, nullptr, nullptr, d_jobs, active);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

@@ -134,7 +134,10 @@ int projalign_doit(mf_series* s, float* max_err);
 int coarse_align(mf_series* s, float pitch_angle, float offset);
 int proj_align(mf_series* s, float zshift, int align_z, int nproj, int* passes);
 int correct_stack_device(mf_series* s, int out_bin, float* d_out);
-// groups (mf_batch.cu): all series in `ctx`, same shape and precision
+// groups (mf_batch.cu): series of one context and precision, of any shapes;
+// align_z per series in the first form, shared in the second
+int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift,
+                 const int* align_z, int nproj, mf_group** out);
 int group_create(mf_context* ctx, mf_series* const* series, int nser, float zshift, int align_z,
                  int nproj, mf_group** out);
 int group_proj_align(mf_group* g, int* passes);

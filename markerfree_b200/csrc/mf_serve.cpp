@@ -1,6 +1,6 @@
 // Serving loop: tilt series arrive as requests, are admitted against a device
 // memory budget, prepared (upload, pre-processing, coarse alignment) and then
-// projection-matched in groups of series of the same shape (continuous batching).
+// projection-matched in groups of series of any shapes (continuous batching).
 //
 // The reference aligns exactly one series per process run (Markerfree/src/main/
 // Process.cpp:34-92).  Here a pool of worker threads, each with its own stream
@@ -9,10 +9,12 @@
 //     bytes of all admitted requests stay within the budget;
 //   * prepare: an admitted request is uploaded, pre-processed and coarse-aligned
 //     (PreProcess, Transform, CalcTIltAxis, FindOffset) on the worker's stream;
-//   * match: prepared requests of one shape are taken together as a group (up to
-//     max_group, or fewer when no more of that shape is on its way, or when the
-//     oldest has waited group_wait_ms) and run through projection matching, the
-//     aligned-stack correction and the parameter read-out.
+//   * match: prepared requests that share the options a group applies to all its
+//     series (precision, -p, z shift) are taken together as a group -- of any
+//     image sizes, tilt counts and slab thicknesses -- (up to max_group, or fewer
+//     when no more such requests are on their way, or when the oldest has waited
+//     group_wait_ms) and run through projection matching, the aligned-stack
+//     correction and the parameter read-out.
 // Work of different workers overlaps on the GPU; a request that arrives while
 // others run is admitted as soon as memory frees up.  Each request's result is
 // the one it gets when aligned alone (groups keep per-series arithmetic).
@@ -57,12 +59,12 @@ struct Job {
   double t_submit = 0, t_admit = 0, t_ready = 0, t_done = 0;
 };
 
-// Requests that may share a group: same shape and the same options of the
-// projection-matching stage (which a group applies to all its series).
+// Requests that may share a group: the same options of the projection-matching
+// stage that a group applies to all its series (any image size, tilt count and
+// slab thickness may mix).
 std::vector<float> group_key(const Job* j) {
-  return {(float)j->nx,          (float)j->ny,        (float)j->nz,
-          (float)j->opt.precision, (float)j->opt.align_z, (float)j->opt.nproj,
-          j->opt.zshift,         (float)j->opt.out_bin};
+  return {(float)j->opt.precision, (float)(j->opt.align_z != 0), (float)j->opt.nproj,
+          j->opt.zshift};
 }
 
 // Device bytes a request may hold at its peak: the pre-processed stack, the
@@ -123,7 +125,7 @@ struct mf_server {
     group->clear();
     *wait_s = 0.25;
     const double t = now_s();
-    // ready jobs grouped by shape and by the options a group shares, oldest first
+    // ready jobs grouped by the options a group shares, oldest first
     std::map<std::vector<float>, std::vector<Job*>> by_shape;
     for (Job* j : ready) by_shape[group_key(j)].push_back(j);
     auto coming = [&](const std::vector<float>& key) {
@@ -150,7 +152,7 @@ struct mf_server {
     for (auto& kv : by_shape)
       if ((int)kv.second.size() >= max_group || t - kv.second.front()->t_ready >= starve_s)
         return take(kv.second);
-    // 2. preparing admitted jobs comes next: it lets same-shape jobs join the
+    // 2. preparing admitted jobs comes next: it lets more jobs join the
     //    ready groups, so the matching that follows runs on larger groups
     if (!admitted.empty()) {
       *prep = admitted.front();
@@ -160,7 +162,7 @@ struct mf_server {
       return true;
     }
     // 3. with nothing to prepare, a group runs once it has waited the grouping
-    //    window or no job of its shape is on the way
+    //    window or no job of its kind is on the way
     for (auto& kv : by_shape) {
       std::vector<Job*>& v = kv.second;
       const bool waited = t - v.front()->t_ready >= group_wait_s;
@@ -230,10 +232,11 @@ struct mf_server {
         ss.push_back(j->s);
       }
       const mf_options& o = group[0]->opt;
-      std::vector<int> passes(group.size(), 0);
+      std::vector<int> passes(group.size(), 0), align_z;
+      for (Job* j : group) align_z.push_back(j->opt.align_z);
       if (o.align_z != 0) {
         mf_group* g = nullptr;
-        rc = group_create(ctx, ss.data(), (int)ss.size(), o.zshift, o.align_z, o.nproj, &g);
+        rc = group_create(ctx, ss.data(), (int)ss.size(), o.zshift, align_z.data(), o.nproj, &g);
         if (rc == MF_OK) rc = group_proj_align(g, passes.data());
         delete g;
       }

@@ -202,17 +202,102 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
   return MF_OK;
 }
 
-int norm_mask_pad_group(Context* c, const float* const* d_ptrs, const int* active, int nimg,
-                        int w, int h, int pad, size_t dst_img_stride, float cx, float cy,
-                        float msx, float msy, float power, const float* mask, float* dst,
-                        double2* d_part, float2* d_stats, cudaStream_t st) {
-  const int nb = moment_parts(h);
-  const ImgTable tab{d_ptrs, active};
-  k_moments<<<dim3(nb, nimg), 256, 0, st>>>(nullptr, nullptr, w, h, w, 0, d_part, tab);
-  k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, 0, d_stats);
-  dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
-  k_norm_mask<<<grd, blk, 0, st>>>(nullptr, nullptr, w, 0, w, h, pad, dst_img_stride, d_stats,
-                                   cx, cy, msx, msy, power, mask, dst, tab);
+// Group form of PANorm for one step: image 2b is series b's re-projection, image
+// 2b+1 its held-out projection (corr + ip * bpix), each with its series' size,
+// mask and buffers; the arithmetic and its order are norm_mask_pad's.
+__device__ __forceinline__ const float* group_image(const GroupSeriesDev& S, const GroupStepDev& T,
+                                                    int img) {
+  return (img & 1) ? S.corr + (size_t)T.ip * S.bpix : S.reproj;
+}
+
+__global__ void __launch_bounds__(256) k_moments_group(const GroupSeriesDev* __restrict__ ser,
+                                                       const GroupStepDev* __restrict__ steps,
+                                                       const int* __restrict__ active) {
+  const int img = blockIdx.y, b = img >> 1;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const GroupStepDev T = steps[b];
+  const int nblk = (S.yb + kMomRows - 1) / kMomRows;  // moment_parts(yb)
+  if (T.ip < 0 || (int)blockIdx.x >= nblk) return;
+  const float* p = group_image(S, T, img);
+  const int w = S.xb, h = S.yb;
+  double a = 0.0, bb = 0.0;
+  const int y0 = blockIdx.x * kMomRows, nrows = min(h - y0, kMomRows);
+  const int npair = w >> 1;
+  for (int q = threadIdx.x; q < npair; q += blockDim.x) {
+    float2 v[kMomRows];
+#pragma unroll
+    for (int k = 0; k < kMomRows; ++k)
+      v[k] = k < nrows ? __ldg(reinterpret_cast<const float2*>(p + (size_t)(y0 + k) * w) + q)
+                       : make_float2(-1e30f, -1e30f);
+#pragma unroll
+    for (int k = 0; k < kMomRows; ++k) {
+      moment_add(v[k].x, &a, &bb);
+      moment_add(v[k].y, &a, &bb);
+    }
+  }
+  if ((w & 1) && threadIdx.x == 0)
+    for (int k = 0; k < nrows; ++k) moment_add(__ldg(p + (size_t)(y0 + k) * w + w - 1), &a, &bb);
+  double2 s2 = block_sum2(a, bb);
+  if (threadIdx.x == 0) S.mpart[(size_t)(img & 1) * nblk + blockIdx.x] = s2;
+}
+
+__global__ void __launch_bounds__(256) k_moments_final_group(
+    const GroupSeriesDev* __restrict__ ser, const GroupStepDev* __restrict__ steps,
+    const int* __restrict__ active) {
+  const int img = blockIdx.x, b = img >> 1;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  if (steps[b].ip < 0) return;
+  const int nblk = (S.yb + kMomRows - 1) / kMomRows;  // moment_parts(yb)
+  const double2* p = S.mpart + (size_t)(img & 1) * nblk;
+  double a0 = 0.0, b0 = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    a0 += p[i].x;
+    b0 += p[i].y;
+  }
+  double2 s2 = block_sum2(a0, b0);
+  if (threadIdx.x != 0) return;
+  double n = (double)S.xb * (double)S.yb;
+  S.stats[img & 1] = make_float2((float)(s2.x / n), 1.0f);  // PANorm: std = 1
+}
+
+__global__ void k_norm_mask_group(const GroupSeriesDev* __restrict__ ser,
+                                  const GroupStepDev* __restrict__ steps,
+                                  const int* __restrict__ active) {
+  const int img = blockIdx.z, b = img >> 1;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const GroupStepDev T = steps[b];
+  if (T.ip < 0) return;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int w = S.xb, pad = S.pad;
+  if (x >= pad || y >= S.yb) return;
+  float* d = S.cc + (size_t)(img & 1) * S.ppix + (size_t)y * pad + x;
+  if (x >= w) {
+    *d = 0.0f;
+    return;
+  }
+  float v = group_image(S, T, img)[(size_t)y * w + x];
+  const float2 st = S.stats[img & 1];
+  if (!(v < -1e10f)) v = __fsub_rn(v, st.x);  // GNormalize with std 1
+  if (v < -1e10f) {
+    *d = 0.0f;
+    return;
+  }
+  const float fr = __ldg(S.mask + (size_t)y * w + x);
+  *d = fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
+}
+
+int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                        const int* active, int nseries, int xb_max, int yb_max, int pad_max,
+                        cudaStream_t st) {
+  (void)xb_max;
+  k_moments_group<<<dim3(moment_parts(yb_max), 2 * nseries), 256, 0, st>>>(ser, steps, active);
+  k_moments_final_group<<<2 * nseries, 256, 0, st>>>(ser, steps, active);
+  dim3 blk(64, 4), grd((pad_max + 63) / 64, (yb_max + 3) / 4, 2 * nseries);
+  k_norm_mask_group<<<grd, blk, 0, st>>>(ser, steps, active);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -258,6 +343,51 @@ __global__ void k_xcorr_filter(const cufftComplex* __restrict__ ref, size_t ref_
     im = -im;
   }
   *Bp = make_cuComplex(re, im);
+}
+
+// Group form: blockIdx.z = series; its pair's spectra in its cc buffer.
+__global__ void k_xcorr_filter_group(const GroupSeriesDev* __restrict__ ser,
+                                     const GroupStepDev* __restrict__ steps,
+                                     const int* __restrict__ active, float bfactor) {
+  const int b = blockIdx.z;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  if (steps[b].ip < 0) return;
+  const int cmp = S.cmp, ny = S.yb;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cmp || y >= ny) return;
+  size_t i = (size_t)y * cmp + x;
+  const cufftComplex A = reinterpret_cast<const cufftComplex*>(S.cc)[i];
+  cufftComplex* Bp = reinterpret_cast<cufftComplex*>(S.cc + S.ppix) + i;
+  const cufftComplex B = *Bp;
+  float re = __fmaf_rn(A.x, B.x, __fmul_rn(A.y, B.y));
+  float im = __fmaf_rn(A.x, B.y, -__fmul_rn(A.y, B.x));
+  int yy = y;
+  if (yy > ny / 2) yy -= ny;
+  float fnx = __fmul_rn(2.0f, (float)(cmp - 1));
+  float filt = __fdiv_rn(__fmul_rn(-2.0f, bfactor), __fmaf_rn(fnx, fnx, (float)(ny * ny)));
+  float k2 = (float)((unsigned)(x * x) + (unsigned)(yy * yy));
+  filt = expf(__fmul_rn(filt, k2));
+  float amp = sqrtf(__fmaf_rn(re, re, __fmul_rn(im, im)));
+  filt = __fdiv_rn(filt, sqrtf(__fadd_rn(amp, 0.01f)));
+  re = __fmul_rn(re, filt);
+  im = __fmul_rn(im, filt);
+  if ((x + y) & 1) {
+    re = -re;
+    im = -im;
+  }
+  *Bp = make_cuComplex(re, im);
+}
+
+int xcorr_filter_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                       const int* active, int nseries, int cmp_max, int yb_max, float bfactor,
+                       cudaStream_t st) {
+  dim3 blk(64, 4), grd((cmp_max + 63) / 64, (yb_max + 3) / 4, nseries);
+  k_xcorr_filter_group<<<grd, blk, 0, st>>>(ser, steps, active, bfactor);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
 }
 
 int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,
@@ -482,41 +612,77 @@ __global__ void k_pa_peak_update(const float* __restrict__ map, int stride, int 
             meas);
 }
 
-// Group form: blockIdx.x = series b, map b at maps + b * map_stride, partials
-// part + b * nparts.
-__global__ void k_pa_peak_update_group(const float* __restrict__ maps, size_t map_stride,
-                                       int stride, int xb, int yb,
-                                       const float2* __restrict__ part, int nparts,
-                                       const GroupSeriesDev* __restrict__ ser,
-                                       const GroupStepDev* __restrict__ steps,
-                                       const int* __restrict__ active, int nx, int ny) {
-  const int b = blockIdx.x;
+// Group form of the peak search: blockIdx.y = series; its correlation map (the
+// second image of its cc buffer), its own search window, partials in its ppart.
+__global__ void __launch_bounds__(256) k_peak_partial_group(
+    const GroupSeriesDev* __restrict__ ser, const GroupStepDev* __restrict__ steps,
+    const int* __restrict__ active) {
+  __shared__ float sv[256];
+  __shared__ int si[256];
+  const int b = blockIdx.y;
   if (active && active[b] == 0) return;
-  const float* map = maps + (size_t)b * map_stride;
-  float bv;
-  int bi;
-  reduce_partials(part + (size_t)b * nparts, nparts, &bv, &bi);
-  if (threadIdx.x != 0) return;
   const GroupSeriesDev& S = ser[b];
-  const int ip = steps[b].ip;
-  int px = 0, py = 0;
-  pa_window_peak(bi, stride, xb, yb, &px, &py);
-  pa_update(map, stride, xb, yb, px, py, ip, nx, ny, S.angles, S.sx, S.sy, S.sx64, S.sy64, S.rot,
-            *S.z0, S.err, S.meas);
-}
-
-int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,
-                         int yb, float2* d_part, const GroupSeriesDev* ser,
-                         const GroupStepDev* steps, const int* active, int nseries, int nx,
-                         int ny, cudaStream_t st) {
+  if (steps[b].ip < 0) return;
+  const int xb = S.xb, yb = S.yb, stride = S.pad;
   int sx = xb / 20, sy = yb / 20;
   if (sx < 3) sx = 3;
   if (sy < 3) sy = 3;
+  const int ex = xb - sx, ey = yb - sy;
+  const float* m = S.cc + S.ppix;
+  const int rows = ey - sy;
+  const int r0 = sy + (int)((long long)rows * blockIdx.x / gridDim.x);
+  const int r1 = sy + (int)((long long)rows * (blockIdx.x + 1) / gridDim.x);
+  float bv = -INFINITY;
+  int bi = INT_MAX;
+  for (int y = r0; y < r1; ++y) {
+#pragma unroll 4
+    for (int x = sx + threadIdx.x; x < ex; x += blockDim.x) {
+      int li = y * stride + x;
+      float v = __ldg(m + li);
+      if (better(v, li, bv, bi)) {
+        bv = v;
+        bi = li;
+      }
+    }
+  }
+  sv[threadIdx.x] = bv;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h && better(sv[threadIdx.x + h], si[threadIdx.x + h], sv[threadIdx.x],
+                                  si[threadIdx.x])) {
+      sv[threadIdx.x] = sv[threadIdx.x + h];
+      si[threadIdx.x] = si[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) S.ppart[blockIdx.x] = make_float2(sv[0], __int_as_float(si[0]));
+}
+
+// Group form of the peak + ClacAlignProj update: blockIdx.x = series b.
+__global__ void k_pa_peak_update_group(const GroupSeriesDev* __restrict__ ser,
+                                       const GroupStepDev* __restrict__ steps,
+                                       const int* __restrict__ active, int nparts) {
+  const int b = blockIdx.x;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const int ip = steps[b].ip;
+  if (ip < 0) return;
+  float bv;
+  int bi;
+  reduce_partials(S.ppart, nparts, &bv, &bi);
+  if (threadIdx.x != 0) return;
+  int px = 0, py = 0;
+  pa_window_peak(bi, S.pad, S.xb, S.yb, &px, &py);
+  pa_update(S.cc + S.ppix, S.pad, S.xb, S.yb, px, py, ip, S.nx, S.ny, S.angles, S.sx, S.sy,
+            S.sx64, S.sy64, S.rot, *S.z0, S.err, S.meas);
+}
+
+int pa_peak_update_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                         const int* active, int nseries, cudaStream_t st) {
   const int nb = kPeakParts;
-  k_peak_partial<<<dim3(nb, nseries), 256, 0, st>>>(maps, map_stride, stride, sx, xb - sx, sy,
-                                                    yb - sy, d_part);
-  k_pa_peak_update_group<<<nseries, 32, 0, st>>>(maps, map_stride, stride, xb, yb, d_part, nb,
-                                                 ser, steps, active, nx, ny);
+  k_peak_partial_group<<<dim3(nb, nseries), 256, 0, st>>>(ser, steps, active);
+  k_pa_peak_update_group<<<nseries, 32, 0, st>>>(ser, steps, active, nb);
   c->launches += 2;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
@@ -632,37 +798,37 @@ __global__ void k_fit_z0(int nz, int zt, const float* __restrict__ angles, float
 }
 
 __global__ void k_fit_z0_group(const GroupSeriesDev* __restrict__ ser,
-                               const int* __restrict__ active, int nz) {
+                               const int* __restrict__ active) {
   const int b = blockIdx.x;
   if (threadIdx.x != 0 || (active && active[b] == 0)) return;
   const GroupSeriesDev& S = ser[b];
-  fit_z0_one(nz, S.zt, S.angles, S.sx, S.sy, S.sx64, S.sy64, S.rot, S.z0);
+  fit_z0_one(S.nz, S.zt, S.angles, S.sx, S.sy, S.sx64, S.sy64, S.rot, S.z0);
 }
 
 // max over err[order[i]] (the DoIt return value), initial -1e20, per series
 __global__ void k_max_err_group(const GroupSeriesDev* __restrict__ ser,
-                                const int* __restrict__ active, int n, float* out) {
+                                const int* __restrict__ active, float* out) {
   const int b = blockIdx.x;
   if (threadIdx.x != 0 || (active && active[b] == 0)) return;
   float m = -1e20f;
-  for (int i = 0; i < n; ++i) {
+  for (int i = 0; i < ser[b].n; ++i) {
     float e = ser[b].err[ser[b].order[i]];
     if (e > m) m = e;
   }
   out[b] = m;
 }
 
-int fit_z0_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int nz,
+int fit_z0_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries,
                  cudaStream_t st) {
-  k_fit_z0_group<<<nseries, 32, 0, st>>>(ser, active, nz);
+  k_fit_z0_group<<<nseries, 32, 0, st>>>(ser, active);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
 }
 
-int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int n,
+int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries,
                   float* d_out, cudaStream_t st) {
-  k_max_err_group<<<nseries, 32, 0, st>>>(ser, active, n, d_out);
+  k_max_err_group<<<nseries, 32, 0, st>>>(ser, active, d_out);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

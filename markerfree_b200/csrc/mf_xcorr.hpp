@@ -19,20 +19,22 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
 int make_round_mask(Context* c, int w, int h, float cx, float cy, float msx, float msy,
                     float power, float* d_mask, cudaStream_t st);
 int moment_parts(int h);
-// Group form: image i is d_ptrs[i] (w x h, dense rows); image pairs of series with
-// active[i / 2] == 0 are skipped.
-int norm_mask_pad_group(Context* c, const float* const* d_ptrs, const int* active, int nimg,
-                        int w, int h, int pad, size_t dst_img_stride, float cx, float cy,
-                        float msx, float msy, float power, const float* mask, float* dst,
-                        double2* d_part, float2* d_stats, cudaStream_t st);
-// Group forms of the peak + parameter update, FitRotCenterZ and the pass maximum.
-int pa_peak_update_group(Context* c, const float* maps, size_t map_stride, int stride, int xb,
-                         int yb, float2* d_part, const GroupSeriesDev* ser,
-                         const GroupStepDev* steps, const int* active, int nseries, int nx,
-                         int ny, cudaStream_t st);
-int fit_z0_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int nz,
+// Group forms (one launch over the series of a group at one step; each series
+// with its own geometry and buffers, see GroupSeriesDev): PANorm of the pair
+// (re-projection, held-out tilt) into the series' cc buffer; the conjugate
+// product and filter of the pair's spectra; the peak + parameter update;
+// FitRotCenterZ; the pass maximum.
+int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                        const int* active, int nseries, int xb_max, int yb_max, int pad_max,
+                        cudaStream_t st);
+int xcorr_filter_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                       const int* active, int nseries, int cmp_max, int yb_max, float bfactor,
+                       cudaStream_t st);
+int pa_peak_update_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                         const int* active, int nseries, cudaStream_t st);
+int fit_z0_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries,
                  cudaStream_t st);
-int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries, int n,
+int max_err_group(Context* c, const GroupSeriesDev* ser, const int* active, int nseries,
                   float* d_out, cudaStream_t st);
 
 int xcorr_filter(Context* c, const cufftComplex* ref, size_t ref_stride, const int* d_ref_idx,

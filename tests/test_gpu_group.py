@@ -98,3 +98,44 @@ def test_group_pass_with_inactive_series(ctx, mflib):
     qa = ser.get_param()
     assert np.abs(q0.shift_x - qa.shift_x).max() < 1e-3
     assert np.abs(q0.shift_y - qa.shift_y).max() < 1e-3
+
+
+def uneven_set():
+    """Three series that differ in image size, tilt count, tilt range and slab
+    thickness (the uneven batches of many-series alignment)."""
+    return [
+        (synth.make_series(nx=192, ny=160, vol_z=40, n_blobs=70, tilt_min=-42, tilt_max=42,
+                           tilt_step=3.0, axis=85.0, shift_sd=3.0, snr=0.8, seed=71,
+                           thickness=30), 30),
+        (synth.make_series(nx=160, ny=128, vol_z=32, n_blobs=50, tilt_min=-30, tilt_max=30,
+                           tilt_step=3.0, axis=88.0, shift_sd=2.5, snr=1.0, seed=72,
+                           thickness=24), 24),
+        (synth.make_series(nx=256, ny=224, vol_z=48, n_blobs=90, tilt_min=-48, tilt_max=48,
+                           tilt_step=4.0, axis=83.0, shift_sd=3.0, snr=0.7, seed=73,
+                           thickness=40), 40),
+    ]
+
+
+@pytest.mark.parametrize("prec", [0, 2])
+def test_uneven_group_matches_alone(ctx, mflib, prec):
+    """Series of different sizes, tilt counts and thicknesses aligned in one group
+    (one launch per stage over all of them) give what each gets alone."""
+    import torch
+    ss = uneven_set()
+    alone = []
+    for s, az in ss:
+        p, out, passes = mflib.align(ctx, s.stack, s.angles, offset=1e-4, align_z=az, nproj=10,
+                                     want_stack=True, precision=prec)
+        alone.append((p, out, passes))
+    d_raws = [to_dev(s.stack) for s, _ in ss]
+    d_outs = [torch.empty(s.stack.shape, dtype=torch.float32, device="cuda") for s, _ in ss]
+    params, passes = mflib.align_batch_device(ctx, d_raws, [s.angles for s, _ in ss],
+                                              [az for _, az in ss], d_outs, offset=1e-4,
+                                              nproj=10, precision=prec)
+    for i, (p, (pa, out_alone, npa)) in enumerate(zip(params, alone)):
+        assert passes[i] == npa, (i, passes[i], npa)
+        assert np.abs(p.rotate - pa.rotate).max() <= AXIS_TOL
+        assert np.abs(p.shift_x - pa.shift_x).max() <= SHIFT_TOL, i
+        assert np.abs(p.shift_y - pa.shift_y).max() <= SHIFT_TOL, i
+        if np.array_equal(p.shift_x, pa.shift_x) and np.array_equal(p.shift_y, pa.shift_y):
+            assert np.array_equal(d_outs[i].cpu().numpy(), out_alone)
