@@ -288,18 +288,19 @@ def _time_steps(stream, fn, steps):
 
 
 def served_pool(dev):
-    """Distinct seeded series for the serving run, by size class: 2048^2 (the bench
-    workload's generator), 1024^2 and 4096^2 (the same generator at half and double
-    the size; 4096^2 is auto-binned to 2048^2 for matching, as the reference does).
+    """Distinct seeded series for the serving run, by size class (2048^2, 1024^2,
+    4096^2), each drawn like the uneven batch (synth.uneven_params with the size
+    fixed: 31/41/61 tilts, slab 150/200/300, axis, SNR); 4096^2 is auto-binned to
+    2048^2 for matching, as the reference does.
     Returns {class: [(pinned host tensor, angles, thickness), ...]}."""
     import torch
     from markerfree_b200 import synth
     pool = {}
-    for key, scale, count, seed0 in (("2048", 1.0, 4, 3000), ("1024", 0.5, 3, 3100),
-                                     ("4096", 2.0, 2, 3200)):
+    for key, size, count, seed0 in (("2048", 2048, 4, 5000), ("1024", 1024, 3, 5100),
+                                    ("4096", 4096, 2, 5200)):
         out = []
         for j in range(count):
-            s = synth.config_fast(2, seed=seed0 + j, device=f"cuda:{dev}", scale=scale)
+            s = synth.uneven_series(j, f"cuda:{dev}", size=size, seed0=seed0)
             h = torch.empty(s.stack.shape, dtype=torch.float32).pin_memory()
             h.copy_(s.stack)
             out.append((h, s.angles, s.thickness))
@@ -312,8 +313,9 @@ def served_pool(dev):
 def served_run(mf, dev, n_req, precision, seed=5):
     """The serving loop (continuous batching) on the served-request mix: sizes 50%
     2048^2, 30% 1024^2, 20% 4096^2, each request one of a pool of distinct seeded
-    series of its size class, from pinned host memory; results are the per-tilt
-    parameters.
+    series of its size class (tilt counts and slab thicknesses vary too), from
+    pinned host memory; requests of any shape share groups; results are the
+    per-tilt parameters.
 
     Capacity: all n_req requests arrive at once; series/min = n_req / makespan
     (also in 2048^2-equivalents, weighting each request by its pixel count).
@@ -370,6 +372,43 @@ def served_run(mf, dev, n_req, precision, seed=5):
             "precision": {0: "f32", 1: "bf16 operands, f32 accumulation",
                           2: "fp16 operands, f32 accumulation"}[precision],
             "returns": "per-tilt parameters (aligned stacks not copied back)"}
+
+
+def uneven_run(mf, ctx, stream, dev, precisions, n=32, per_call=16, steps=1):
+    """The uneven batch: n distinct seeded series of sizes U{1024..4096}^2, 31/41/61
+    tilts over +-45..60 degrees, slab 150/200/300, axis U(80, 95), SNR
+    U(0.03, 0.2) (synth.uneven_params), raw stacks resident in HBM.  One step
+    aligns all n through mf_align_batch_device, per_call series per call, each
+    call one lockstep group whose every stage is one launch over series of
+    different sizes; no output stacks.  Returns series/min per precision."""
+    import torch
+    from markerfree_b200 import synth
+    series = [synth.uneven_series(j, f"cuda:{dev}") for j in range(n)]
+    torch.cuda.synchronize()
+    out = {"series": n, "per_call": per_call,
+           "sizes": sorted({int(s.stack.shape[2]) for s in series}),
+           "tilts": sorted({int(s.stack.shape[0]) for s in series}),
+           "raw_gb": sum(s.stack.numel() * 4 for s in series) / 1e9}
+    for prec in precisions:
+        passes = []
+
+        def step():
+            passes.clear()
+            for h in range(0, n, per_call):
+                part = series[h:h + per_call]
+                _, ps = mf.align_batch_device(ctx, [s.stack for s in part], [s.angles for s in part],
+                                              [s.thickness for s in part], None, nproj=10,
+                                              precision=PRECISIONS[prec])
+                passes.extend(int(x) for x in ps)
+
+        step()
+        torch.cuda.synchronize()
+        ms = _time_steps(stream, step, steps)
+        out[prec] = {"value": 60000.0 * n / (ms / steps), "unit": "series/min", "steps": steps,
+                     "mean_passes": float(np.mean(passes))}
+    del series
+    torch.cuda.empty_cache()
+    return out
 
 
 def _params_diff(pa, pb):
@@ -591,9 +630,16 @@ def run_ours(args):
             "tc_tuning": ctx.tc_tuning(),
             "stage_ms_per_step": {k: round(v, 2) for k, v in stages.items()},
             "roofline": roof, "roofline_other": others, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_uneven:
+        log("uneven batch")
+        del d_outs
+        torch.cuda.empty_cache()
+        d_outs = None
+        line["uneven_batch"] = uneven_run(mf, ctx, stream, dev, [args.precision, "fp16"])
+        log("uneven batch done")
     if rank == 0 and world == 1 and not args.no_serve:
         log("serving run")
-        del d_outs
+        d_outs = None
         torch.cuda.empty_cache()
         line["served"] = served_run(mf, dev, args.serve_requests, PRECISIONS["fp16"])
         log("serving run done")
@@ -690,6 +736,7 @@ def main():
                     help="skip the fp16/bf16 forms of the batched step")
     ap.add_argument("--batch", type=int, default=8, help="series per group (one step)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch run")
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--kernel-method", type=int, default=1,
                     help="re-projection method of --kernel-case reproject (1 FP32, 2 FP16, 3 BF16)")

@@ -214,3 +214,26 @@ def config_fast(cfg: int, seed: int | None = None, device="cpu", scale: float = 
                                 thickness=max(8, int(300 * scale)) // 2 * 2, name="cfg2",
                                 device=device)
     raise ValueError(f"no fast form of configuration {cfg}")
+
+
+def uneven_params(j: int, size=None, seed0: int = 4000) -> dict:
+    """Parameters of series j of the uneven batch: image size U{1024, 2048, 3072,
+    4096}^2 (or `size`), tilt count U{31, 41, 61} over a range of +-45..+-60
+    degrees, slab thickness U{150, 200, 300}, tilt axis U(80, 95) degrees, shifts
+    N(0, 6 px), SNR U(0.03, 0.2); drawn from a generator seeded with seed0 + j."""
+    rng = np.random.default_rng(seed0 + j)
+    n = int(rng.choice([1024, 2048, 3072, 4096]))
+    if size is not None:
+        n = int(size)
+    tilts = int(rng.choice([31, 41, 61]))
+    rng_deg = float(rng.uniform(45.0, 60.0))
+    return dict(nx=n, ny=n, vol_z=max(32, n * 300 // 2048), n_blobs=max(100, 3000 * n * n // 2048 ** 2),
+                sigma=(1.5, 5.0), tilt_min=-rng_deg, tilt_max=rng_deg, n_tilts=tilts,
+                axis=float(rng.uniform(80.0, 95.0)), shift_sd=6.0, snr=float(rng.uniform(0.03, 0.2)),
+                poisson=True, background=True, seed=seed0 + j,
+                thickness=int(rng.choice([150, 200, 300])), name=f"uneven{j}")
+
+
+def uneven_series(j: int, device="cpu", size=None, seed0: int = 4000) -> Series:
+    """Series j of the uneven batch (uneven_params), generated with make_series_fast."""
+    return make_series_fast(device=device, **uneven_params(j, size=size, seed0=seed0))
