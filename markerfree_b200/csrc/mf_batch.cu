@@ -17,6 +17,7 @@
 // the per-series arithmetic and its order are unchanged.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 
@@ -39,8 +40,10 @@ struct GroupMember {
   TmaDesc imgmap;
   std::vector<int> order;
   int op0 = 0;  // index of this series' first operator in the group's operator set
-  cufftHandle rows_fwd_all = 0, rows_inv_all = 0, rows_fwd_one = 0, rows_inv_one = 0;
-  cufftHandle cc_fwd = 0, cc_inv = 0;
+  cufftHandle rows_fwd_all = 0, rows_inv_all = 0;
+  // the per-step transforms, one plan per side stream of the context
+  static constexpr int kS = mf_context::kFftStreams;
+  cufftHandle rows_fwd_one[kS] = {}, rows_inv_one[kS] = {}, cc_fwd[kS] = {}, cc_inv[kS] = {};
 };
 
 }  // namespace
@@ -372,10 +375,12 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     GroupMember& M = *g->m[b];
     MF_TRY(ctx->plan({0, M.xb, M.yb, (long long)M.nz * M.yb}, &M.rows_fwd_all));
     MF_TRY(ctx->plan({1, M.xb, M.yb, (long long)M.nz * M.yb}, &M.rows_inv_all));
-    MF_TRY(ctx->plan({0, M.xb, M.yb, (long long)M.yb}, &M.rows_fwd_one));
-    MF_TRY(ctx->plan({1, M.xb, M.yb, (long long)M.yb}, &M.rows_inv_one));
-    MF_TRY(ctx->plan({2, M.xb, M.yb, 2}, &M.cc_fwd));
-    MF_TRY(ctx->plan({3, M.xb, M.yb, 1}, &M.cc_inv));
+    for (int i = 0; i < mf_context::kFftStreams; ++i) {
+      MF_TRY(ctx->plan({0, M.xb, M.yb, (long long)M.yb, i}, &M.rows_fwd_one[i]));
+      MF_TRY(ctx->plan({1, M.xb, M.yb, (long long)M.yb, i}, &M.rows_inv_one[i]));
+      MF_TRY(ctx->plan({2, M.xb, M.yb, 2, i}, &M.cc_fwd[i]));
+      MF_TRY(ctx->plan({3, M.xb, M.yb, 1, i}, &M.cc_inv[i]));
+    }
   }
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   return MF_OK;
@@ -415,9 +420,30 @@ static int group_enqueue(mf_group* g) {
   MF_TRY(fit_z0_group(c, ser, active, B, st));
   const bool prof = c->profiling && (int)g->events.size() >= 3 * nmax;
   std::vector<TcJob> jobs;
+  // A per-step FFT stage: the transforms of the series that take part run on the
+  // context's side streams, forked from the stream after the work queued so far
+  // and joined back before the next kernel; each series' own plans, so the
+  // results are those of the transforms run one after another.
+  mf_context* ctx = g->ctx;
+  const int nfs = mf_context::kFftStreams;
+  auto fft_stage = [&](int k, const std::function<int(GroupMember&, int)>& exec) -> int {
+    MF_CHECK_CUDA(cudaEventRecord(ctx->fork_ev, st));
+    int used = 0;
+    for (int b = 0; b < B; ++b) {
+      if (!g->active[b] || k >= g->m[b]->n) continue;
+      const int slot = used % nfs;
+      if (used < nfs) MF_CHECK_CUDA(cudaStreamWaitEvent(ctx->aux[slot], ctx->fork_ev, 0));
+      MF_TRY(exec(*g->m[b], slot));
+      ++used;
+    }
+    for (int i = 0; i < std::min(used, nfs); ++i) {
+      MF_CHECK_CUDA(cudaEventRecord(ctx->join_ev[i], ctx->aux[i]));
+      MF_CHECK_CUDA(cudaStreamWaitEvent(st, ctx->join_ev[i], 0));
+    }
+    return MF_OK;
+  };
   for (int k = 0; k < nmax; ++k) {
     const GroupStepDev* sk = steps + (size_t)k * B;
-    auto takes_part = [&](int b) { return g->active[b] && k < g->m[b]->n; };
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k], st));
     if (tc) {
       jobs.clear();
@@ -437,32 +463,32 @@ static int group_enqueue(mf_group* g) {
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 1], st));
     // MeaAlignProj for every series: PANorm both images, FFT, filter, inverse, peak
     MF_TRY(norm_mask_pad_group(c, ser, sk, active, B, g->xb_max, g->yb_max, g->pad_max, st));
-    for (int b = 0; b < B; ++b)
-      if (takes_part(b)) {
-        float* cb = g->m[b]->cc.as<float>();
-        MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->cc_fwd, cb, (cufftComplex*)cb));
-      }
+    MF_TRY(fft_stage(k, [&](GroupMember& M, int i) -> int {
+      float* cb = M.cc.as<float>();
+      MF_CHECK_CUFFT(cufftExecR2C(M.cc_fwd[i], cb, (cufftComplex*)cb));
+      return MF_OK;
+    }));
     MF_TRY(xcorr_filter_group(c, ser, sk, active, B, g->cmp_max, g->yb_max, 500.0f, st));
-    for (int b = 0; b < B; ++b)
-      if (takes_part(b)) {
-        float* mb = g->m[b]->cc.as<float>() + g->m[b]->ppix;
-        MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->cc_inv, (cufftComplex*)mb, mb));
-      }
+    MF_TRY(fft_stage(k, [&](GroupMember& M, int i) -> int {
+      float* mb = M.cc.as<float>() + M.ppix;
+      MF_CHECK_CUFFT(cufftExecC2R(M.cc_inv[i], (cufftComplex*)mb, mb));
+      return MF_OK;
+    }));
     MF_TRY(pa_peak_update_group(c, ser, sk, active, B, st));
     // re-correct the aligned tilt of every series (mCorrectProj)
     GroupCorrArgs rc{ser, sk, active, g->nz_max, 1};
     MF_TRY(launch_correct_group(c, rc, B, g->xb_max, g->yb_max, st));
-    for (int b = 0; b < B; ++b)
-      if (takes_part(b)) {
-        float* rb = g->m[b]->recorr.as<float>();
-        MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->rows_fwd_one, rb, (cufftComplex*)rb));
-      }
+    MF_TRY(fft_stage(k, [&](GroupMember& M, int i) -> int {
+      float* rb = M.recorr.as<float>();
+      MF_CHECK_CUFFT(cufftExecR2C(M.rows_fwd_one[i], rb, (cufftComplex*)rb));
+      return MF_OK;
+    }));
     MF_TRY(launch_rweight_group(c, ser, sk, active, B, g->cmp_max, g->yb_max, st));
-    for (int b = 0; b < B; ++b)
-      if (takes_part(b))
-        MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->rows_inv_one,
-                                    (cufftComplex*)g->m[b]->recorr.as<float>(),
-                                    g->m[b]->recorr_out.as<float>()));
+    MF_TRY(fft_stage(k, [&](GroupMember& M, int i) -> int {
+      MF_CHECK_CUFFT(cufftExecC2R(M.rows_inv_one[i], (cufftComplex*)M.recorr.as<float>(),
+                                  M.recorr_out.as<float>()));
+      return MF_OK;
+    }));
     k_group_scatter<<<dim3(64, B), 256, 0, st>>>(ser, sk, active);
     c->launches++;
     MF_CHECK_CUDA(cudaGetLastError());

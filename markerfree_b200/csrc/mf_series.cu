@@ -34,7 +34,22 @@ mf_context::~mf_context() {
   std::lock_guard<std::recursive_mutex> lk(fft_mutex());
   for (auto& kv : plans) cufftDestroy(kv.second);
   plans.clear();
+  for (int i = 0; i < kFftStreams; ++i) {
+    if (aux[i]) cudaStreamDestroy(aux[i]);
+    if (join_ev[i]) cudaEventDestroy(join_ev[i]);
+  }
+  if (fork_ev) cudaEventDestroy(fork_ev);
   if (c.stream) cudaStreamDestroy(c.stream);
+}
+
+int mf_context::ensure_aux() {
+  if (fork_ev) return MF_OK;
+  for (int i = 0; i < kFftStreams; ++i) {
+    MF_CHECK_CUDA(cudaStreamCreateWithFlags(&aux[i], cudaStreamNonBlocking));
+    MF_CHECK_CUDA(cudaEventCreateWithFlags(&join_ev[i], cudaEventDisableTiming));
+  }
+  MF_CHECK_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  return MF_OK;
 }
 
 int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
@@ -85,7 +100,16 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   if (r != CUFFT_SUCCESS)
     return set_error(MF_ERR_CUFFT, "cufftPlanMany(kind %lld, %d x %d, batch %d) failed: %d", kind,
                      nx, ny, batch, (int)r);
-  cufftSetStream(h, c.stream);
+  cudaStream_t bind = c.stream;
+  if (key.size() > 4 && key[4] >= 0) {
+    if (key[4] >= kFftStreams) {
+      cufftDestroy(h);
+      return set_error(MF_ERR_ARG, "FFT side stream %lld out of range", key[4]);
+    }
+    MF_TRY(ensure_aux());
+    bind = aux[key[4]];
+  }
+  cufftSetStream(h, bind);
   plans[key] = h;
   *out = h;
   return MF_OK;

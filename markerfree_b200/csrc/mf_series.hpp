@@ -13,9 +13,17 @@ struct mf_context {
     mf::DevBuf a, b, c, d;
   } scratch;
   std::map<std::vector<long long>, cufftHandle> plans;
+  // Side streams that run the per-series cuFFT calls of one group stage side by
+  // side (each with plans of its own, so that no work area is shared), forked
+  // from and joined back into the context stream with the events below.
+  static constexpr int kFftStreams = 4;
+  cudaStream_t aux[kFftStreams] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kFftStreams] = {};
   ~mf_context();
-  // Plan cache keyed by (kind, sizes, batch, layout); bound to the context stream.
+  // Plan cache keyed by (kind, sizes, batch); bound to the context stream, or with
+  // a fifth key entry i >= 0 to side stream i.
   int plan(const std::vector<long long>& key, cufftHandle* out);
+  int ensure_aux();  // creates the side streams and events on first use
 };
 
 namespace mf {

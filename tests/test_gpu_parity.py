@@ -301,3 +301,71 @@ def test_preprocessed_stack_entry_point(ctx, mflib, series):
     assert np.array_equal(pa.shift_x, pb.shift_x) and np.array_equal(pa.shift_y, pb.shift_y)
     with pytest.raises(mflib.MfError):
         mflib.Series(ctx, st, np.sort(series.angles)[::-1].copy(), preprocessed=True)
+
+
+def oracle_passes_cuda_trig(ctx, st, angles, rot, thick, npass, nproj=10):
+    """The oracle's projection-matching passes with CUDA's cosf/sinf registered for
+    every argument they evaluate (the reference's device code calls them; the
+    oracle's own trigonometry is correctly rounded, and a last-place difference
+    moves nearest-neighbour indices).  The arguments depend on the shifts, so the
+    registration is repeated until the passes evaluate no new argument.
+    Returns [(max error, shift_x, shift_y, z0, measured)] per pass."""
+    nz = st.shape[0]
+    known = np.zeros(0, np.float32)
+    for _ in range(4):
+        if known.size:
+            O.trig_set(known, *ctx.device_cos_sin(known))
+        try:
+            with O.trig_recording() as rec:
+                po = O.Param(nz)
+                po.rotate[:] = rot
+                pa = O.ProjAlign(st, angles, po, 0.0, thick, nproj)
+                out = []
+                for _ in range(npass):
+                    e = pa.doit()
+                    out.append((e, po.shift_x.copy(), po.shift_y.copy(), pa.z0,
+                                pa.measured().copy()))
+        finally:
+            O.trig_clear()
+        args = np.union1d(known, rec.args).astype(np.float32)
+        if args.size == known.size:
+            return out
+        known = args
+    return out
+
+
+def smoke_series():
+    return synth.make_series(nx=128, ny=128, vol_z=32, n_blobs=40, tilt_step=4.0, axis=86.0,
+                             shift_sd=2.0, snr=1.0, seed=42, thickness=24), 24
+
+
+def bin2_series():
+    """3072 px wide: the reference bins projection matching by 2 (ProjAlign.cpp:57-61;
+    round(3072 / 2048) = 2) and halves the slab (100 -> 50)."""
+    return synth.make_series(nx=3072, ny=320, vol_z=64, n_blobs=240, seed=1301, snr=4.0,
+                             shift_sd=3.0, axis=87.0, tilt_min=-40, tilt_max=40,
+                             tilt_step=4.0, thickness=100), 100
+
+
+@pytest.mark.parametrize("make", [smoke_series, bin2_series], ids=["smoke128", "bin2_3072"])
+def test_projalign_passes_match_oracle_with_device_trig(ctx, mflib, make):
+    """Two projection-matching passes on the GPU against the oracle given CUDA's
+    cosf/sinf: every per-tilt shift, the pass maximum and the rotation centre within
+    0.02 px.  The 3072-px series runs the reference's bin-2 matching."""
+    s, thick = make()
+    nz = s.stack.shape[0]
+    st = O.preprocess(s.stack, s.angles)
+    ser = mflib.Series(ctx, s.stack, s.angles)
+    p = mflib.Param(nz)
+    p.rotate[:] = s.axis
+    ser.set_param(p)
+    ser.projalign_setup(0.0, thick, 10)
+    want = oracle_passes_cuda_trig(ctx, st, s.angles, s.axis, thick, 2)
+    for k, (e_o, sx, sy, z0, _) in enumerate(want):
+        e_g = ser.projalign_doit()
+        g = ser.get_param()
+        dx = float(np.abs(g.shift_x - sx).max())
+        dy = float(np.abs(g.shift_y - sy).max())
+        print(f"pass {k}: max shift {e_g:.4f} / {e_o:.4f}; shift differences {dx:.4f}, {dy:.4f}")
+        assert abs(e_g - e_o) < 0.02 and abs(ser.z0 - z0) < 0.02
+        assert dx < 0.02 and dy < 0.02
