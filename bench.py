@@ -487,11 +487,11 @@ def run_ours(args):
     log("batched timing done")
     # e2e through the C ABI with host buffers: per step B uploads from pinned memory,
     # the group alignment, B downloads of the aligned stacks
-    h_raws = []
-    for d in d_raws:
-        h = torch.empty(d.shape, dtype=torch.float32).pin_memory()
-        h.copy_(d)
-        h_raws.append(h)
+    # (built without loop variables: a pinned buffer still referenced when the
+    # context's stream is gone would record its release on a destroyed stream)
+    h_raws = [torch.empty(d.shape, dtype=torch.float32).pin_memory() for d in d_raws]
+    for i in range(B):
+        h_raws[i].copy_(d_raws[i])
     h_out = torch.empty((nz, yo, xo), dtype=torch.float32).pin_memory()
     d_ins = [torch.empty_like(d_raws[0]) for _ in range(B)]
 

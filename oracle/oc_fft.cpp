@@ -1,7 +1,9 @@
 // Double-precision FFT for the CPU oracle.  See oc_fft.hpp for conventions.
 #include "oc_fft.hpp"
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -156,11 +158,41 @@ void fft_c2c(cd* data, int n, int sign) {
   mixed_radix(data, n, sign, scratch);
 }
 
+// Perturbation of every transform's output at the size of single-precision
+// rounding (a sensitivity probe, off unless a test sets a seed): each output value
+// v becomes v (1 + e), |e| <= 2^-24 sqrt(log2 n), e drawn from a hash of the seed,
+// the value's bits and its index, so it is deterministic and thread-safe.
+static unsigned long long g_perturb_seed = 0;
+
+static double perturb_factor(double v, size_t k, int n) {
+  unsigned long long h;
+  std::memcpy(&h, &v, sizeof(h));
+  h ^= g_perturb_seed * 0x9E3779B97F4A7C15ull + (unsigned long long)k * 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 31;
+  h *= 0x94D049BB133111EBull;
+  h ^= h >> 29;
+  const double u = (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+  return 1.0 + u * std::ldexp(1.0, -24) * std::sqrt(std::log2((double)std::max(n, 2)));
+}
+
+static void perturb(cd* x, size_t m, int n) {
+  if (!g_perturb_seed) return;
+  for (size_t k = 0; k < m; ++k)
+    x[k] = cd(x[k].real() * perturb_factor(x[k].real(), 2 * k, n),
+              x[k].imag() * perturb_factor(x[k].imag(), 2 * k + 1, n));
+}
+
+static void perturb(double* x, size_t m, int n) {
+  if (!g_perturb_seed) return;
+  for (size_t k = 0; k < m; ++k) x[k] *= perturb_factor(x[k], k, n);
+}
+
 void fft_r2c_1d(const double* in, cd* out, int n) {
   std::vector<cd> buf(n);
   for (int i = 0; i < n; ++i) buf[i] = cd(in[i], 0.0);
   fft_c2c(buf.data(), n, -1);
   for (int k = 0; k <= n / 2; ++k) out[k] = buf[k];
+  perturb(out, n / 2 + 1, n);
 }
 
 void fft_c2r_1d(const cd* in, double* out, int n) {
@@ -173,6 +205,7 @@ void fft_c2r_1d(const cd* in, double* out, int n) {
   if (n % 2 == 0) buf[h] = cd(in[h].real(), 0.0);
   fft_c2c(buf.data(), n, +1);
   for (int i = 0; i < n; ++i) out[i] = buf[i].real();
+  perturb(out, n, n);
 }
 
 void fft_r2c_2d(const double* in, int in_stride, cd* out, int nx, int ny) {
@@ -199,6 +232,8 @@ void fft_c2r_2d(const cd* in, double* out, int out_stride, int nx, int ny) {
 }
 
 }  // namespace oc
+
+extern "C" void oc_fft_perturb(unsigned long long seed) { oc::g_perturb_seed = seed; }
 
 // Checked against numpy in the oracle's own tests.
 extern "C" void oc_rfft(const double* in, double* out_re_im, int n) {

@@ -55,6 +55,8 @@ def lib():
         L.oc_projalign_set_f64.restype = None
         L.oc_trig_set.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p]
         L.oc_trig_set.restype = None
+        L.oc_fft_perturb.argtypes = [ctypes.c_ulonglong]
+        L.oc_fft_perturb.restype = None
         L.oc_trig_record.argtypes = [ctypes.c_int]
         L.oc_trig_record.restype = None
         L.oc_trig_recorded.argtypes = [_f32p, ctypes.c_int]
@@ -148,6 +150,13 @@ class Param:
 
 def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def fft_perturb(seed: int):
+    """Perturb every FFT output of the oracle by a relative 2^-24 sqrt(log2 n) at most
+    (deterministic per seed; 0 turns it off): a probe of how far single-precision
+    transform rounding, such as cuFFT's, can move the results."""
+    lib().oc_fft_perturb(ctypes.c_ulonglong(int(seed)))
 
 
 def trig_set(x, c, s):

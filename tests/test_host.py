@@ -185,3 +185,25 @@ def test_entry_points_reject_bad_arguments_before_touching_the_gpu(mflib):
                            None) == -1
     assert L.mf_device_cos_sin(None, a, 3, a, a) == -1
     assert L.mf_projalign_measured(None, a) == -1
+
+
+def test_oracle_fft_perturbation_probe():
+    """oracle.fft_perturb: transform outputs move by at most 2^-24 sqrt(log2 n)
+    relative, the same way for the same seed and input, and not at all with seed 0."""
+    import ctypes
+    L = O.lib()
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    L.oc_rfft.argtypes = [dp, dp, ctypes.c_int]
+    x = np.random.default_rng(2).normal(size=2048)
+    outs = []
+    try:
+        for seed in (0, 7, 7, 8):
+            O.fft_perturb(seed)
+            o = np.zeros(2 * 1025)
+            L.oc_rfft(x, o, 2048)
+            outs.append(o)
+    finally:
+        O.fft_perturb(0)
+    rel = np.abs(outs[1] - outs[0]) / np.maximum(np.abs(outs[0]), 1e-300)
+    assert 0 < rel.max() <= 2.0 ** -24 * np.sqrt(11) * 1.0001
+    assert np.array_equal(outs[1], outs[2]) and not np.array_equal(outs[1], outs[3])

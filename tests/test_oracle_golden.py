@@ -89,7 +89,7 @@ def transform_passes(g):
     return passes
 
 
-@pytest.mark.parametrize("name", ["c1s256", "c1s256b"])
+@pytest.mark.parametrize("name", ["c1s256", "c1s256b", "bin2"])
 def test_first_coarse_pass_matches_reference(name):
     g, s, angles = load(name)
     st = O.preprocess(s.stack, angles)
@@ -268,7 +268,7 @@ def determined_pixels(params, nx, ny, z, y0, x0, h, w, margin=SHIFT_PRINT + 2e-4
 
 def reference_aligned_runs():
     out = []
-    for name in ["c1s256", "c1s256b", "cfg1", "hi384"]:
+    for name in ["c1s256", "c1s256b", "cfg1", "hi384", "bin2"]:
         for g in reference_logs(name):
             sfx = "" if g.get("perturbation_seed") is None else f"_p{g['perturbation_seed']}"
             out.append(f"{name}{sfx}")
@@ -306,3 +306,57 @@ def test_aligned_stack_matches_reference_output(run):
     print(f"{run}: {det.mean():.4f} of the crop determined; crop rel-L2 {rel:.2e}, "
           f"largest slice-sum difference {srel:.2e}")
     assert srel < 2e-4
+
+
+def test_xf_matches_reference_output(mflib, tmp_path):
+    """The .xf writer (SaveParam::SaveXf, SaveParam.cpp:15-53, with its height = X
+    quirk and -s 1's reversed row order) given the parameters the reference wrote
+    for hi384, against the .xf the reference wrote for the same input with -s 1:
+    same rows in the same order and layout, values within the rounding of the
+    .txt's printed parameters (shifts 3 decimals, axis 4)."""
+    import re
+    g, s, angles = load("hi384")
+    params = np.array(g["params"], np.float64)
+    nz = len(angles)
+    p = mflib.Param(nz)
+    p.rotate[:] = params[:, 1]
+    p.shift_x[:] = params[:, 2]
+    p.shift_y[:] = params[:, 3]
+    out = str(tmp_path / "hi384.mrc")
+    mflib.save_param(out, 1, p, angles, s.stack.shape[2], s.stack.shape[1])
+    mine = open(str(tmp_path / "hi384.xf")).read().splitlines()
+    ref = open(os.path.join(GOLD, "ref_hi384_s1.xf")).read().splitlines()
+    assert len(mine) == len(ref) == nz
+    pat = re.compile(r"^( *-?\d+\.\d{3} {2}){5} *-?\d+\.\d{3} $")
+    for a, b in zip(mine, ref):
+        assert pat.match(a) and pat.match(b), (a, b)
+        va = np.array([float(v) for v in a.split()])
+        vb = np.array([float(v) for v in b.split()])
+        assert np.abs(va - vb).max() <= 0.0021, (a, b)
+
+
+def test_bin2_first_projection_pass_matches_reference():
+    """The 3072 px series that the reference matches at bin 2 (ProjAlign.cpp:57-61,
+    slab 100 / 2 = 50): the oracle follows its coarse stage and every per-tilt
+    shift of its first projection-matching pass, to print rounding plus the spread
+    of the reference's runs on that trajectory."""
+    g, s, angles = load("bin2")
+    logs = reference_logs("bin2")
+    nz = len(angles)
+    st = O.preprocess(s.stack, angles)
+    p = O.Param(nz)
+    t = O.Transform(st, angles, p)
+    for i in (1, 2, 3):
+        e = t.doit()
+        ax = O.tilt_axis(st, angles, p, 180.0 / i)
+        assert min(abs(e - events(r, "maxerr")[i - 1][1]) for r in logs) < PRINT_TOL
+        assert min(abs(ax - events(r, "axis")[i - 1][1]) for r in logs) < PRINT_TOL
+    ang = angles + np.float32(0.0001)
+    p.shift_x[:] = 0
+    p.shift_y[:] = 0
+    pa = O.ProjAlign(st, ang, p, 0.0, g["thickness"], g["nproj"])
+    pa.doit()
+    meas = pa.measured()
+    dev = [pass_deviation(meas, ang, events(r, "meas")[: nz - 1]) for r in logs]
+    best = int(np.argmin(dev))
+    assert dev[best] < pass_tolerance(logs, best, nz, 0), dev
