@@ -61,7 +61,7 @@ struct mf_group {
   std::vector<float> z0;
   // device tables
   DevBuf d_ser, d_steps, d_active, d_bp, d_applyjobs, d_maxerr, d_z0, d_err, d_meas, d_tcerr;
-  DevBuf d_order, rowflags;
+  DevBuf d_order;
   ReprojOpSet ops;
   TcOpSet tcops;
   std::vector<TmaDesc> maps;               // per series
@@ -219,10 +219,8 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
       it = g->masks.emplace(key, std::move(mk)).first;
     }
     M.mask = it->second->as<float>();
-    if (g->prec != MF_PREC_FP32) {
-      MF_TRY(M.corr16.alloc((size_t)2 * M.xpitch * M.yb * M.nz));
-      MF_TRY(M.tflags.alloc(sizeof(int) * (size_t)M.nz * M.ytiles * kFlagParts));
-    }
+    if (g->prec != MF_PREC_FP32) MF_TRY(M.corr16.alloc((size_t)2 * M.xpitch * M.yb * M.nz));
+    MF_TRY(M.tflags.alloc(sizeof(int) * (size_t)M.nz * M.ytiles * kFlagParts));
     for (int z : M.order) orders.push_back(z);
   }
   MF_TRY(g->d_steps.alloc(sizeof(GroupStepDev) * steps.size()));
@@ -339,13 +337,11 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
   } else {
     MF_TRY(build_reproj_ops_any(c, geoms, &g->ops, st));
-    MF_TRY(g->rowflags.alloc(sizeof(int) * (size_t)nmax * B * g->ytiles_max));
     std::vector<ApplyJob> jobs((size_t)nmax * B);
     for (int k = 0; k < nmax; ++k)
       for (int b = 0; b < B; ++b) {
         const GroupMember& M = *g->m[b];
         ApplyJob J{};
-        J.rowflags = g->rowflags.as<int>() + ((size_t)k * B + b) * g->ytiles_max;
         if (k < M.n) {
           const ReprojOpView& v = g->ops.ops[M.op0 + k];
           J.tiles = v.tiles;
@@ -397,9 +393,6 @@ static int group_enqueue(mf_group* g) {
   const GroupSeriesDev* ser = g->d_ser.as<GroupSeriesDev>();
   const GroupStepDev* steps = g->d_steps.as<GroupStepDev>();
   const int* active = g->d_active.as<int>();
-  if (!tc)
-    MF_CHECK_CUDA(cudaMemsetAsync(g->rowflags.p, 0,
-                                  sizeof(int) * (size_t)nmax * B * g->ytiles_max, st));
   // CorrTomoStack::DoIt for every tilt of every active series
   GroupCorrArgs ca{ser, nullptr, active, g->nz_max, 1};
   MF_TRY(launch_correct_group(c, ca, B, g->xb_max, g->yb_max, st));
@@ -417,6 +410,8 @@ static int group_enqueue(mf_group* g) {
   if (tc)
     MF_TRY(launch_to_half_group(c, ser, nullptr, active, B, g->nz_max, g->ytiles_max, g->prec,
                                 st));
+  else
+    MF_TRY(launch_flag_tiles_group(c, ser, nullptr, active, B, g->nz_max, g->ytiles_max, st));
   MF_TRY(fit_z0_group(c, ser, active, B, st));
   const bool prof = c->profiling && (int)g->events.size() >= 3 * nmax;
   std::vector<TcJob> jobs;
@@ -456,9 +451,8 @@ static int group_enqueue(mf_group* g) {
     } else {
       MF_TRY(launch_reproject_apply_group(c, g->ops, g->d_applyjobs.as<ApplyJob>() + (size_t)k * B,
                                           active, B, g->ntiles_max, g->yb_max, st));
-      MF_TRY(launch_reproject_exact_group(
-          c, ser, sk, active, B, g->xb_max, g->ytiles_max, g->d_bp.as<float>(), false,
-          g->rowflags.as<int>() + (size_t)k * B * g->ytiles_max, st));
+      MF_TRY(launch_reproject_exact_group(c, ser, sk, active, B, g->xb_max, g->ytiles_max,
+                                          g->d_bp.as<float>(), true, nullptr, st));
     }
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 1], st));
     // MeaAlignProj for every series: PANorm both images, FFT, filter, inverse, peak
@@ -494,6 +488,8 @@ static int group_enqueue(mf_group* g) {
     MF_CHECK_CUDA(cudaGetLastError());
     if (tc)
       MF_TRY(launch_to_half_group(c, ser, sk, active, B, g->nz_max, g->ytiles_max, g->prec, st));
+    else
+      MF_TRY(launch_flag_tiles_group(c, ser, sk, active, B, g->nz_max, g->ytiles_max, st));
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k + 2], st));
   }
   MF_TRY(max_err_group(c, ser, active, B, g->d_maxerr.as<float>(), st));

@@ -392,7 +392,7 @@ struct GroupSeriesDev {
   float2* stats;       // 2: (mean, std) of the pair
   float2* ppart;       // kPeakParts peak partials
   void* corr16;        // FP16/BF16: nz x yb x xpitch 16-bit copy of corr
-  int* tflags;         // FP16/BF16: nz x ytiles x kFlagParts flags of the copy
+  int* tflags;         // nz x ytiles x kFlagParts flags: tiles the operator cannot carry
 };
 struct GroupStepDev {  // the held-out tilt of one series at one step of the pass
   int ip, i0, nk, ray_len, thick, bp_off;  // ip < 0: the series has no tilt at this step
@@ -419,12 +419,18 @@ int launch_to_half_group(Context* c, const GroupSeriesDev* ser, const GroupStepD
                          const int* active, int nseries, int nz_max, int ytiles_max,
                          int half_kind, cudaStream_t st);
 // exact re-projection of the flagged 128-row tiles of every active series at one
-// step into its reproj buffer; flags: the 16-bit copy's tflags when tc, else the
-// FP32 apply's rowflags of the step (rowflags[b * ytiles_max + tile])
+// step into its reproj buffer; flags: the series' tflags when tc (16-bit copy or
+// FP32 sentinel flags), else rowflags of the step (rowflags[b * ytiles_max + tile])
 int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
                                  const int* active, int nseries, int xb_max, int ytiles_max,
                                  const float* d_bp, bool tc, const int* rowflags,
                                  cudaStream_t st);
+// FP32 groups: per-(tilt, 128-row tile, column part) sentinel flags of the
+// corrected stacks (the tflags layout of the 16-bit copies), for all tilts of
+// every series (steps == null) or each series' held-out tilt of a step
+int launch_flag_tiles_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                            const int* active, int nseries, int nz_max, int ytiles_max,
+                            cudaStream_t st);
 struct ApplyJob {  // one series of a group at one step of the FP32 apply
   const OpTile* tiles;
   const int* colvalid;

@@ -1053,12 +1053,188 @@ int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr
   return MF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Group form of the FP32 apply, for whole groups of series: a CTA computes 256
+// image rows x 64 output columns with 256 threads, each an 8 x 8 register tile
+// (rows ty*4..+3 and 128+ty*4..+3, columns tx*4..+3 and 32+tx*4..+3, so that the
+// warp's shared-memory reads are contiguous 16-byte vectors).  Operator rows are
+// consumed 16 at a time through a 3-stage shared-memory ring fed by cp.async: the
+// gathered neighbour values (4-byte copies, zero-filled below the image) and the
+// coefficient chunk (16-byte copies) go straight from global to shared memory,
+// with no staging registers.  Sentinels are not tested here: the per-(tilt,
+// 128-row tile) flags of the corrected stack (k_flag_tiles_group) send the tiles
+// whose neighbours hold a -1e30 to the exact path, which overwrites them.
+constexpr int kA2Y = 256;        // image rows per CTA
+constexpr int kA2Stages = 3;     // cp.async ring depth
+constexpr int kA2Pitch = 260;    // floats per operator row of the A tile (256 + 4)
+constexpr int kA2SmemBytes = kA2Stages * kOpChunk * (kA2Pitch + kOpTileX) * 4;
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 2)
+    k_op_apply_group(const float* __restrict__ coef, const int2* __restrict__ rowmap,
+                     const ApplyJob* __restrict__ jobs, const int* __restrict__ active) {
+  if (active && active[blockIdx.z] == 0) return;
+  const ApplyJob J = jobs[blockIdx.z];
+  if ((int)blockIdx.x >= J.ntiles || (int)blockIdx.y * kA2Y >= J.yb) return;
+  extern __shared__ __align__(16) float smem[];
+  float* As = smem;                                      // [stage][16][kA2Pitch]
+  float* Bs = smem + kA2Stages * kOpChunk * kA2Pitch;    // [stage][16][64]
+  const int xb = J.xb, yb = J.yb;
+  const size_t pix = (size_t)xb * yb;
+  const int y0 = blockIdx.y * kA2Y;
+  const int x0 = blockIdx.x * kOpTileX;
+  const OpTile tile = J.tiles[blockIdx.x];
+  const int nchunks = tile.rows / kOpChunk;
+  const int tid = threadIdx.x;
+  const int lr = tid % kOpChunk, ly = tid / kOpChunk;  // loader: operator row, first image row
+  const uint32_t as_base = (uint32_t)__cvta_generic_to_shared(As);
+  const uint32_t bs_base = (uint32_t)__cvta_generic_to_shared(Bs);
+  auto load = [&](int c) {
+    const int st = c % kA2Stages;
+    const int row = tile.row0 + c * kOpChunk;
+    const int2 rm = __ldg(rowmap + row + lr);
+    const float* src = J.corr + (size_t)rm.x * pix + rm.y;
+    const uint32_t a = as_base + (uint32_t)((st * kOpChunk + lr) * kA2Pitch) * 4u;
+#pragma unroll
+    for (int q = 0; q < kA2Y / 16; ++q) {
+      const int y = ly + 16 * q;
+      const bool in = y0 + y < yb;
+      cp_async4(a + (uint32_t)y * 4u, in ? src + (size_t)(y0 + y) * xb : src, in);
+    }
+    cp_async16(bs_base + (uint32_t)(st * kOpChunk * kOpTileX + tid * 4) * 4u,
+               coef + (size_t)row * kOpTileX + tid * 4);
+  };
+  const int tx = tid % 8, ty = tid / 8;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+#pragma unroll
+  for (int c = 0; c < kA2Stages - 1; ++c) {
+    if (c < nchunks) load(c);
+    cp_async_commit();
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait<kA2Stages - 2>();
+    __syncthreads();
+    if (c + kA2Stages - 1 < nchunks) load(c + kA2Stages - 1);
+    cp_async_commit();
+    const float* A = As + (c % kA2Stages) * kOpChunk * kA2Pitch;
+    const float* Bt = Bs + (c % kA2Stages) * kOpChunk * kOpTileX;
+#pragma unroll
+    for (int rr = 0; rr < kOpChunk; ++rr) {
+      const float4 a0 = *reinterpret_cast<const float4*>(A + rr * kA2Pitch + ty * 4);
+      const float4 a1 = *reinterpret_cast<const float4*>(A + rr * kA2Pitch + 128 + ty * 4);
+      const float4 b0 = *reinterpret_cast<const float4*>(Bt + rr * kOpTileX + tx * 4);
+      const float4 b1 = *reinterpret_cast<const float4*>(Bt + rr * kOpTileX + 32 + tx * 4);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+  }
+  cp_async_wait<0>();
+  int cv[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int x = x0 + (j < 4 ? tx * 4 + j : 32 + tx * 4 + j - 4);
+    cv[j] = x < xb ? J.colvalid[x] : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int y = y0 + (i < 4 ? ty * 4 + i : 128 + ty * 4 + i - 4);
+    if (y >= yb) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int xc = x0 + h * 32 + tx * 4;
+      float v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = cv[4 * h + j] ? acc[i][4 * h + j] : kSentinel;
+      float* o = J.out + (size_t)y * xb + xc;
+      if (xc + 3 < xb && (xb & 3) == 0) {
+        *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (xc + j < xb) o[j] = v[j];
+      }
+    }
+  }
+}
+
 int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
                                  const int* active, int njobs, int ntiles_max, int yb_max,
                                  cudaStream_t st) {
-  dim3 grd(ntiles_max, (yb_max + kApplyTileY - 1) / kApplyTileY, njobs);
-  k_op_apply<<<grd, 256, 0, st>>>(nullptr, 0, 0, 0, set.coef.as<float>(), set.rowmap.as<int2>(),
-                                  nullptr, nullptr, nullptr, nullptr, d_jobs, active);
+  static bool attr_set[64] = {};  // per device ordinal
+  if (!attr_set[c->gpu & 63]) {
+    MF_CHECK_CUDA(cudaFuncSetAttribute(k_op_apply_group,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kA2SmemBytes));
+    attr_set[c->gpu & 63] = true;
+  }
+  dim3 grd(ntiles_max, (yb_max + kA2Y - 1) / kA2Y, njobs);
+  k_op_apply_group<<<grd, 256, kA2SmemBytes, st>>>(set.coef.as<float>(), set.rowmap.as<int2>(),
+                                                   d_jobs, active);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Per-(tilt, 128-row tile, column part) flags of an FP32 corrected stack: set when
+// the piece holds a -1e30 sentinel (the banded operator cannot carry one; the exact
+// path then recomputes every output tile that reads it).  All tilts of every
+// series (steps == null) or each series' held-out tilt of a step.
+__global__ void k_flag_tiles_group(const GroupSeriesDev* __restrict__ ser,
+                                   const GroupStepDev* __restrict__ steps,
+                                   const int* __restrict__ active, int nz_max) {
+  const int j = blockIdx.z;
+  const int b = steps ? j : j / nz_max;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  const int tz = steps ? steps[b].ip : j % nz_max;
+  if (tz < 0 || tz >= S.nz || (int)blockIdx.y >= S.ytiles) return;
+  const int xb = S.xb, yb = S.yb;
+  const float* s = S.corr + (size_t)tz * xb * yb;
+  const int ya = blockIdx.y * kApplyTileY, yz = min(yb, ya + kApplyTileY);
+  const int half_x = xb / 2;
+  const int p0 = half_x * blockIdx.x / kFlagParts, p1 = half_x * (blockIdx.x + 1) / kFlagParts;
+  int bad = 0;
+  for (int y = ya + threadIdx.y; y < yz; y += blockDim.y) {
+    const float2* row = reinterpret_cast<const float2*>(s + (size_t)y * xb);
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+      const float2 v = row[p];
+      bad |= (v.x < -1e10f) | (v.y < -1e10f);
+    }
+  }
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    S.tflags[((size_t)tz * S.ytiles + blockIdx.y) * kFlagParts + blockIdx.x] = bad ? 1 : 0;
+}
+
+int launch_flag_tiles_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
+                            const int* active, int nseries, int nz_max, int ytiles_max,
+                            cudaStream_t st) {
+  if (nseries <= 0) return MF_OK;
+  dim3 blk(64, 8), grd(kFlagParts, ytiles_max, steps ? nseries : nseries * nz_max);
+  k_flag_tiles_group<<<grd, blk, 0, st>>>(ser, steps, active, nz_max);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
