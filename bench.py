@@ -637,10 +637,16 @@ def run_ours(args):
         d_outs = None
         line["uneven_batch"] = uneven_run(mf, ctx, stream, dev, [args.precision, "fp16"])
         log("uneven batch done")
+    # the serving run and the CPU sample need none of the above: release the
+    # stacks and the context (with its cuFFT plans) first
+    del d_raws, series, s0
+    d_outs = None
+    torch.cuda.synchronize()
+    ctx.close()
+    ctx = None
+    torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_serve:
         log("serving run")
-        d_outs = None
-        torch.cuda.empty_cache()
         line["served"] = served_run(mf, dev, args.serve_requests, PRECISIONS["fp16"])
         log("serving run done")
         line["served_over_plain"] = line["served"]["equiv_2048_series_per_min"] / plain_value
@@ -650,9 +656,6 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_sample(cpu)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del d_raws, series
-    torch.cuda.synchronize()
-    ctx.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

@@ -275,7 +275,7 @@ MF_API int mf_align_batch_device(mf_context* ctx, int n, const mf_series_desc* s
 /* ---- serving: continuous batching of requests ------------------------------
  * Not in the reference.  A server keeps `workers` streams busy with requests
  * (tilt series) that arrive at any time: a request is admitted when its
- * estimated device memory fits in `hbm_budget` bytes (0 = 80% of the free
+ * estimated device memory fits in `hbm_budget` bytes (0 = 65% of the free
  * memory), prepared on its own (upload, pre-processing, coarse alignment), then
  * projection-matched in a group with other prepared requests of any shape that
  * share its precision, -p and z shift (up to `max_group`).  A worker runs a full

@@ -275,14 +275,16 @@ MF_API int mf_server_create(int gpu, size_t hbm_budget, int max_group, int worke
   if (workers < 1 || workers > 16) return set_error(MF_ERR_ARG, "workers must be 1..16");
   MF_CHECK_CUDA(cudaSetDevice(gpu));
   if (hbm_budget == 0) {
-    // 80 % of the free memory once the pool's cached blocks are returned: the rest
+    // 65 % of the free memory once the pool's cached blocks are returned: the rest
     // is left to what the estimate does not count (cuFFT plans and work areas,
-    // which cuFFT allocates outside the pool, and group working sets)
+    // which cuFFT allocates outside the pool for every shape each worker meets,
+    // the coarse stages' transient buffers of the requests being prepared, and
+    // group working sets of mixed shapes)
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     size_t fr = 0, tot = 0;
     MF_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-    hbm_budget = fr / 10 * 8;
+    hbm_budget = fr / 100 * 65;
   }
   std::unique_ptr<mf_server> s(new mf_server());
   s->gpu = gpu;
