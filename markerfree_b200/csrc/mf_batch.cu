@@ -56,6 +56,12 @@ struct mf_group {
   int nz_max = 0, xb_max = 0, yb_max = 0, pad_max = 0, cmp_max = 0, ytiles_max = 0;
   int ntiles_max = 0, rows_max = 0, tc_nb = 256;
   std::vector<std::unique_ptr<GroupMember>> m;
+  // distinct re-projection operators (series with the same angles, size and slab
+  // share theirs): per (series, step) entry op0 + k of the geometry list, its
+  // operator's index; per operator, the bytes an apply reads and writes for the
+  // images (per series) and reads of the operator itself (once per launch), MACs
+  std::vector<int> opidx;
+  std::vector<double> op_io, op_coef, op_mac;
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> masks;  // per (xb, yb)
   std::vector<int> active;
   std::vector<float> z0;
@@ -67,7 +73,6 @@ struct mf_group {
   std::vector<TmaDesc> maps;               // per series
   std::vector<std::vector<TcJob>> tcjobs;  // per step: the series with a tilt at that step
   std::vector<cudaEvent_t> events;         // 3 per step when the context profiles
-  double op_bytes = 0, op_fma = 0;  // mean compulsory bytes / MACs of one operator apply
   ~mf_group() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
   }
@@ -298,15 +303,46 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
   }
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_ser.p, sd.data(), sizeof(GroupSeriesDev) * B,
                                 cudaMemcpyHostToDevice, st));
-  // re-projection operators of every (series, step): geometry index op0 + k
+  // re-projection operators of every (series, step): geometry index op0 + k.
+  // Series of one acquisition scheme have identical geometries (same angles, size,
+  // slab): each distinct one is built once and shared.
+  std::vector<ReprojGeom> uniq;
+  g->opidx.assign(geoms.size(), 0);
+  {
+    auto bits = [](float v) {
+      uint32_t u;
+      memcpy(&u, &v, 4);
+      return u;
+    };
+    std::map<std::vector<uint32_t>, int> seen;
+    for (size_t i = 0; i < geoms.size(); ++i) {
+      const ReprojGeom& gm = geoms[i];
+      std::vector<uint32_t> key = {(uint32_t)gm.xb,  (uint32_t)gm.yb, (uint32_t)gm.thick,
+                                   (uint32_t)gm.ip,  (uint32_t)gm.i0, (uint32_t)gm.i1,
+                                   (uint32_t)gm.nk,  (uint32_t)gm.ray_len, bits(gm.fcos),
+                                   bits(gm.fsin)};
+      for (float v : gm.bp) key.push_back(bits(v));
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        it = seen.emplace(std::move(key), (int)uniq.size()).first;
+        uniq.push_back(gm);
+      }
+      g->opidx[i] = it->second;
+    }
+  }
   g->tcjobs.assign(nmax, {});
   if (g->prec != MF_PREC_FP32) {
-    MF_TRY(build_reproj_tc_ops_any(c, geoms, g->prec, &g->tcops, st));
+    MF_TRY(build_reproj_tc_ops_any(c, uniq, g->prec, &g->tcops, st));
+    for (const TcOpView& v : g->tcops.ops) {
+      g->op_io.push_back(2.0 * v.xb * v.yb * v.nk + 4.0 * v.xb * v.yb);
+      g->op_coef.push_back((double)v.nchunks * kTcM * kTcK * 2);
+      g->op_mac.push_back((double)v.nchunks * kTcM * kTcK * v.yb);
+    }
     g->maps.assign(B, TmaDesc());
     for (int b = 0; b < B; ++b) {
       const GroupMember& M = *g->m[b];
       for (int k = 0; k < M.n; ++k) {
-        const TcOpView& v = g->tcops.ops[M.op0 + k];
+        const TcOpView& v = g->tcops.ops[g->opidx[M.op0 + k]];
         g->tcjobs[k].push_back(TcJob{v.xt, v.colvalid, M.reproj.as<float>(), b, b, M.xb, M.yb,
                                      0, 0});
       }
@@ -336,14 +372,19 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     }
     MF_CHECK_CUDA(cudaMemsetAsync(g->d_tcerr.p, 0, sizeof(int), st));
   } else {
-    MF_TRY(build_reproj_ops_any(c, geoms, &g->ops, st));
+    MF_TRY(build_reproj_ops_any(c, uniq, &g->ops, st));
+    for (const ReprojOpView& v : g->ops.ops) {
+      g->op_io.push_back(4.0 * v.xb * v.yb * (v.nk + 1));
+      g->op_coef.push_back((double)v.total_rows * (kOpTileX * 4 + 8));
+      g->op_mac.push_back((double)v.yb * v.total_rows * kOpTileX);
+    }
     std::vector<ApplyJob> jobs((size_t)nmax * B);
     for (int k = 0; k < nmax; ++k)
       for (int b = 0; b < B; ++b) {
         const GroupMember& M = *g->m[b];
         ApplyJob J{};
         if (k < M.n) {
-          const ReprojOpView& v = g->ops.ops[M.op0 + k];
+          const ReprojOpView& v = g->ops.ops[g->opidx[M.op0 + k]];
           J.tiles = v.tiles;
           J.colvalid = v.colvalid;
           J.corr = M.corr.as<float>();
@@ -358,9 +399,6 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     MF_CHECK_CUDA(cudaMemcpyAsync(g->d_applyjobs.p, jobs.data(), sizeof(ApplyJob) * jobs.size(),
                                   cudaMemcpyHostToDevice, st));
   }
-  const double nops = std::max<double>(1.0, (double)geoms.size());
-  g->op_bytes = (g->prec != MF_PREC_FP32 ? g->tcops.bytes : g->ops.bytes) / nops;
-  g->op_fma = (g->prec != MF_PREC_FP32 ? g->tcops.fma : g->ops.fma) / nops;
   // FFT plans (cached per context).  The same plan shapes as the series' own pass,
   // executed once per series: a plan batched over the group may round
   // differently, and a different rounding can flip a near-tied decision later
@@ -526,13 +564,28 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
   if (tcerr != 0)
     return set_error(MF_ERR_CUDA, "tensor-core re-projection pipeline stalled (code %d)", tcerr);
-  double steps_run = 0;
   for (int b = 0; b < B; ++b)
     if (active[b]) {
       max_err[b] = me[b];
       g->ser[b]->pa.z0 = g->z0[b];
-      steps_run += g->m[b]->n;
     }
+  // compulsory bytes and MACs of this pass's re-projection launches: per step, the
+  // images and output of every series taking part, each distinct operator once
+  double pass_bytes = 0, pass_mac = 0;
+  std::vector<int> used;
+  for (int k = 0; k < g->nmax; ++k) {
+    used.clear();
+    for (int b = 0; b < B; ++b) {
+      if (!active[b] || k >= g->m[b]->n) continue;
+      const int o = g->opidx[g->m[b]->op0 + k];
+      pass_bytes += g->op_io[o];
+      pass_mac += g->op_mac[o];
+      if (std::find(used.begin(), used.end(), o) == used.end()) {
+        used.push_back(o);
+        pass_bytes += g->op_coef[o];
+      }
+    }
+  }
   if (c->profiling && (int)g->events.size() >= 3 * g->nmax) {
     // stage times of this pass: [0] re-projection launches (one per step for the
     // whole group), [2] the rest of each step; bytes and MACs of the active series
@@ -545,8 +598,8 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
     }
     c->stage[1] += g->nmax;
     c->stage[3] += 1;
-    c->stage[4] += g->op_bytes * steps_run;
-    c->stage[5] += g->op_fma * steps_run;
+    c->stage[4] += pass_bytes;
+    c->stage[5] += pass_mac;
   }
   return MF_OK;
 }
