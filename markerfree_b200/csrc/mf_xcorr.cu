@@ -262,6 +262,14 @@ __global__ void __launch_bounds__(256) k_moments_final_group(
   S.stats[img & 1] = make_float2((float)(s2.x / n), 1.0f);  // PANorm: std = 1
 }
 
+// Two neighbouring pixels per thread (widths and pitches are even): the image,
+// mask and output rows are read and written as float2.
+__device__ __forceinline__ float norm_mask_one(float v, float mean, float fr) {
+  if (!(v < -1e10f)) v = __fsub_rn(v, mean);  // GNormalize with std 1
+  if (v < -1e10f) return 0.0f;
+  return fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
+}
+
 __global__ void k_norm_mask_group(const GroupSeriesDev* __restrict__ ser,
                                   const GroupStepDev* __restrict__ steps,
                                   const int* __restrict__ active) {
@@ -270,24 +278,19 @@ __global__ void k_norm_mask_group(const GroupSeriesDev* __restrict__ ser,
   const GroupSeriesDev& S = ser[b];
   const GroupStepDev T = steps[b];
   if (T.ip < 0) return;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;  // pixel pair
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int w = S.xb, pad = S.pad;
-  if (x >= pad || y >= S.yb) return;
-  float* d = S.cc + (size_t)(img & 1) * S.ppix + (size_t)y * pad + x;
-  if (x >= w) {
-    *d = 0.0f;
+  if (2 * q >= pad || y >= S.yb) return;
+  float2* d = reinterpret_cast<float2*>(S.cc + (size_t)(img & 1) * S.ppix + (size_t)y * pad) + q;
+  if (2 * q >= w) {
+    *d = make_float2(0.0f, 0.0f);
     return;
   }
-  float v = group_image(S, T, img)[(size_t)y * w + x];
-  const float2 st = S.stats[img & 1];
-  if (!(v < -1e10f)) v = __fsub_rn(v, st.x);  // GNormalize with std 1
-  if (v < -1e10f) {
-    *d = 0.0f;
-    return;
-  }
-  const float fr = __ldg(S.mask + (size_t)y * w + x);
-  *d = fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
+  const float2 v = reinterpret_cast<const float2*>(group_image(S, T, img) + (size_t)y * w)[q];
+  const float2 fr = __ldg(reinterpret_cast<const float2*>(S.mask + (size_t)y * w) + q);
+  const float mean = S.stats[img & 1].x;
+  *d = make_float2(norm_mask_one(v.x, mean, fr.x), norm_mask_one(v.y, mean, fr.y));
 }
 
 int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
@@ -296,7 +299,7 @@ int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDe
   (void)xb_max;
   k_moments_group<<<dim3(moment_parts(yb_max), 2 * nseries), 256, 0, st>>>(ser, steps, active);
   k_moments_final_group<<<2 * nseries, 256, 0, st>>>(ser, steps, active);
-  dim3 blk(64, 4), grd((pad_max + 63) / 64, (yb_max + 3) / 4, 2 * nseries);
+  dim3 blk(128, 2), grd((pad_max / 2 + 127) / 128, (yb_max + 1) / 2, 2 * nseries);
   k_norm_mask_group<<<grd, blk, 0, st>>>(ser, steps, active);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
