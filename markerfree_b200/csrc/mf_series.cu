@@ -34,6 +34,9 @@ mf_context::~mf_context() {
   std::lock_guard<std::recursive_mutex> lk(fft_mutex());
   for (auto& kv : plans) cufftDestroy(kv.second);
   plans.clear();
+  for (int i = 0; i <= kFftStreams; ++i)
+    if (work[i]) cudaFree(work[i]);
+  for (void* p : retired_work) cudaFree(p);
   for (int i = 0; i < kFftStreams; ++i) {
     if (aux[i]) cudaStreamDestroy(aux[i]);
     if (join_ev[i]) cudaEventDestroy(join_ev[i]);
@@ -59,56 +62,69 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
     return MF_OK;
   }
   // key: kind (0 rows R2C in place, 1 rows C2R out of place, 2 2-D R2C in place,
-  //            3 2-D C2R in place), nx, ny, batch
+  //            3 2-D C2R in place, 4 1-D R2C lines, 5 2-D C2R pairs), nx, ny, batch,
+  //      and optionally the side stream the plan is bound to
   std::lock_guard<std::recursive_mutex> lk(fft_mutex());
-  // cuFFT allocates its work areas with cudaMalloc, outside the stream-ordered
-  // pool: refuse (instead of letting the planner fail inside cuFFT) when the
-  // device is nearly full.
-  {
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < ((size_t)1 << 30))
-      return set_error(MF_ERR_NOMEM, "%zu MB of device memory left for an FFT plan",
-                       fr >> 20);
-    cudaGetLastError();
-  }
+  const int slot = (key.size() > 4 && key[4] >= 0) ? (int)key[4] : kFftStreams;
+  if (slot > kFftStreams) return set_error(MF_ERR_ARG, "FFT side stream %d out of range", slot);
+  if (slot < kFftStreams) MF_TRY(ensure_aux());
+  cudaStream_t bind = slot < kFftStreams ? aux[slot] : c.stream;
   long long kind = key[0];
   int nx = (int)key[1], ny = (int)key[2], batch = (int)key[3];
   int pad = (nx / 2 + 1) * 2, cmp = nx / 2 + 1;
   cufftHandle h;
+  if (cufftCreate(&h) != CUFFT_SUCCESS) return set_error(MF_ERR_CUFFT, "cufftCreate failed");
+  // The work area is the context's, one per stream (see work[]): plans of one
+  // stream run one after another, so they share it.
+  cufftSetAutoAllocation(h, 0);
+  size_t ws = 0;
   cufftResult r;
   if (kind == 0) {
     int n[1] = {nx}, inem[1] = {pad}, onem[1] = {cmp};
-    r = cufftPlanMany(&h, 1, n, inem, 1, pad, onem, 1, cmp, CUFFT_R2C, batch);
+    r = cufftMakePlanMany(h, 1, n, inem, 1, pad, onem, 1, cmp, CUFFT_R2C, batch, &ws);
   } else if (kind == 1) {
     int n[1] = {nx}, inem[1] = {cmp}, onem[1] = {nx};
-    r = cufftPlanMany(&h, 1, n, inem, 1, cmp, onem, 1, nx, CUFFT_C2R, batch);
+    r = cufftMakePlanMany(h, 1, n, inem, 1, cmp, onem, 1, nx, CUFFT_C2R, batch, &ws);
   } else if (kind == 4) {
     // 1-D R2C in place with the default padded layout (tilt-axis lines)
-    r = cufftPlan1d(&h, nx, CUFFT_R2C, batch);
+    r = cufftMakePlan1d(h, nx, CUFFT_R2C, batch, &ws);
   } else if (kind == 5) {
-    // 2-D C2R in place over `batch` maps spaced two padded images apart (the second
-    // image of each (reference, image) pair of a group's cross-correlation buffer)
+    // 2-D C2R in place over `batch` maps spaced two padded images apart
     int n[2] = {ny, nx}, inem[2] = {ny, cmp}, onem[2] = {ny, pad};
-    r = cufftPlanMany(&h, 2, n, inem, 1, 2 * ny * cmp, onem, 1, 2 * ny * pad, CUFFT_C2R, batch);
+    r = cufftMakePlanMany(h, 2, n, inem, 1, 2 * ny * cmp, onem, 1, 2 * ny * pad, CUFFT_C2R,
+                          batch, &ws);
   } else if (kind == 2) {
     int n[2] = {ny, nx}, inem[2] = {ny, pad}, onem[2] = {ny, cmp};
-    r = cufftPlanMany(&h, 2, n, inem, 1, ny * pad, onem, 1, ny * cmp, CUFFT_R2C, batch);
+    r = cufftMakePlanMany(h, 2, n, inem, 1, ny * pad, onem, 1, ny * cmp, CUFFT_R2C, batch, &ws);
   } else {
     int n[2] = {ny, nx}, inem[2] = {ny, cmp}, onem[2] = {ny, pad};
-    r = cufftPlanMany(&h, 2, n, inem, 1, ny * cmp, onem, 1, ny * pad, CUFFT_C2R, batch);
+    r = cufftMakePlanMany(h, 2, n, inem, 1, ny * cmp, onem, 1, ny * pad, CUFFT_C2R, batch, &ws);
   }
-  if (r != CUFFT_SUCCESS)
-    return set_error(MF_ERR_CUFFT, "cufftPlanMany(kind %lld, %d x %d, batch %d) failed: %d", kind,
-                     nx, ny, batch, (int)r);
-  cudaStream_t bind = c.stream;
-  if (key.size() > 4 && key[4] >= 0) {
-    if (key[4] >= kFftStreams) {
+  if (r != CUFFT_SUCCESS) {
+    cufftDestroy(h);
+    return set_error(MF_ERR_CUFFT, "cufftMakePlanMany(kind %lld, %d x %d, batch %d) failed: %d",
+                     kind, nx, ny, batch, (int)r);
+  }
+  if (ws > work_bytes[slot]) {
+    // grow this stream's work area and point every plan of the stream at the new
+    // one.  The old area is kept until the context goes: a pass captured into a
+    // CUDA graph holds the address its plans had at capture time.
+    void* p = nullptr;
+    if (cudaMalloc(&p, ws) != cudaSuccess) {
+      cudaGetLastError();
       cufftDestroy(h);
-      return set_error(MF_ERR_ARG, "FFT side stream %lld out of range", key[4]);
+      return set_error(MF_ERR_NOMEM, "FFT work area of %zu MB: device memory exhausted",
+                       ws >> 20);
     }
-    MF_TRY(ensure_aux());
-    bind = aux[key[4]];
+    if (work[slot]) retired_work.push_back(work[slot]);
+    work[slot] = p;
+    work_bytes[slot] = ws;
+    for (auto& kv : plans) {
+      const int ks = (kv.first.size() > 4 && kv.first[4] >= 0) ? (int)kv.first[4] : kFftStreams;
+      if (ks == slot) cufftSetWorkArea(kv.second, work[slot]);
+    }
   }
+  if (ws > 0) cufftSetWorkArea(h, work[slot]);
   cufftSetStream(h, bind);
   plans[key] = h;
   *out = h;

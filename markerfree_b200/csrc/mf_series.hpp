@@ -19,6 +19,12 @@ struct mf_context {
   static constexpr int kFftStreams = 4;
   cudaStream_t aux[kFftStreams] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[kFftStreams] = {};
+  // cuFFT work areas, one per side stream and one (the last) for the context
+  // stream, each as large as the largest plan bound to that stream needs: cuFFT
+  // would otherwise allocate one per plan, and a context meets many shapes
+  void* work[kFftStreams + 1] = {};
+  size_t work_bytes[kFftStreams + 1] = {};
+  std::vector<void*> retired_work;  // outgrown areas (captured graphs may hold them)
   ~mf_context();
   // Plan cache keyed by (kind, sizes, batch); bound to the context stream, or with
   // a fifth key entry i >= 0 to side stream i.
