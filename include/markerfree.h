@@ -85,6 +85,10 @@ typedef struct mf_series mf_series;
 /* ---- errors ------------------------------------------------------------- */
 MF_API const char* mf_last_error(void);
 MF_API const char* mf_version(void);
+/* Test hook: device allocations number first .. first+count-1, counted in this
+ * process from this call on, fail as if the device were full (MF_ERR_NOMEM)
+ * without reaching the driver.  count 0 turns it off. */
+MF_API void mf_debug_fail_device_allocations(int64_t first, int64_t count);
 
 /* ---- context (replaces main.cpp:26 cudaSetDevice and the per-class plans) - */
 MF_API int mf_context_create(int gpu, mf_context** out);
@@ -301,6 +305,11 @@ MF_API int mf_server_wait(mf_server* s, int64_t job_id, double timeout_s, mf_ali
  * completion, [2] p50 and [3] p99 latency (s), [4] peak admitted bytes, [5]
  * groups run, [6] mean group size, [7] seconds from first submit to last done. */
 MF_API int mf_server_stats(mf_server* s, double* out8);
+/* The memory budget: as created (budget0), as learned (budget_now: lowered to
+ * what the other requests held whenever a prepare or a group set-up found the
+ * device full while others held memory -- such a request is retried, not
+ * failed), and how many such retries there were.  Any output may be null. */
+MF_API int mf_server_memory(mf_server* s, size_t* budget0, size_t* budget_now, int64_t* retries);
 /* Finishes every submitted request, then releases the workers. */
 MF_API void mf_server_destroy(mf_server* s);
 

@@ -142,6 +142,10 @@ SIGNATURES = [
                                       ctypes.POINTER(AlignParamC), _c_int_p,
                                       ctypes.POINTER(ctypes.c_double)]),
     ("mf_server_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("mf_server_memory", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_int64)]),
+    ("mf_debug_fail_device_allocations", None, [ctypes.c_int64, ctypes.c_int64]),
     ("mf_server_destroy", None, [ctypes.c_void_p]),
     ("mf_dev_correct_proj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_float, ctypes.c_float,
@@ -614,7 +618,12 @@ class Server:
         _check(lib().mf_server_stats(self.h, out))
         keys = ("jobs", "series_per_min", "p50_s", "p99_s", "peak_bytes", "groups",
                 "mean_group", "span_s")
-        return dict(zip(keys, out))
+        st = dict(zip(keys, out))
+        b0, bn, r = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int64()
+        _check(lib().mf_server_memory(self.h, ctypes.byref(b0), ctypes.byref(bn),
+                                      ctypes.byref(r)))
+        st.update(budget_bytes=b0.value, learned_budget_bytes=bn.value, memory_retries=r.value)
+        return st
 
     def close(self):
         if getattr(self, "h", None) and _lib is not None:
@@ -623,6 +632,12 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def fail_device_allocations(first, count):
+    """Test hook: device allocations number first .. first+count-1, counted from
+    this call, fail as if the device were full; count 0 turns it off."""
+    lib().mf_debug_fail_device_allocations(int(first), int(count))
 
 
 def find_proj_range(angles, skip, iproj, nproj):

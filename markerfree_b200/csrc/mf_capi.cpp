@@ -36,6 +36,10 @@ extern "C" {
 MF_API const char* mf_last_error(void) { return mf::last_error(); }
 MF_API const char* mf_version(void) { return "markerfree-b200 0.1 (sm_100a)"; }
 
+MF_API void mf_debug_fail_device_allocations(int64_t first, int64_t count) {
+  fail_device_allocations(first, count);
+}
+
 MF_API int mf_context_create(int gpu, mf_context** out) {
   MF_GUARD_BEGIN
   if (!out) return set_error(MF_ERR_ARG, "null output pointer");

@@ -1,4 +1,5 @@
 // Error reporting and device buffers.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 
@@ -26,10 +27,21 @@ void set_alloc_stream(cudaStream_t s) { g_alloc_stream = s; }
 void set_free_stream(cudaStream_t s) { g_free_stream = s; }
 void set_sync_free(bool on) { g_sync_free = on; }
 
+static std::atomic<long long> g_alloc_seq{0}, g_fail_first{0}, g_fail_end{0};
+
+void fail_device_allocations(long long first, long long count) {
+  const long long base = g_alloc_seq.load();
+  g_fail_first = base + first;
+  g_fail_end = count > 0 ? base + first + count : 0;
+}
+
 int DevBuf::alloc(size_t n) {
   if (n == 0) n = 16;
   if (p && bytes >= n) return MF_OK;
   release();
+  const long long k = g_alloc_seq++;
+  if (k < g_fail_end && k >= g_fail_first)
+    return set_error(MF_ERR_NOMEM, "device allocation of %zu bytes failed: injected", n);
   st = g_alloc_stream;
   cudaError_t e = st ? cudaMallocAsync(&p, n, st) : cudaMalloc(&p, n);
   if (e != cudaSuccess) {

@@ -62,6 +62,8 @@ void set_alloc_stream(cudaStream_t s);
 // While set, buffers are released with a synchronous cudaFree (used when the
 // owning stream may already be gone).
 void set_sync_free(bool on);
+// Device allocations number first .. first+count-1 from now on fail (test hook).
+void fail_device_allocations(long long first, long long count);
 // The stream DevBuf::release frees on in this thread (null: each buffer's own).
 void set_free_stream(cudaStream_t s);
 

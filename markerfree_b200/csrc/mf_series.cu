@@ -102,8 +102,9 @@ int mf_context::plan(const std::vector<long long>& key, cufftHandle* out) {
   }
   if (r != CUFFT_SUCCESS) {
     cufftDestroy(h);
-    return set_error(MF_ERR_CUFFT, "cufftMakePlanMany(kind %lld, %d x %d, batch %d) failed: %d",
-                     kind, nx, ny, batch, (int)r);
+    return set_error(r == CUFFT_ALLOC_FAILED ? MF_ERR_NOMEM : MF_ERR_CUFFT,
+                     "cufftMakePlanMany(kind %lld, %d x %d, batch %d) failed: %d", kind, nx, ny,
+                     batch, (int)r);
   }
   if (ws > work_bytes[slot]) {
     // grow this stream's work area and point every plan of the stream at the new

@@ -18,6 +18,15 @@
 // Work of different workers overlaps on the GPU; a request that arrives while
 // others run is admitted as soon as memory frees up.  Each request's result is
 // the one it gets when aligned alone (groups keep per-series arithmetic).
+//
+// The byte estimate does not see everything a worker holds (cuFFT plans, the
+// operators of a group's distinct geometries, blocks cached by the stream-ordered
+// pool).  When a prepare or a group set-up still finds the device full while
+// other requests hold memory, the request is not failed: what it allocated is
+// given back, it returns to the head of its queue, the budget drops to what the
+// other requests hold (so the scheduler learns where the device really fills),
+// and a group that failed is retried at half the size.  Only a request that
+// finds the device full with nothing else on it fails.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -56,8 +65,18 @@ struct Job {
   std::vector<float> sx, sy, rot;
   float angle_offset = 0.0f;
   int passes = 0;
+  int64_t mem_wait = -1;  // finished-job count when a group set-up ran out of memory
   double t_submit = 0, t_admit = 0, t_ready = 0, t_done = 0;
 };
+
+// Return the blocks the stream-ordered pool caches to the device, once this
+// worker's own work has drained.
+void return_cached_memory(int gpu, cudaStream_t st) {
+  cudaStreamSynchronize(st);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
+}
 
 // Requests that may share a group: the same options of the projection-matching
 // stage that a group applies to all its series (any image size, tilt count and
@@ -85,8 +104,10 @@ size_t estimate_bytes(int nx, int ny, int nz, const mf_options& o) {
 
 struct mf_server {
   int gpu = 0;
-  size_t budget = 0, used = 0, peak_used = 0;
+  size_t budget0 = 0, budget = 0, used = 0, peak_used = 0;
   int max_group = 8;
+  int group_cap = kMaxGroup;  // lowered when a group set-up runs out of memory
+  int64_t done_count = 0, mem_retries = 0;
   double group_wait_s = 0.05;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -95,6 +116,7 @@ struct mf_server {
   std::vector<Job*> admitted;  // waiting for a prepare task
   std::vector<Job*> ready;     // prepared, waiting for a group
   int preparing = 0;
+  int matching = 0;  // groups being matched
   int64_t next_id = 1;
   bool stop = false;
   std::vector<mf_context*> ctxs;
@@ -126,8 +148,12 @@ struct mf_server {
     *wait_s = 0.25;
     const double t = now_s();
     // ready jobs grouped by the options a group shares, oldest first
+    // (a job whose group ran out of memory waits for some job to finish, or for
+    // the device to go idle)
+    const bool idle = preparing == 0 && matching == 0;
     std::map<std::vector<float>, std::vector<Job*>> by_shape;
-    for (Job* j : ready) by_shape[group_key(j)].push_back(j);
+    for (Job* j : ready)
+      if (j->mem_wait != done_count || idle) by_shape[group_key(j)].push_back(j);
     auto coming = [&](const std::vector<float>& key) {
       for (Job* j : admitted)
         if (group_key(j) == key) return true;
@@ -136,12 +162,13 @@ struct mf_server {
       return preparing > 0;
     };
     auto take = [&](std::vector<Job*>& v) {
-      const int m = std::min((int)v.size(), max_group);
+      const int m = std::min((int)v.size(), std::min(max_group, group_cap));
       group->assign(v.begin(), v.begin() + m);
       for (Job* j : *group) {
         j->state = kMatching;
         ready.erase(std::find(ready.begin(), ready.end(), j));
       }
+      matching++;
       return true;
     };
     for (auto& kv : by_shape)
@@ -150,7 +177,8 @@ struct mf_server {
     // 1. a full group, or one whose oldest job has waited too long, runs first
     const double starve_s = 20.0 * group_wait_s;
     for (auto& kv : by_shape)
-      if ((int)kv.second.size() >= max_group || t - kv.second.front()->t_ready >= starve_s)
+      if ((int)kv.second.size() >= std::min(max_group, group_cap) ||
+          t - kv.second.front()->t_ready >= starve_s)
         return take(kv.second);
     // 2. preparing admitted jobs comes next: it lets more jobs join the
     //    ready groups, so the matching that follows runs on larger groups
@@ -182,6 +210,7 @@ struct mf_server {
     j->state = kDone;
     j->t_done = now_s();
     used -= j->bytes;
+    done_count++;
     last_done = j->t_done;
     latencies.push_back(j->t_done - j->t_submit);
   }
@@ -211,12 +240,25 @@ struct mf_server {
         }
         if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
           rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
+        if (rc == MF_ERR_NOMEM) {
+          mf_series_destroy(prep->s);
+          prep->s = nullptr;
+          return_cached_memory(gpu, ctx->c.stream);
+        }
         lk.lock();
         preparing--;
         if (rc == MF_OK) {
           prep->state = kReady;
           prep->t_ready = now_s();
           ready.push_back(prep);
+        } else if (rc == MF_ERR_NOMEM && used > prep->bytes) {
+          // the others hold the memory it needs: back to the head of the queue,
+          // admitted again once enough of them have finished
+          used -= prep->bytes;
+          budget = std::min(budget, used);
+          prep->state = kQueued;
+          queued.push_front(prep);
+          mem_retries++;
         } else {
           finish_locked(prep, rc);
           cv_done.notify_all();
@@ -237,8 +279,33 @@ struct mf_server {
       if (o.align_z != 0) {
         mf_group* g = nullptr;
         rc = group_create(ctx, ss.data(), (int)ss.size(), o.zshift, align_z.data(), o.nproj, &g);
-        if (rc == MF_OK) rc = group_proj_align(g, passes.data());
-        delete g;
+        if (rc == MF_ERR_NOMEM) {
+          // set-up allocates everything before any series changes: nothing to undo
+          delete g;
+          return_cached_memory(gpu, ctx->c.stream);
+          lk.lock();
+          size_t gb = 0;
+          for (Job* j : group) gb += j->bytes;
+          // others that will give memory back: requests being prepared or matched
+          const bool others = preparing > 0 || matching > 1;
+          if (others || group.size() > 1) {
+            if (group.size() > 1) group_cap = std::max(1, (int)group.size() / 2);
+            if (used > gb) budget = std::min(budget, used);
+            for (Job* j : group) {
+              j->state = kReady;
+              j->mem_wait = others ? done_count : -1;
+              ready.push_back(j);
+            }
+            matching--;
+            mem_retries++;
+            cv_work.notify_all();
+            continue;
+          }
+          lk.unlock();
+        } else if (rc == MF_OK) {
+          rc = group_proj_align(g, passes.data());
+          delete g;
+        }
       }
       std::vector<int> rcs(group.size(), rc);
       for (size_t i = 0; i < group.size(); ++i) {
@@ -255,6 +322,7 @@ struct mf_server {
       if (cudaStreamSynchronize(ctx->c.stream) != cudaSuccess && rc == MF_OK)
         for (int& r : rcs) r = set_error(MF_ERR_CUDA, "stream synchronize failed");
       lk.lock();
+      matching--;
       groups++;
       grouped_jobs += (int64_t)group.size();
       for (size_t i = 0; i < group.size(); ++i) finish_locked(group[i], rcs[i]);
@@ -288,7 +356,7 @@ MF_API int mf_server_create(int gpu, size_t hbm_budget, int max_group, int worke
   }
   std::unique_ptr<mf_server> s(new mf_server());
   s->gpu = gpu;
-  s->budget = hbm_budget;
+  s->budget0 = s->budget = hbm_budget;
   s->max_group = max_group;
   s->group_wait_s = group_wait_ms / 1000.0;
   for (int w = 0; w < workers; ++w) {
@@ -328,9 +396,9 @@ MF_API int mf_server_submit(mf_server* s, const float* raw, int nx, int ny, int 
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return set_error(MF_ERR_STATE, "server is shutting down");
-    if (j->bytes > s->budget)
+    if (j->bytes > s->budget0)
       return set_error(MF_ERR_NOMEM, "request needs about %zu bytes, budget is %zu", j->bytes,
-                       s->budget);
+                       s->budget0);
     j->id = s->next_id++;
     j->t_submit = now_s();
     if (s->first_submit < 0) s->first_submit = j->t_submit;
@@ -385,6 +453,16 @@ MF_API int mf_server_stats(mf_server* s, double* out8) {
   out8[5] = (double)s->groups;
   out8[6] = s->groups ? (double)s->grouped_jobs / (double)s->groups : 0.0;
   out8[7] = span;
+  return MF_OK;
+}
+
+MF_API int mf_server_memory(mf_server* s, size_t* budget0, size_t* budget_now,
+                            int64_t* retries) {
+  if (!s) return set_error(MF_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (budget0) *budget0 = s->budget0;
+  if (budget_now) *budget_now = s->budget;
+  if (retries) *retries = s->mem_retries;
   return MF_OK;
 }
 
