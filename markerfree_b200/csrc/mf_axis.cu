@@ -274,21 +274,31 @@ __device__ __forceinline__ void radon_line(const float* __restrict__ proj, int s
 // loop then runs without bounds tests; the samples taken and their order (left
 // to right, as the reference's two loops) are unchanged.
 //
-// Neighbouring threads take neighbouring lines, whose samples at one x lie one
+// Neighbouring lanes take neighbouring lines, whose samples at one x lie one
 // step of (-sin, cos) apart.  For a steep candidate (|sin| >= |cos|) that step
 // runs along an image row, so a warp reads one row segment from the row-major
 // stack; otherwise it runs along a column and the warp reads the column-major copy
 // `stack_t` instead.  Both hold the same values: only the address changes.
-__global__ void k_radon(const float* __restrict__ stack, const float* __restrict__ stack_t,
-                        const int* __restrict__ neg, int width, int height, int L, int num,
-                        const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
-                        const float* __restrict__ sxs, const float* __restrict__ sys,
-                        const int* __restrict__ region, float* __restrict__ lines,
-                        unsigned long long* __restrict__ samples) {
-  int y = blockIdx.y * blockDim.x + threadIdx.x;
-  int b = blockIdx.x;
-  int z = blockIdx.z;
-  if (y >= L) return;
+// The warps of a block take the same 32 lines of kRadonCand neighbouring
+// candidates: their lines differ by a fraction of a degree, so at each x they
+// gather from nearly the same pixels, and the block's warps share those cache
+// lines in L1 instead of each fetching them from L2.
+#ifndef MF_RADON_CAND
+#define MF_RADON_CAND 4
+#endif
+constexpr int kRadonCand = MF_RADON_CAND;  // candidates (warps) per block
+
+__global__ void __launch_bounds__(32 * kRadonCand)
+    k_radon(const float* __restrict__ stack, const float* __restrict__ stack_t,
+            const int* __restrict__ neg, int width, int height, int L, int num,
+            const float2* __restrict__ cs, const float* __restrict__ tilt_cos,
+            const float* __restrict__ sxs, const float* __restrict__ sys,
+            const int* __restrict__ region, float* __restrict__ lines,
+            unsigned long long* __restrict__ samples) {
+  const int y = blockIdx.y * 32 + (threadIdx.x & 31);
+  const int b = blockIdx.x * kRadonCand + (threadIdx.x >> 5);
+  const int z = blockIdx.z;
+  if (y >= L || b >= num) return;
   RadonLine ln;
   ln.s = cs[b].y;
   ln.c = cs[b].x;
@@ -309,7 +319,7 @@ __global__ void k_radon(const float* __restrict__ stack, const float* __restrict
   float sum;
   int cnt;
   const bool nonneg = neg != nullptr && neg[z] == 0;
-  if (stack_t != nullptr && fabsf(ln.c) > fabsf(ln.s)) {  // uniform over the block
+  if (stack_t != nullptr && fabsf(ln.c) > fabsf(ln.s)) {  // uniform over the warp
     if (nonneg)
       radon_line<true, true>(stack_t + off, height, ln, lo, hi, &sum, &cnt);
     else
@@ -523,7 +533,8 @@ int tilt_axis_scores_enqueue(Context* c, cufftHandle plan, const float* stack,
     MF_CHECK_CUDA(cudaEventCreate(&J->ev[1]));
     MF_CHECK_CUDA(cudaEventRecord(J->ev[0], st));
   }
-  k_radon<<<dim3(num, (L + 127) / 128, nz), 128, 0, st>>>(
+  k_radon<<<dim3((num + kRadonCand - 1) / kRadonCand, (L + 31) / 32, nz), 32 * kRadonCand, 0,
+             st>>>(
       stack, stack_t, d_neg, nx, ny, L, num, cs.as<float2>(), tcos.as<float>(),
       d_sx.as<float>(), d_sy.as<float>(), region.as<int>(), lines.as<float>(),
       count.as<unsigned long long>());

@@ -926,6 +926,25 @@ int build_reproj_tc_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, in
   return MF_OK;
 }
 
+// Packed FP32 pairs for fma.rn.f32x2 (sm_100): each lane is the scalar IEEE
+// fused multiply-add, so a pair of accumulators advances exactly as two fmaf.
+__device__ __forceinline__ unsigned long long f2pack(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 f2unpack(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Operator apply: out[y][x] = sum_r A[y][r] * B_t[r][x] with A gathered from the
 // neighbour rows through rowmap.  One CTA computes a kApplyTileY x kOpTileX
@@ -934,6 +953,7 @@ int build_reproj_tc_ops_any(Context* c, const std::vector<ReprojGeom>& geoms, in
 // next chunk's global loads are issued before the current chunk's FMAs, so
 // memory latency hides behind arithmetic.  Every loaded neighbour value is
 // tested for the -1e30 sentinel; a hit flags the row tile for the exact path.
+// The multiply-adds run as packed pairs (fma.rn.f32x2), lane for lane fmaf.
 constexpr int kApplyThreads = 256;
 constexpr int kAPerThread = kOpChunk * kApplyTileY / kApplyThreads;  // 8
 
@@ -967,11 +987,11 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
   const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;  // 16 x 4 columns, 16 x 8 rows
   if (tid == 0) s_flag = 0;
-  float acc[8][4];
+  unsigned long long acc2[8][2];  // columns 2h, 2h + 1 of row i (packed FMA pairs)
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    for (int h = 0; h < 2; ++h) acc2[i][h] = 0ull;
   const int lr = tid % kOpChunk;  // operator row this thread loads for A
   const int ly = tid / kOpChunk;  // first y row it loads (then every 16th)
   bool bad = false;
@@ -1009,15 +1029,26 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
       const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][rr][ty * 8 + 4]);
       const float4 b = *reinterpret_cast<const float4*>(&Bs[buf][rr][tx * 4]);
       const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[4] = {b.x, b.y, b.z, b.w};
+      const unsigned long long bp[2] = {f2pack(b.x, b.y), f2pack(b.z, b.w)};
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 8; ++i) {
+        const unsigned long long ap = f2pack(av[i], av[i]);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        for (int h = 0; h < 2; ++h) acc2[i][h] = ffma2(ap, bp[h], acc2[i][h]);
+      }
     }
     if (c + 1 < nchunks) store_chunk(buf ^ 1);
     __syncthreads();
   }
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float2 v = f2unpack(acc2[i][h]);
+      acc[i][2 * h] = v.x;
+      acc[i][2 * h + 1] = v.y;
+    }
   if (bad) s_flag = 1;
   __syncthreads();
   if (tid == 0 && s_flag) atomicOr(&rowflags[blockIdx.y], 1);
@@ -1064,6 +1095,10 @@ int launch_reproject_apply(Context* c, const ReprojOpView& op, const float* corr
 // with no staging registers.  Sentinels are not tested here: the per-(tilt,
 // 128-row tile) flags of the corrected stack (k_flag_tiles_group) send the tiles
 // whose neighbours hold a -1e30 to the exact path, which overwrites them.
+// The multiply-adds run as packed pairs (fma.rn.f32x2, two columns per
+// instruction), lane for lane the fmaf of the scalar form in the same order, so
+// the output is bit for bit that of one fmaf chain per output over the operator
+// rows, with half the FMA instructions to issue.
 constexpr int kA2Y = 256;        // image rows per CTA
 constexpr int kA2Stages = 3;     // cp.async ring depth
 constexpr int kA2Pitch = 260;    // floats per operator row of the A tile (256 + 4)
@@ -1120,11 +1155,12 @@ __global__ void __launch_bounds__(256, 2)
                coef + (size_t)row * kOpTileX + tid * 4);
   };
   const int tx = tid % 8, ty = tid / 8;
-  float acc[8][8];
+  // acc2[i][h] holds the accumulators of columns 2h and 2h + 1 of row i
+  unsigned long long acc2[8][4];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    for (int h = 0; h < 4; ++h) acc2[i][h] = 0ull;
 #pragma unroll
   for (int c = 0; c < kA2Stages - 1; ++c) {
     if (c < nchunks) load(c);
@@ -1144,14 +1180,26 @@ __global__ void __launch_bounds__(256, 2)
       const float4 b0 = *reinterpret_cast<const float4*>(Bt + rr * kOpTileX + tx * 4);
       const float4 b1 = *reinterpret_cast<const float4*>(Bt + rr * kOpTileX + 32 + tx * 4);
       const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      const unsigned long long bp[4] = {f2pack(b0.x, b0.y), f2pack(b0.z, b0.w),
+                                        f2pack(b1.x, b1.y), f2pack(b1.z, b1.w)};
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 8; ++i) {
+        const unsigned long long ap = f2pack(av[i], av[i]);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        for (int h = 0; h < 4; ++h) acc2[i][h] = ffma2(ap, bp[h], acc2[i][h]);
+      }
     }
   }
   cp_async_wait<0>();
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const float2 v = f2unpack(acc2[i][h]);
+      acc[i][2 * h] = v.x;
+      acc[i][2 * h + 1] = v.y;
+    }
   int cv[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -76,6 +77,23 @@ void return_cached_memory(int gpu, cudaStream_t st) {
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   cudaGetLastError();
+}
+
+// The device's memory state, appended to an out-of-memory failure.
+std::string memory_report(int gpu) {
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  uint64_t reserved = 0, in_use = 0;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) {
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &in_use);
+  }
+  cudaGetLastError();
+  char b[200];
+  snprintf(b, sizeof(b), " [device: %.2f GB free of %.2f; pool %.2f GB reserved, %.2f in use]",
+           fr / 1e9, tot / 1e9, reserved / 1e9, in_use / 1e9);
+  return b;
 }
 
 // Requests that may share a group: the same options of the projection-matching
@@ -203,6 +221,12 @@ struct mf_server {
   void finish_locked(Job* j, int rc) {
     j->rc = rc;
     if (rc != MF_OK) j->err = mf_last_error();
+    if (rc == MF_ERR_NOMEM) {
+      char b[160];
+      snprintf(b, sizeof(b), " [server: %.2f GB admitted of a %.2f GB budget (%.2f as created)]",
+               used / 1e9, budget / 1e9, budget0 / 1e9);
+      j->err += b + memory_report(gpu);
+    }
     if (j->s) {
       mf_series_destroy(j->s);
       j->s = nullptr;
@@ -231,19 +255,29 @@ struct mf_server {
       }
       lk.unlock();
       if (prep) {
-        int rc = mf_series_create(ctx, prep->raw, prep->nx, prep->ny, prep->nz,
-                                  prep->angles.data(), &prep->s);
-        if (rc == MF_OK) {
-          prep->s->precision = (mf_precision)prep->opt.precision;
-          if (prep->opt.align_z != 0)
-            rc = coarse_align(prep->s, prep->opt.pitch_angle, prep->opt.offset);
-        }
-        if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
-          rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
-        if (rc == MF_ERR_NOMEM) {
+        int rc = MF_OK;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+          rc = mf_series_create(ctx, prep->raw, prep->nx, prep->ny, prep->nz,
+                                prep->angles.data(), &prep->s);
+          if (rc == MF_OK) {
+            prep->s->precision = (mf_precision)prep->opt.precision;
+            if (prep->opt.align_z != 0)
+              rc = coarse_align(prep->s, prep->opt.pitch_angle, prep->opt.offset);
+          }
+          if (rc == MF_OK && cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
+            rc = set_error(MF_ERR_CUDA, "stream synchronize failed");
+          if (rc != MF_ERR_NOMEM) break;
+          // give back what it holds and what the pool caches; with no other request
+          // holding memory, try once more before failing
           mf_series_destroy(prep->s);
           prep->s = nullptr;
           return_cached_memory(gpu, ctx->c.stream);
+          bool alone;
+          {
+            std::lock_guard<std::mutex> g(mu);
+            alone = used <= prep->bytes;
+          }
+          if (!alone) break;
         }
         lk.lock();
         preparing--;
@@ -405,6 +439,7 @@ MF_API int mf_server_submit(mf_server* s, const float* raw, int nx, int ny, int 
     *job_id = j->id;
     s->queued.push_back(j.get());
     s->jobs[j->id] = std::move(j);
+    s->admit_locked();  // admitted now if it fits, not only when a worker asks
   }
   s->cv_work.notify_all();
   return MF_OK;

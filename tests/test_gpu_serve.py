@@ -88,8 +88,10 @@ def test_served_requests_survive_a_full_device(ctx, mflib, first, count):
              for s, k in zip(reqs, kw)]
     srv = mflib.Server(gpu=0, hbm_budget=0, max_group=4, workers=2, group_wait_ms=30.0)
     try:
-        mflib.fail_device_allocations(first, count)
+        # every request is queued before the failures start, so that others hold
+        # memory when one meets them (a request alone on a full device fails)
         ids = [srv.submit(s.stack, s.angles, **k) for s, k in zip(reqs, kw)]
+        mflib.fail_device_allocations(first, count)
         got = [srv.wait(j) for j in ids]
         st = srv.stats()
     finally:
