@@ -287,6 +287,23 @@ def _time_steps(stream, fn, steps):
     return sum(a.elapsed_time(b) for a, b in evs)
 
 
+def device_memory(dev):
+    """Device memory in GB: free, torch's cache, and the stream-ordered pool the
+    library allocates from (reserved / in use; needs cuda-python)."""
+    import torch
+    free, total = torch.cuda.mem_get_info(dev)
+    out = f"free {free / 1e9:.1f}/{total / 1e9:.1f} GB, torch {torch.cuda.memory_reserved(dev) / 1e9:.1f}"
+    try:
+        from cuda.bindings import runtime as rt
+        _, pool = rt.cudaDeviceGetDefaultMemPool(dev)
+        _, res = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+        _, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+        out += f", pool {int(res) / 1e9:.1f} reserved / {int(used) / 1e9:.1f} in use"
+    except Exception:  # cuda-python absent
+        pass
+    return out
+
+
 def served_pool(dev):
     """Distinct seeded series for the serving run, by size class (2048^2, 1024^2,
     4096^2), each drawn like the uneven batch (synth.uneven_params with the size
@@ -346,6 +363,8 @@ def served_run(mf, dev, n_req, precision, seed=5):
         st_cap = srv.stats()
     finally:
         srv.close()
+        print(f"[bench] serving capacity run over | {device_memory(dev)}", file=sys.stderr,
+              flush=True)
     cap_spm = 60.0 * n_req / makespan
     cap_eq = 60.0 * sum(weight[k] for k in kinds) / makespan
     # latency: Poisson arrivals at 80% of the capacity just measured
@@ -440,7 +459,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", dev))
         pg = dist
-    log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
+
+    def log(m):
+        print(f"[bench] {m} | {device_memory(dev)}", file=sys.stderr, flush=True)
     B = args.batch
     series = make_batch(B, f"cuda:{dev}", args.scale)
     s0 = series[0]

@@ -35,7 +35,7 @@ struct GroupMember {
   int bin = 1, xb = 0, yb = 0, pad = 0, cmp = 0, thick = 0, ytiles = 0, xpitch = 0;
   int out_x = 0, binx = 1, biny = 1;
   size_t bpix = 0, ppix = 0;
-  DevBuf corr, scratch, reproj, cc, recorr, recorr_out, mpart, stats, ppart, corr16, tflags;
+  DevBuf corr, scratch, reproj, cc, recorr, mpart, stats, ppart, corr16, tflags;
   const float* mask = nullptr;
   TmaDesc imgmap;
   std::vector<int> order;
@@ -79,21 +79,6 @@ struct mf_group {
 };
 
 namespace mf {
-
-// corr[b][ip_b] = recorr_out[b] for the series with a held-out tilt at the step
-__global__ void k_group_scatter(const GroupSeriesDev* __restrict__ ser,
-                                const GroupStepDev* __restrict__ steps,
-                                const int* __restrict__ active) {
-  const int b = blockIdx.y;
-  if (active[b] == 0 || steps[b].ip < 0) return;
-  const GroupSeriesDev& S = ser[b];
-  const float4* s = reinterpret_cast<const float4*>(S.recorr_out);
-  float4* d = reinterpret_cast<float4*>(S.corr + (size_t)steps[b].ip * S.bpix);
-  const size_t n4 = S.bpix / 4;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4;
-       i += (size_t)gridDim.x * blockDim.x)
-    d[i] = s[i];
-}
 
 // ProjAlign::Setsize (ProjAlign.cpp:48-125) and CorrTomoStack's sizes
 // (CorrStack.cu:65-100) of one series.
@@ -209,7 +194,6 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     MF_TRY(M.reproj.alloc(sizeof(float) * M.bpix));
     MF_TRY(M.cc.alloc(sizeof(float) * M.ppix * 2));
     MF_TRY(M.recorr.alloc(sizeof(float) * M.ppix));
-    MF_TRY(M.recorr_out.alloc(sizeof(float) * M.bpix));
     MF_TRY(M.mpart.alloc(sizeof(double2) * moment_parts(M.yb) * 2));
     MF_TRY(M.stats.alloc(sizeof(float2) * 2));
     MF_TRY(M.ppart.alloc(sizeof(float2) * kPeakParts));
@@ -293,7 +277,6 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
     d.reproj = M.reproj.as<float>();
     d.cc = M.cc.as<float>();
     d.recorr = M.recorr.as<float>();
-    d.recorr_out = M.recorr_out.as<float>();
     d.mask = M.mask;
     d.mpart = M.mpart.as<double2>();
     d.stats = M.stats.as<float2>();
@@ -516,14 +499,13 @@ static int group_enqueue(mf_group* g) {
       return MF_OK;
     }));
     MF_TRY(launch_rweight_group(c, ser, sk, active, B, g->cmp_max, g->yb_max, st));
+    // the inverse row transforms write the re-corrected tilt into its place in
+    // the corrected stack (nothing reads the old one after the measurement)
     MF_TRY(fft_stage(k, [&](GroupMember& M, int i) -> int {
       MF_CHECK_CUFFT(cufftExecC2R(M.rows_inv_one[i], (cufftComplex*)M.recorr.as<float>(),
-                                  M.recorr_out.as<float>()));
+                                  M.corr.as<float>() + (size_t)M.order[k] * M.bpix));
       return MF_OK;
     }));
-    k_group_scatter<<<dim3(64, B), 256, 0, st>>>(ser, sk, active);
-    c->launches++;
-    MF_CHECK_CUDA(cudaGetLastError());
     if (tc)
       MF_TRY(launch_to_half_group(c, ser, sk, active, B, g->nz_max, g->ytiles_max, g->prec, st));
     else

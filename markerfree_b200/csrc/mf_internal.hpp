@@ -388,7 +388,6 @@ struct GroupSeriesDev {
   float* reproj;       // yb x xb: re-projection of the step's held-out tilt
   float* cc;           // 2 x yb x pad: the normalised pair, then spectrum / correlation
   float* recorr;       // yb x pad: re-corrected held-out tilt before its R-weight
-  float* recorr_out;   // yb x xb
   const float* mask;   // yb x xb round-edge factors of the correlation mask
   double2* mpart;      // 2 x moment_parts(yb) moment partials
   float2* stats;       // 2: (mean, std) of the pair

@@ -293,6 +293,7 @@ struct OpGeomDev {
   int lohi_off;  // int offset of this tilt's lo/hi arrays (xb * nk each)
   int tile_off;  // first OpTile of this tilt
   int seg_off;   // first int2 of this tilt's segment table (ntiles * nk)
+  int i0;        // absolute index of the first neighbour tilt
 };
 
 __global__ void k_op_scan(int xb, const OpGeomDev* __restrict__ geoms,
@@ -331,6 +332,102 @@ __global__ void k_op_scan(int xb, const OpGeomDev* __restrict__ geoms,
     }
   }
   cnt[(size_t)blockIdx.y * xb + bx] = n;
+}
+
+// Layout of the operator rows, on the device.  For (tilt i, x-tile t) and each
+// neighbour k, the bins touched by the tile's columns are [min lo, max hi]; they
+// become consecutive rows of the tile, neighbour after neighbour, and the tile's
+// rows are padded to a whole number of kOpChunk (at least one chunk).
+// seg[seg_off + t*nk + k] = (row offset within the tile, first bin), segn = its
+// row count (0 when the neighbour touches nothing).
+__global__ void k_op_tiles(int xb, int ntiles, int n, const OpGeomDev* __restrict__ geoms,
+                           const int* __restrict__ lo, const int* __restrict__ hi,
+                           int2* __restrict__ seg, int* __restrict__ segn,
+                           int* __restrict__ tile_rows, int* __restrict__ tile_used) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n * ntiles) return;
+  const int i = q / ntiles, t = q % ntiles;
+  const OpGeomDev g = geoms[i];
+  const int nk = g.nk;
+  const int x0 = t * kOpTileX, x1 = min(xb, x0 + kOpTileX);
+  const int* lo_t = lo + g.lohi_off;
+  const int* hi_t = hi + g.lohi_off;
+  int rows = 0;
+  for (int k = 0; k < nk; ++k) {
+    int l = INT_MAX, h = -1;
+    for (int x = x0; x < x1; ++x) {
+      l = min(l, lo_t[(size_t)x * nk + k]);
+      h = max(h, hi_t[(size_t)x * nk + k]);
+    }
+    const size_t e = (size_t)g.seg_off + (size_t)t * nk + k;
+    if (h < 0) {
+      seg[e] = make_int2(rows, 0);
+      segn[e] = 0;
+      continue;
+    }
+    seg[e] = make_int2(rows, l);
+    segn[e] = h - l + 1;
+    rows += h - l + 1;
+  }
+  int padded = (rows + kOpChunk - 1) / kOpChunk * kOpChunk;
+  if (padded == 0) padded = kOpChunk;
+  tile_rows[q] = padded;
+  tile_used[q] = rows;
+}
+
+// Exclusive prefix sum of count ints in one block of 1024 threads:
+// out[j] = sum of in[0..j), out[count] = the total.
+__global__ void __launch_bounds__(1024) k_scan_rows(int count, const int* __restrict__ in,
+                                                    int* __restrict__ out) {
+  __shared__ long long part[1024];
+  const int tid = threadIdx.x;
+  const int per = (count + 1023) / 1024;
+  const int b = min(count, tid * per), e = min(count, b + per);
+  long long sum = 0;
+  for (int j = b; j < e; ++j) sum += in[j];
+  part[tid] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan
+    const long long v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  long long run = part[tid] - sum;
+  for (int j = b; j < e; ++j) {
+    out[j] = (int)run;
+    run += in[j];
+  }
+  if (tid == 1023) out[count] = (int)part[1023];
+}
+
+// Per (tilt, x-tile) block: its OpTile and its rows' (tilt, bin) map; padding
+// rows point at bin 0 of the first neighbour (their coefficients stay zero).
+__global__ void k_op_layout(int ntiles, const OpGeomDev* __restrict__ geoms,
+                            const int2* __restrict__ seg, const int* __restrict__ segn,
+                            const int* __restrict__ tile_rows, const int* __restrict__ tile_used,
+                            const int* __restrict__ row0, OpTile* __restrict__ tiles,
+                            int2* __restrict__ rowmap) {
+  const int q = blockIdx.x;
+  const int i = q / ntiles, t = q % ntiles;
+  const OpGeomDev g = geoms[i];
+  const int r0 = row0[q], rows = tile_rows[q], used = tile_used[q];
+  if (threadIdx.x == 0) {
+    OpTile ot;
+    ot.row0 = r0;
+    ot.rows = rows;
+    tiles[q] = ot;
+  }
+  const size_t e0 = (size_t)g.seg_off + (size_t)t * g.nk;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    int2 m = make_int2(g.i0, 0);
+    if (r < used) {
+      int k = 0;
+      while (k + 1 < g.nk && (segn[e0 + k] == 0 || r >= seg[e0 + k].x + segn[e0 + k])) ++k;
+      m = make_int2(g.i0 + k, seg[e0 + k].y + (r - seg[e0 + k].x));
+    }
+    rowmap[(size_t)r0 + r] = m;
+  }
 }
 
 // Pass 2: accumulate coefficients.  seg[t*nk + k] = (row offset within the tile,
@@ -394,6 +491,7 @@ int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpS
   std::vector<OpGeomDev> gd(n);
   std::vector<float> bps;
   int lohi = 0, nkmax = 0;
+  size_t nseg = 0;
   for (int i = 0; i < n; ++i) {
     const ReprojGeom& g = geoms[i];
     gd[i].nk = g.nk;
@@ -404,17 +502,25 @@ int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpS
     gd[i].fsin = g.fsin;
     gd[i].lohi_off = lohi;
     gd[i].tile_off = i * ntiles;
-    gd[i].seg_off = 0;  // set below
+    gd[i].seg_off = (int)nseg;
+    gd[i].i0 = g.i0;
     bps.insert(bps.end(), g.bp.begin(), g.bp.end());
     lohi += xb * g.nk;
+    nseg += (size_t)ntiles * g.nk;
     nkmax = std::max(nkmax, g.nk);
   }
-  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi;
+  const int nt_all = n * ntiles;
+  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi, d_seg, d_segn, d_trows, d_tused, d_row0;
   MF_TRY(d_geom.alloc(sizeof(OpGeomDev) * n));
   MF_TRY(d_bp.alloc(sizeof(float) * bps.size()));
   MF_TRY(d_cnt.alloc(sizeof(int) * (size_t)n * xb));
   MF_TRY(d_lo.alloc(sizeof(int) * (size_t)lohi));
   MF_TRY(d_hi.alloc(sizeof(int) * (size_t)lohi));
+  MF_TRY(d_seg.alloc(sizeof(int2) * std::max<size_t>(nseg, 1)));
+  MF_TRY(d_segn.alloc(sizeof(int) * std::max<size_t>(nseg, 1)));
+  MF_TRY(d_trows.alloc(sizeof(int) * nt_all));
+  MF_TRY(d_tused.alloc(sizeof(int) * nt_all));
+  MF_TRY(d_row0.alloc(sizeof(int) * (nt_all + 1)));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
                                 cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_bp.p, bps.data(), sizeof(float) * bps.size(),
@@ -422,81 +528,45 @@ int build_reproj_ops(Context* c, const std::vector<ReprojGeom>& geoms, ReprojOpS
   k_op_scan<<<dim3((xb + 127) / 128, n), 128, 0, st>>>(xb, d_geom.as<OpGeomDev>(),
                                                        d_bp.as<float>(), d_cnt.as<int>(),
                                                        d_lo.as<int>(), d_hi.as<int>());
-  c->launches++;
+  k_op_tiles<<<(nt_all + 127) / 128, 128, 0, st>>>(
+      xb, ntiles, n, d_geom.as<OpGeomDev>(), d_lo.as<int>(), d_hi.as<int>(), d_seg.as<int2>(),
+      d_segn.as<int>(), d_trows.as<int>(), d_tused.as<int>());
+  k_scan_rows<<<1, 1024, 0, st>>>(nt_all, d_trows.as<int>(), d_row0.as<int>());
+  c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
-  std::vector<int> lo(lohi), hi(lohi);
-  MF_CHECK_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
+  // the host needs only the row offsets (allocation size, per-tilt row counts)
+  std::vector<int> row0(nt_all + 1);
+  MF_CHECK_CUDA(cudaMemcpyAsync(row0.data(), d_row0.p, sizeof(int) * (nt_all + 1),
+                                cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  // Tile layout of every tilt, rows concatenated across tilts.
-  std::vector<OpTile> tiles((size_t)n * ntiles);
-  std::vector<int2> seg;
-  std::vector<int2> rowmap;
-  int total = 0;
+  const int total = row0[nt_all];
   for (int i = 0; i < n; ++i) {
     const ReprojGeom& g = geoms[i];
-    const int nk = g.nk;
-    gd[i].seg_off = (int)seg.size();
-    seg.resize(seg.size() + (size_t)ntiles * nk);
-    const int* lo_t = lo.data() + gd[i].lohi_off;
-    const int* hi_t = hi.data() + gd[i].lohi_off;
-    int first_row = total;
-    for (int t = 0; t < ntiles; ++t) {
-      int x0 = t * kOpTileX, x1 = std::min(xb, x0 + kOpTileX);
-      int rows = 0;
-      for (int k = 0; k < nk; ++k) {
-        int l = INT_MAX, h = -1;
-        for (int x = x0; x < x1; ++x) {
-          l = std::min(l, lo_t[(size_t)x * nk + k]);
-          h = std::max(h, hi_t[(size_t)x * nk + k]);
-        }
-        int2& sgk = seg[gd[i].seg_off + (size_t)t * nk + k];
-        if (h < 0) {
-          sgk = make_int2(rows, 0);
-          continue;
-        }
-        sgk = make_int2(rows, l);
-        for (int b = l; b <= h; ++b) rowmap.push_back(make_int2(g.i0 + k, b));
-        rows += h - l + 1;
-      }
-      int padded = (rows + kOpChunk - 1) / kOpChunk * kOpChunk;
-      if (padded == 0) padded = kOpChunk;
-      for (int r = rows; r < padded; ++r) rowmap.push_back(make_int2(g.i0, 0));
-      tiles[(size_t)i * ntiles + t].row0 = total;
-      tiles[(size_t)i * ntiles + t].rows = padded;
-      total += padded;
-    }
     ReprojOpView v;
     v.ip = g.ip;
     v.i0 = g.i0;
-    v.nk = nk;
+    v.nk = g.nk;
     v.xb = xb;
     v.yb = yb;
     v.ntiles = ntiles;
-    v.total_rows = total - first_row;
+    v.total_rows = row0[(i + 1) * ntiles] - row0[i * ntiles];
     set->ops.push_back(v);
-    set->bytes += 4.0 * (double)xb * yb * (nk + 1) + (double)v.total_rows * (kOpTileX * 4 + 8);
+    set->bytes += 4.0 * (double)xb * yb * (g.nk + 1) + (double)v.total_rows * (kOpTileX * 4 + 8);
     set->fma += (double)yb * v.total_rows * kOpTileX;
   }
   MF_TRY(set->coef.alloc(sizeof(float) * (size_t)total * kOpTileX));
   MF_TRY(set->rowmap.alloc(sizeof(int2) * (size_t)total));
-  MF_TRY(set->tiles.alloc(sizeof(OpTile) * tiles.size()));
+  MF_TRY(set->tiles.alloc(sizeof(OpTile) * nt_all));
   MF_TRY(set->colvalid.alloc(sizeof(int) * (size_t)n * xb));
-  DevBuf d_seg;
-  MF_TRY(d_seg.alloc(sizeof(int2) * seg.size()));
   MF_CHECK_CUDA(cudaMemsetAsync(set->coef.p, 0, sizeof(float) * (size_t)total * kOpTileX, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(set->rowmap.p, rowmap.data(), sizeof(int2) * rowmap.size(),
-                                cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(set->tiles.p, tiles.data(), sizeof(OpTile) * tiles.size(),
-                                cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(d_seg.p, seg.data(), sizeof(int2) * seg.size(),
-                                cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
-                                cudaMemcpyHostToDevice, st));
+  k_op_layout<<<nt_all, 128, 0, st>>>(ntiles, d_geom.as<OpGeomDev>(), d_seg.as<int2>(),
+                                      d_segn.as<int>(), d_trows.as<int>(), d_tused.as<int>(),
+                                      d_row0.as<int>(), set->tiles.as<OpTile>(),
+                                      set->rowmap.as<int2>());
   k_op_fill<<<dim3((xb + 127) / 128, nkmax, n), 128, 0, st>>>(
       xb, d_geom.as<OpGeomDev>(), d_bp.as<float>(), d_cnt.as<int>(), set->tiles.as<OpTile>(),
       d_seg.as<int2>(), set->coef.as<float>(), set->colvalid.as<int>());
-  c->launches++;
+  c->launches += 2;
   MF_CHECK_CUDA(cudaGetLastError());
   for (int i = 0; i < n; ++i) {
     ReprojOpView& v = set->ops[i];
@@ -1265,6 +1335,7 @@ __global__ void k_flag_tiles_group(const GroupSeriesDev* __restrict__ ser,
   const int half_x = xb / 2;
   const int p0 = half_x * blockIdx.x / kFlagParts, p1 = half_x * (blockIdx.x + 1) / kFlagParts;
   int bad = 0;
+#pragma unroll 4  // several rows' loads in flight per thread
   for (int y = ya + threadIdx.y; y < yz; y += blockDim.y) {
     const float2* row = reinterpret_cast<const float2*>(s + (size_t)y * xb);
     for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {

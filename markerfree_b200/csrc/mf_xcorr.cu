@@ -270,6 +270,11 @@ __device__ __forceinline__ float norm_mask_one(float v, float mean, float fr) {
   return fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
 }
 
+// Each thread takes a pixel pair in kNmRows consecutive rows and issues all their
+// loads before the arithmetic, so that enough bytes are in flight to stream the
+// images at memory speed.
+constexpr int kNmRows = 4;
+
 __global__ void k_norm_mask_group(const GroupSeriesDev* __restrict__ ser,
                                   const GroupStepDev* __restrict__ steps,
                                   const int* __restrict__ active) {
@@ -279,18 +284,32 @@ __global__ void k_norm_mask_group(const GroupSeriesDev* __restrict__ ser,
   const GroupStepDev T = steps[b];
   if (T.ip < 0) return;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;  // pixel pair
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int w = S.xb, pad = S.pad;
-  if (2 * q >= pad || y >= S.yb) return;
-  float2* d = reinterpret_cast<float2*>(S.cc + (size_t)(img & 1) * S.ppix + (size_t)y * pad) + q;
+  const int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * kNmRows;
+  const int w = S.xb, pad = S.pad, yb = S.yb;
+  if (2 * q >= pad || y0 >= yb) return;
+  const int nr = min(kNmRows, yb - y0);
+  float2* d = reinterpret_cast<float2*>(S.cc + (size_t)(img & 1) * S.ppix + (size_t)y0 * pad) + q;
+  const size_t dstep = pad / 2;  // float2 per output row
   if (2 * q >= w) {
-    *d = make_float2(0.0f, 0.0f);
+    for (int r = 0; r < nr; ++r) d[r * dstep] = make_float2(0.0f, 0.0f);
     return;
   }
-  const float2 v = reinterpret_cast<const float2*>(group_image(S, T, img) + (size_t)y * w)[q];
-  const float2 fr = __ldg(reinterpret_cast<const float2*>(S.mask + (size_t)y * w) + q);
+  const float2* src = reinterpret_cast<const float2*>(group_image(S, T, img) + (size_t)y0 * w) + q;
+  const float2* msk = reinterpret_cast<const float2*>(S.mask + (size_t)y0 * w) + q;
+  const size_t sstep = w / 2;
+  float2 v[kNmRows], fr[kNmRows];
+#pragma unroll
+  for (int r = 0; r < kNmRows; ++r)
+    if (r < nr) {
+      v[r] = src[r * sstep];
+      fr[r] = __ldg(msk + r * sstep);
+    }
   const float mean = S.stats[img & 1].x;
-  *d = make_float2(norm_mask_one(v.x, mean, fr.x), norm_mask_one(v.y, mean, fr.y));
+#pragma unroll
+  for (int r = 0; r < kNmRows; ++r)
+    if (r < nr)
+      d[r * dstep] = make_float2(norm_mask_one(v[r].x, mean, fr[r].x),
+                                 norm_mask_one(v[r].y, mean, fr[r].y));
 }
 
 int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
@@ -299,7 +318,8 @@ int norm_mask_pad_group(Context* c, const GroupSeriesDev* ser, const GroupStepDe
   (void)xb_max;
   k_moments_group<<<dim3(moment_parts(yb_max), 2 * nseries), 256, 0, st>>>(ser, steps, active);
   k_moments_final_group<<<2 * nseries, 256, 0, st>>>(ser, steps, active);
-  dim3 blk(128, 2), grd((pad_max / 2 + 127) / 128, (yb_max + 1) / 2, 2 * nseries);
+  dim3 blk(128, 2), grd((pad_max / 2 + 127) / 128, (yb_max + 2 * kNmRows - 1) / (2 * kNmRows),
+                        2 * nseries);
   k_norm_mask_group<<<grd, blk, 0, st>>>(ser, steps, active);
   c->launches += 3;
   MF_CHECK_CUDA(cudaGetLastError());
