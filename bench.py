@@ -657,6 +657,10 @@ def run_ours(args):
             "gpu_launches": int(launches), "passes_per_series": passes_main,
             "tc_tuning": ctx.tc_tuning(),
             "stage_ms_per_step": {k: round(v, 2) for k, v in stages.items()},
+            # inside pass_ms: the re-projection of every held-out-tilt step, and its
+            # measurement (normalise, FFTs, filter, peak) with the re-correction
+            "pass_ms_split": {"reproject_ms": round(st["reproj_ms"], 2),
+                              "measure_recorrect_ms": round(st["xcorr_ms"], 2)},
             "roofline": roof, "roofline_other": others, "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_uneven:
         log("uneven batch")

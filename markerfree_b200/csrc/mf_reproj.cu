@@ -659,6 +659,72 @@ __global__ void k_op_to_bf16(const float* __restrict__ src, size_t n, float scal
     dst[i] = __float2bfloat16_rn(src[i] * scale);
 }
 
+// Segment table of the tensor-core operators, on the device.  Entry (tilt i,
+// x-tile t, neighbour k), flattened in that order from the tilt's segidx_off:
+// the bins [min lo, max hi] of the tile's columns become a segment from b0 = lo
+// rounded down to a multiple of 8, of nch chunks of kTcK bins (none when the
+// neighbour touches nothing).
+__global__ void k_optc_tiles(int xb, int ntx, int n, const OpGeomDev* __restrict__ geoms,
+                             const int* __restrict__ lo, const int* __restrict__ hi,
+                             int* __restrict__ ent_b0, int* __restrict__ ent_nch,
+                             int* __restrict__ ent_seg) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n * ntx) return;
+  const int i = q / ntx, t = q % ntx;
+  const OpGeomDev g = geoms[i];
+  const int nk = g.nk;
+  const int x0 = t * kTcM, x1 = min(xb, x0 + kTcM);
+  const int* lo_t = lo + g.lohi_off;
+  const int* hi_t = hi + g.lohi_off;
+  for (int k = 0; k < nk; ++k) {
+    int l = INT_MAX, h = -1;
+    for (int x = x0; x < x1; ++x) {
+      l = min(l, lo_t[(size_t)x * nk + k]);
+      h = max(h, hi_t[(size_t)x * nk + k]);
+    }
+    const size_t e = (size_t)g.seg_off + (size_t)t * nk + k;
+    const int b0 = l & ~7;
+    ent_b0[e] = h < 0 ? 0 : b0;
+    ent_nch[e] = h < 0 ? 0 : (h - b0 + kTcK) / kTcK;
+    ent_seg[e] = h < 0 ? 0 : 1;
+  }
+}
+
+// From the entries and their exclusive prefix sums (segment index, first chunk):
+// segidx (-1 for an empty entry), the segments, and every x-tile's summary.
+__global__ void k_optc_layout(int ntx, const OpGeomDev* __restrict__ geoms,
+                              const int* __restrict__ ent_b0, const int* __restrict__ ent_nch,
+                              const int* __restrict__ ent_seg, const int* __restrict__ seg_pre,
+                              const int* __restrict__ chunk_pre, int* __restrict__ segidx,
+                              TcSeg* __restrict__ segs, TcXTile* __restrict__ xts) {
+  const int i = blockIdx.x;
+  const OpGeomDev g = geoms[i];
+  const int nk = g.nk, ne = ntx * nk;
+  for (int j = threadIdx.x; j < ne; j += blockDim.x) {
+    const size_t e = (size_t)g.seg_off + j;
+    if (ent_seg[e]) {
+      TcSeg sg;
+      sg.tilt = g.i0 + j % nk;
+      sg.b0 = ent_b0[e];
+      sg.nch = ent_nch[e];
+      sg.chunk0 = chunk_pre[e];
+      segs[seg_pre[e]] = sg;
+      segidx[e] = seg_pre[e];
+    } else {
+      segidx[e] = -1;
+    }
+  }
+  for (int t = threadIdx.x; t < ntx; t += blockDim.x) {
+    const size_t e0 = (size_t)g.seg_off + (size_t)t * nk, e1 = e0 + nk;
+    TcXTile X;
+    X.seg0 = seg_pre[e0];
+    X.nseg = seg_pre[e1] - seg_pre[e0];
+    X.nch = chunk_pre[e1] - chunk_pre[e0];
+    X.pad = 0;
+    xts[(size_t)i * ntx + t] = X;
+  }
+}
+
 int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int half_kind,
                         TcOpSet* set, cudaStream_t st) {
   const int n = (int)geoms.size();
@@ -672,10 +738,13 @@ int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int ha
   if (n == 0) return MF_OK;
   const int xb = geoms[0].xb, yb = geoms[0].yb;
   const int ntx = (xb + kTcM - 1) / kTcM;
-  // pass 1: per column valid-sample count and per neighbour bin range
+  // pass 1: per column valid-sample count and per neighbour bin range; then the
+  // segment table, laid out on the device (the host reads back only prefix sums)
   std::vector<OpGeomDev> gd(n);
   std::vector<float> bps;
   int lohi = 0;
+  std::vector<int> segidx_off(n);
+  size_t nent = 0;
   for (int i = 0; i < n; ++i) {
     const ReprojGeom& g = geoms[i];
     gd[i].nk = g.nk;
@@ -686,16 +755,24 @@ int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int ha
     gd[i].fsin = g.fsin;
     gd[i].lohi_off = lohi;
     gd[i].tile_off = 0;
-    gd[i].seg_off = 0;
+    gd[i].seg_off = (int)nent;
+    gd[i].i0 = g.i0;
+    segidx_off[i] = (int)nent;
     bps.insert(bps.end(), g.bp.begin(), g.bp.end());
     lohi += xb * g.nk;
+    nent += (size_t)ntx * g.nk;
   }
-  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi;
+  DevBuf d_geom, d_bp, d_cnt, d_lo, d_hi, d_b0, d_nch, d_has, d_segpre, d_chpre;
   MF_TRY(d_geom.alloc(sizeof(OpGeomDev) * n));
   MF_TRY(d_bp.alloc(sizeof(float) * bps.size()));
   MF_TRY(d_cnt.alloc(sizeof(int) * (size_t)n * xb));
   MF_TRY(d_lo.alloc(sizeof(int) * (size_t)lohi));
   MF_TRY(d_hi.alloc(sizeof(int) * (size_t)lohi));
+  MF_TRY(d_b0.alloc(sizeof(int) * std::max<size_t>(nent, 1)));
+  MF_TRY(d_nch.alloc(sizeof(int) * std::max<size_t>(nent, 1)));
+  MF_TRY(d_has.alloc(sizeof(int) * std::max<size_t>(nent, 1)));
+  MF_TRY(d_segpre.alloc(sizeof(int) * (nent + 1)));
+  MF_TRY(d_chpre.alloc(sizeof(int) * (nent + 1)));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_geom.p, gd.data(), sizeof(OpGeomDev) * n,
                                 cudaMemcpyHostToDevice, st));
   MF_CHECK_CUDA(cudaMemcpyAsync(d_bp.p, bps.data(), sizeof(float) * bps.size(),
@@ -703,83 +780,54 @@ int build_reproj_tc_ops(Context* c, const std::vector<ReprojGeom>& geoms, int ha
   k_op_scan<<<dim3((xb + 127) / 128, n), 128, 0, st>>>(xb, d_geom.as<OpGeomDev>(),
                                                        d_bp.as<float>(), d_cnt.as<int>(),
                                                        d_lo.as<int>(), d_hi.as<int>());
-  c->launches++;
+  k_optc_tiles<<<(n * ntx + 127) / 128, 128, 0, st>>>(
+      xb, ntx, n, d_geom.as<OpGeomDev>(), d_lo.as<int>(), d_hi.as<int>(), d_b0.as<int>(),
+      d_nch.as<int>(), d_has.as<int>());
+  k_scan_rows<<<1, 1024, 0, st>>>((int)nent, d_has.as<int>(), d_segpre.as<int>());
+  k_scan_rows<<<1, 1024, 0, st>>>((int)nent, d_nch.as<int>(), d_chpre.as<int>());
+  c->launches += 4;
   MF_CHECK_CUDA(cudaGetLastError());
-  std::vector<int> lo(lohi), hi(lohi);
-  MF_CHECK_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, sizeof(int) * lohi, cudaMemcpyDeviceToHost, st));
+  std::vector<int> chpre(nent + 1), segpre_end(1);
+  MF_CHECK_CUDA(cudaMemcpyAsync(chpre.data(), d_chpre.p, sizeof(int) * (nent + 1),
+                                cudaMemcpyDeviceToHost, st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(segpre_end.data(), d_segpre.as<int>() + nent, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
   MF_CHECK_CUDA(cudaStreamSynchronize(st));
-  // segments: per tilt, per x-tile, per neighbour with a non-empty band
-  std::vector<TcSeg> segs;
-  std::vector<TcXTile> xts((size_t)n * ntx);
-  std::vector<int> segidx;  // [tilt][x-tile][neighbour]
-  std::vector<int> segidx_off(n), chunk_first(n + 1);
-  int chunks = 0;
+  std::vector<int> chunk_first(n + 1);
+  for (int i = 0; i < n; ++i) chunk_first[i] = chpre[segidx_off[i]];
+  chunk_first[n] = chpre[nent];
+  const int chunks = chunk_first[n];
   for (int i = 0; i < n; ++i) {
     const ReprojGeom& g = geoms[i];
-    const int nk = g.nk;
-    segidx_off[i] = (int)segidx.size();
-    segidx.resize(segidx.size() + (size_t)ntx * nk, -1);
-    chunk_first[i] = chunks;
-    const int* lo_t = lo.data() + gd[i].lohi_off;
-    const int* hi_t = hi.data() + gd[i].lohi_off;
-    for (int t = 0; t < ntx; ++t) {
-      const int x0 = t * kTcM, x1 = std::min(xb, x0 + kTcM);
-      TcXTile& X = xts[(size_t)i * ntx + t];
-      X.seg0 = (int)segs.size();
-      X.nseg = 0;
-      X.nch = 0;
-      X.pad = 0;
-      for (int k = 0; k < nk; ++k) {
-        int l = INT_MAX, h = -1;
-        for (int x = x0; x < x1; ++x) {
-          l = std::min(l, lo_t[(size_t)x * nk + k]);
-          h = std::max(h, hi_t[(size_t)x * nk + k]);
-        }
-        if (h < 0) continue;
-        TcSeg sg;
-        sg.tilt = g.i0 + k;
-        sg.b0 = l & ~7;
-        sg.nch = (h - sg.b0 + kTcK) / kTcK;
-        sg.chunk0 = chunks;
-        chunks += sg.nch;
-        segidx[segidx_off[i] + t * nk + k] = (int)segs.size();
-        segs.push_back(sg);
-        X.nseg++;
-        X.nch += sg.nch;
-      }
-    }
     TcOpView v;
     v.ip = g.ip;
     v.i0 = g.i0;
-    v.nk = nk;
+    v.nk = g.nk;
     v.xb = xb;
     v.yb = yb;
     v.ntx = ntx;
-    v.nchunks = chunks - chunk_first[i];
+    v.nchunks = chunk_first[i + 1] - chunk_first[i];
     set->ops.push_back(v);
     // compulsory traffic: 16-bit neighbour images, FP32 output, the operator itself
-    set->bytes += 2.0 * xb * yb * nk + 4.0 * xb * yb + (double)v.nchunks * kTcM * kTcK * 2;
+    set->bytes += 2.0 * xb * yb * g.nk + 4.0 * xb * yb + (double)v.nchunks * kTcM * kTcK * 2;
     set->fma += (double)v.nchunks * kTcM * kTcK * yb;
   }
-  chunk_first[n] = chunks;
   set->total_chunks = chunks;
-  set->nsegs = (int)segs.size();
-  set->nxt = (int)xts.size();
+  set->nsegs = segpre_end[0];
+  set->nxt = n * ntx;
   const size_t chunk_elems = (size_t)kTcM * kTcK;
   MF_TRY(set->op16.alloc(2 * chunk_elems * std::max(chunks, 1)));
-  MF_TRY(set->xt.alloc(sizeof(TcXTile) * xts.size()));
-  MF_TRY(set->segs.alloc(sizeof(TcSeg) * std::max<size_t>(segs.size(), 1)));
+  MF_TRY(set->xt.alloc(sizeof(TcXTile) * (size_t)n * ntx));
+  MF_TRY(set->segs.alloc(sizeof(TcSeg) * std::max(set->nsegs, 1)));
   MF_TRY(set->colvalid.alloc(sizeof(int) * (size_t)n * xb));
   DevBuf d_segidx;
-  MF_TRY(d_segidx.alloc(sizeof(int) * segidx.size()));
-  MF_CHECK_CUDA(cudaMemcpyAsync(set->xt.p, xts.data(), sizeof(TcXTile) * xts.size(),
-                                cudaMemcpyHostToDevice, st));
-  if (!segs.empty())
-    MF_CHECK_CUDA(cudaMemcpyAsync(set->segs.p, segs.data(), sizeof(TcSeg) * segs.size(),
-                                  cudaMemcpyHostToDevice, st));
-  MF_CHECK_CUDA(cudaMemcpyAsync(d_segidx.p, segidx.data(), sizeof(int) * segidx.size(),
-                                cudaMemcpyHostToDevice, st));
+  MF_TRY(d_segidx.alloc(sizeof(int) * std::max<size_t>(nent, 1)));
+  k_optc_layout<<<n, 256, 0, st>>>(ntx, d_geom.as<OpGeomDev>(), d_b0.as<int>(), d_nch.as<int>(),
+                                   d_has.as<int>(), d_segpre.as<int>(), d_chpre.as<int>(),
+                                   d_segidx.as<int>(), set->segs.as<TcSeg>(),
+                                   set->xt.as<TcXTile>());
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
   // pass 2 in groups of tilts whose FP32 staging fits in a bounded buffer
   const size_t stage_cap = (size_t)64 << 20;  // floats (256 MB)
   size_t max_one = 0;
