@@ -20,7 +20,9 @@ LIB = os.path.join(OUT, "libmfalign.so")
 CLI = os.path.join(OUT, "Markerfree")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+# deleting an object whose type the file cannot see skips its destructor: an error
+CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler",
+          "-fPIC,-fvisibility=hidden,-Werror=delete-incomplete",
           "-I" + os.path.join(ROOT, "include")] + ARCH
 if os.environ.get("MF_HOST_DEBUG"):  # host debug information (backtraces, addr2line)
     CFLAGS += ["-Xcompiler", "-g"]

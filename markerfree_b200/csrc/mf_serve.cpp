@@ -315,7 +315,7 @@ struct mf_server {
         rc = group_create(ctx, ss.data(), (int)ss.size(), o.zshift, align_z.data(), o.nproj, &g);
         if (rc == MF_ERR_NOMEM) {
           // set-up allocates everything before any series changes: nothing to undo
-          delete g;
+          mf_group_destroy(g);  // defined where mf_group is complete
           return_cached_memory(gpu, ctx->c.stream);
           lk.lock();
           size_t gb = 0;
@@ -338,7 +338,7 @@ struct mf_server {
           lk.unlock();
         } else if (rc == MF_OK) {
           rc = group_proj_align(g, passes.data());
-          delete g;
+          mf_group_destroy(g);  // defined where mf_group is complete
         }
       }
       std::vector<int> rcs(group.size(), rc);

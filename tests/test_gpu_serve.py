@@ -105,3 +105,30 @@ def test_served_requests_survive_a_full_device(ctx, mflib, first, count):
         assert np.abs(p.rotate - pa.rotate).max() <= AXIS_TOL, i
         assert np.abs(p.shift_x - pa.shift_x).max() <= SHIFT_TOL, i
         assert np.abs(p.shift_y - pa.shift_y).max() <= SHIFT_TOL, i
+
+
+def _pool_bytes_in_use():
+    """Bytes of the device's stream-ordered pool (the library's allocations) in use."""
+    import torch
+    rt = pytest.importorskip("cuda.bindings.runtime")
+    torch.cuda.synchronize()
+    _, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    _, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    return int(used)
+
+
+@pytest.mark.parametrize("prec", [2, 0])
+def test_server_returns_all_device_memory(mflib, prec):
+    """Every request's series and every group's buffers go back to the pool: after
+    the server closes, the pool holds no more than before it started."""
+    reqs = requests()
+    before = _pool_bytes_in_use()
+    srv = mflib.Server(gpu=0, hbm_budget=0, max_group=4, workers=2, group_wait_ms=20.0)
+    try:
+        ids = [srv.submit(s.stack, s.angles, offset=1e-4, align_z=s.thickness, nproj=10,
+                          precision=prec) for s in reqs]
+        for j in ids:
+            srv.wait(j)
+    finally:
+        srv.close()
+    assert _pool_bytes_in_use() <= before
