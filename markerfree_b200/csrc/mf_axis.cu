@@ -198,6 +198,12 @@ __device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsi
 // Two consecutive samples are stepped together: each packed f32x2 operation
 // evaluates one coordinate of samples x and x + 1 (lane for lane the scalar IEEE
 // operation), and the samples are added to the sum in order, x first.
+#ifndef MF_RADON_UNROLL
+#define MF_RADON_UNROLL 2
+#endif
+#define MF_RADON_PRAGMA_(x) _Pragma(#x)
+#define MF_RADON_PRAGMA(x) MF_RADON_PRAGMA_(x)
+#define MF_RADON_UNROLL_PRAGMA MF_RADON_PRAGMA(unroll MF_RADON_UNROLL)
 template <bool kByColumn, bool kNonNeg, bool kFold>
 __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, int stride,
                                               const RadonLine& ln, int lo, int hi, float* sum_out,
@@ -220,7 +226,7 @@ __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, in
   float sum = 0.0f;
   int cnt = 0;
   int x = lo;
-#pragma unroll 2
+  MF_RADON_UNROLL_PRAGMA
   for (; x + 1 < hi; x += 2) {
     // X = fma(x, cos, -(y sin)) + ox, Y = fma(x, sin, y cos) + oy, as lin2(), for x, x + 1
     const unsigned long long tx = add2_rz(add2_rn(fma2_rn(fx2, c2, ys2), ox2), big2);
