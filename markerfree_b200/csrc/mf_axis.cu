@@ -199,7 +199,7 @@ __device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsi
 // evaluates one coordinate of samples x and x + 1 (lane for lane the scalar IEEE
 // operation), and the samples are added to the sum in order, x first.
 #ifndef MF_RADON_UNROLL
-#define MF_RADON_UNROLL 2
+#define MF_RADON_UNROLL 4
 #endif
 #define MF_RADON_PRAGMA_(x) _Pragma(#x)
 #define MF_RADON_PRAGMA(x) MF_RADON_PRAGMA_(x)
@@ -606,26 +606,31 @@ __device__ __forceinline__ float stretch_nofill(const float* in, int x, int y, i
   return kSentinel;
 }
 
+// Each pair's image is split into kOffsetParts bands of rows, one block each; a
+// block accumulates its band in FP64 and the bands are added in order.
+constexpr int kOffsetParts = 16;
+
 __global__ void k_offset_moments(const float* __restrict__ corr, int w, int h,
-                                 const OffsetPair* __restrict__ pairs, double* __restrict__ out) {
+                                 const OffsetPair* __restrict__ pairs, double* __restrict__ part) {
   __shared__ double s[6][256];
   OffsetPair p = pairs[blockIdx.x];
   const float* ref = corr + (size_t)p.ref * w * h;
   const float* img = corr + (size_t)p.img * w * h;
+  const int y0 = h * (int)blockIdx.y / kOffsetParts, y1 = h * ((int)blockIdx.y + 1) / kOffsetParts;
   double a[6] = {0, 0, 0, 0, 0, 0};
-  for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
-    int y = i / w, x = i % w;
-    float v1 = ref[i];
-    if (v1 < -1e10f) continue;
-    float v2 = stretch_nofill(img, x, y, w, h, p.m0, p.m1, p.m2);
-    if (v2 < -1e10f) continue;
-    a[0] += v1;
-    a[1] += v2;
-    a[2] += (double)__fmul_rn(v1, v1);
-    a[3] += (double)__fmul_rn(v2, v2);
-    a[4] += (double)__fmul_rn(v1, v2);
-    a[5] += 1.0;
-  }
+  for (int y = y0; y < y1; ++y)
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
+      float v1 = ref[(size_t)y * w + x];
+      if (v1 < -1e10f) continue;
+      float v2 = stretch_nofill(img, x, y, w, h, p.m0, p.m1, p.m2);
+      if (v2 < -1e10f) continue;
+      a[0] += v1;
+      a[1] += v2;
+      a[2] += (double)__fmul_rn(v1, v1);
+      a[3] += (double)__fmul_rn(v2, v2);
+      a[4] += (double)__fmul_rn(v1, v2);
+      a[5] += 1.0;
+    }
   for (int k = 0; k < 6; ++k) s[k][threadIdx.x] = a[k];
   __syncthreads();
   for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
@@ -634,13 +639,30 @@ __global__ void k_offset_moments(const float* __restrict__ corr, int w, int h,
     __syncthreads();
   }
   if (threadIdx.x == 0)
-    for (int k = 0; k < 6; ++k) out[(size_t)blockIdx.x * 6 + k] = s[k][0];
+    for (int k = 0; k < 6; ++k)
+      part[((size_t)blockIdx.x * kOffsetParts + blockIdx.y) * 6 + k] = s[k][0];
+}
+
+__global__ void k_offset_moments_sum(const double* __restrict__ part, int npairs,
+                                     double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npairs * 6) return;
+  const int pr = i / 6, k = i % 6;
+  double acc = 0.0;
+  for (int b = 0; b < kOffsetParts; ++b) acc += part[((size_t)pr * kOffsetParts + b) * 6 + k];
+  out[i] = acc;
 }
 
 int offset_moments(Context* c, const float* corr, int w, int h, const OffsetPair* d_pairs,
                    int npairs, double* d_out, cudaStream_t st) {
-  k_offset_moments<<<npairs, 256, 0, st>>>(corr, w, h, d_pairs, d_out);
-  c->launches++;
+  if (npairs <= 0) return MF_OK;
+  DevBuf part;
+  MF_TRY(part.alloc(sizeof(double) * 6 * kOffsetParts * (size_t)npairs));
+  k_offset_moments<<<dim3(npairs, kOffsetParts), 256, 0, st>>>(corr, w, h, d_pairs,
+                                                                part.as<double>());
+  k_offset_moments_sum<<<(npairs * 6 + 255) / 256, 256, 0, st>>>(part.as<double>(), npairs,
+                                                                 d_out);
+  c->launches += 2;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;
 }

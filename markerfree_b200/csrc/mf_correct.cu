@@ -369,6 +369,10 @@ __global__ void k_min_final(const float* __restrict__ part, int nb, float* __res
 
 // One block per slice: FP64 sum and count of (v - min) over the central box; the
 // minimum is subtracted only when it is below zero (Preprocess.cu:103-160).
+// Each slice's central box is split into kBoxParts bands of rows, one block each;
+// FP64 partial sums, added in order by k_mass_scale.
+constexpr int kBoxParts = 32;
+
 __global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny,
                            const float* __restrict__ mm, double* __restrict__ sums,
                            int* __restrict__ counts) {
@@ -378,16 +382,19 @@ __global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny,
   const bool subtract = !(sub >= 0);
   const int z = blockIdx.x;
   const int x0 = nx * 1 / 6, y0 = ny * 1 / 6, w = nx * 4 / 6, h = ny * 4 / 6;
+  const int ya = h * (int)blockIdx.y / kBoxParts, yz = h * ((int)blockIdx.y + 1) / kBoxParts;
   const float* f = stack + (size_t)z * nx * ny;
   double acc = 0.0;
   int cnt = 0;
-  for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
-    int y = i / w, x = i % w;
-    float v = f[(size_t)(y + y0) * nx + x0 + x];
-    if (subtract && !(v < -1e10f)) v = __fsub_rn(v, sub);
-    if (v <= -1e20f) continue;
-    acc += v;
-    cnt++;
+  for (int y = ya; y < yz; ++y) {
+    const float* row = f + (size_t)(y + y0) * nx + x0;
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
+      float v = row[x];
+      if (subtract && !(v < -1e10f)) v = __fsub_rn(v, sub);
+      if (v <= -1e20f) continue;
+      acc += v;
+      cnt++;
+    }
   }
   s_sum[threadIdx.x] = acc;
   s_cnt[threadIdx.x] = cnt;
@@ -400,19 +407,29 @@ __global__ void k_box_mean(const float* __restrict__ stack, int nx, int ny,
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    sums[z] = s_sum[0];
-    counts[z] = s_cnt[0];
+    sums[(size_t)z * kBoxParts + blockIdx.y] = s_sum[0];
+    counts[(size_t)z * kBoxParts + blockIdx.y] = s_cnt[0];
   }
 }
 
 // MassNormalization's factors (Preprocess.cu:162-250): every slice is scaled to the
 // mean of the zero tilt (file order index `zero`), capped at 1000.
+__device__ __forceinline__ float box_mean_of(const double* sums, const int* counts, int z) {
+  double s = 0.0;
+  long long n = 0;
+  for (int b = 0; b < kBoxParts; ++b) {
+    s += sums[(size_t)z * kBoxParts + b];
+    n += counts[(size_t)z * kBoxParts + b];
+  }
+  return n == 0 ? 0.0f : (float)(s / (double)n);
+}
+
 __global__ void k_mass_scale(const double* __restrict__ sums, const int* __restrict__ counts,
                              int nz, int zero, float* __restrict__ scale) {
-  const float ref0 = counts[zero] == 0 ? 0.0f : (float)(sums[zero] / counts[zero]);
+  const float ref0 = box_mean_of(sums, counts, zero);
   const float ref = ref0 > 1000.0f ? 1000.0f : ref0;
   for (int i = threadIdx.x; i < nz; i += blockDim.x) {
-    const float mean = counts[i] == 0 ? 0.0f : (float)(sums[i] / counts[i]);
+    const float mean = box_mean_of(sums, counts, i);
     scale[i] = __fdiv_rn(ref, __fadd_rn(mean, 0.00001f));
   }
 }
@@ -441,14 +458,14 @@ int preprocess_device(Context* c, float* d_stack, int nx, int ny, int nz,
   const int nb = 1024;
   DevBuf part, sums, counts, scale, mm;
   MF_TRY(part.alloc(sizeof(float) * nb));
-  MF_TRY(sums.alloc(sizeof(double) * nz));
-  MF_TRY(counts.alloc(sizeof(int) * nz));
+  MF_TRY(sums.alloc(sizeof(double) * nz * kBoxParts));
+  MF_TRY(counts.alloc(sizeof(int) * nz * kBoxParts));
   MF_TRY(scale.alloc(sizeof(float) * nz));
   MF_TRY(mm.alloc(sizeof(float)));
   k_block_min<<<nb, 256, 0, st>>>(d_stack, n, part.as<float>());
   k_min_final<<<1, 256, 0, st>>>(part.as<float>(), nb, mm.as<float>());
-  k_box_mean<<<nz, 256, 0, st>>>(d_stack, nx, ny, mm.as<float>(), sums.as<double>(),
-                                  counts.as<int>());
+  k_box_mean<<<dim3(nz, kBoxParts), 256, 0, st>>>(d_stack, nx, ny, mm.as<float>(),
+                                                    sums.as<double>(), counts.as<int>());
   // the zero tilt is looked up in the file-order angles (Preprocess.cu:168)
   const int zero = frame_idx_from_tilt(nz, file_angles, 0.0f);
   k_mass_scale<<<1, 256, 0, st>>>(sums.as<double>(), counts.as<int>(), nz, zero,
