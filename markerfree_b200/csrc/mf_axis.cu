@@ -204,22 +204,38 @@ __device__ __forceinline__ unsigned long long add2_rz(unsigned long long a, unsi
 #define MF_RADON_PRAGMA_(x) _Pragma(#x)
 #define MF_RADON_PRAGMA(x) MF_RADON_PRAGMA_(x)
 #define MF_RADON_UNROLL_PRAGMA MF_RADON_PRAGMA(unroll MF_RADON_UNROLL)
-template <bool kByColumn, bool kNonNeg, bool kFold>
+// kSh > 0 (stride = 2^kSh): the byte offset is formed by shifts alone,
+// (slow bits << (kSh + 2)) + (fast bits << 2) in 32-bit arithmetic: the slow
+// coordinate's bias vanishes (2^23 << (kSh + 2) is a multiple of 2^32), the fast
+// one's leaves 4 * 2^23 mod 2^32 = 0x2C000000, which moves into the base address.
+// Shifts and adds run on the integer pipe, the multiply-add of the index on the
+// FP32 pipe that the coordinates already fill.  (No wrap: 4 * index + 0x2C000000
+// stays below 2^32 for images below 8.8e8 pixels.)
+#ifndef MF_RADON_SHIFT
+#define MF_RADON_SHIFT 1
+#endif
+template <bool kByColumn, bool kNonNeg, bool kFold, int kSh = 0>
 __device__ __forceinline__ void radon_samples(const float* __restrict__ proj, int stride,
                                               const RadonLine& ln, int lo, int hi, float* sum_out,
                                               int* cnt_out) {
   constexpr unsigned kBias = 0x4B000000u;  // bits of 2^23
   const unsigned bias_idx = kFold ? 0u : kBias * (unsigned)stride + kBias;  // mod 2^32
-  const uintptr_t base = (uintptr_t)proj - (kFold ? 4ull * kBias : 0ull);
+  const uintptr_t base = kSh > 0 ? (uintptr_t)proj - 0x2C000000ull
+                                 : (uintptr_t)proj - (kFold ? 4ull * kBias : 0ull);
   const unsigned long long c2 = pack2(ln.c, ln.c), s2 = pack2(ln.s, ln.s);
   const unsigned long long ys2 = pack2(ln.ys, ln.ys), yc2 = pack2(ln.yc, ln.yc);
   const unsigned long long ox2 = pack2(ln.ox, ln.ox), oy2 = pack2(ln.oy, ln.oy);
   const unsigned long long big2 = pack2(8388608.0f, 8388608.0f), two2 = pack2(2.0f, 2.0f);
   auto index = [&](float tx, float ty) -> unsigned {
     const unsigned bx = __float_as_uint(tx), by = __float_as_uint(ty);
+    if (kSh > 0) {  // byte offset (see above)
+      const unsigned slow = kByColumn ? bx : by, fast = kByColumn ? by : bx;
+      return (slow << (kSh + 2)) + (fast << 2);
+    }
     return (kByColumn ? bx * (unsigned)stride + by : by * (unsigned)stride + bx) - bias_idx;
   };
   auto load = [&](unsigned idx) -> float {
+    if (kSh > 0) return __ldg(reinterpret_cast<const float*>(base + (uintptr_t)idx));
     return __ldg(reinterpret_cast<const float*>(base + ((uintptr_t)idx << 2)));
   };
   unsigned long long fx2 = pack2((float)lo, (float)(lo + 1));
@@ -268,7 +284,13 @@ template <bool kByColumn, bool kNonNeg>
 __device__ __forceinline__ void radon_line(const float* __restrict__ proj, int stride,
                                            const RadonLine& ln, int lo, int hi, float* sum,
                                            int* cnt) {
-  if ((stride & 255) == 0)
+  if (MF_RADON_SHIFT && stride == 2048)
+    radon_samples<kByColumn, kNonNeg, true, 11>(proj, stride, ln, lo, hi, sum, cnt);
+  else if (MF_RADON_SHIFT && stride == 1024)
+    radon_samples<kByColumn, kNonNeg, true, 10>(proj, stride, ln, lo, hi, sum, cnt);
+  else if (MF_RADON_SHIFT && stride == 4096)
+    radon_samples<kByColumn, kNonNeg, true, 12>(proj, stride, ln, lo, hi, sum, cnt);
+  else if ((stride & 255) == 0)
     radon_samples<kByColumn, kNonNeg, true>(proj, stride, ln, lo, hi, sum, cnt);
   else
     radon_samples<kByColumn, kNonNeg, false>(proj, stride, ln, lo, hi, sum, cnt);
