@@ -157,7 +157,21 @@ __global__ void k_correct_group(GroupCorrArgs g) {
   const float* img = (L.xs == 1 ? S.stack : S.stack_t) + (size_t)z * nx * ny;
   float* out = g.steps ? S.recorr : S.scratch + (size_t)z * S.ppix;
   // rows in a grid-stride loop: the set-up above is paid once per block
-  for (int by = blockIdx.y * blockDim.y + threadIdx.y; by < S.yb; by += gridDim.y * blockDim.y) {
+  const int step = gridDim.y * blockDim.y;
+  int by0 = blockIdx.y * blockDim.y + threadIdx.y;
+  if (S.bin == 1) {
+    // four rows' gathers in flight before their stores
+    for (; by0 + 3 * step < S.yb; by0 += 4 * step) {
+      float r[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        r[q] = corr_pixel(img, L, nx, ny, bx, by0 + q * step, S.out_x, s_sx, s_sy, s_cs, s_sn,
+                          g.random_fill);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) out[(size_t)(by0 + q * step) * S.pad + bx] = r[q];
+    }
+  }
+  for (int by = by0; by < S.yb; by += step) {
     float res;
     if (S.bin == 1) {
       res = corr_pixel(img, L, nx, ny, bx, by, S.out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);

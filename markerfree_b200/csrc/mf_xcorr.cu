@@ -657,14 +657,22 @@ __global__ void __launch_bounds__(256) k_peak_partial_group(
   const int r1 = sy + (int)((long long)rows * (blockIdx.x + 1) / gridDim.x);
   float bv = -INFINITY;
   int bi = INT_MAX;
+  // pixel pairs (the pitch is even, so rows start on 8-byte boundaries); the
+  // winner is the largest value, ties to the lowest index, whatever the order
+  const int p0 = sx >> 1, p1 = (ex + 1) >> 1;
   for (int y = r0; y < r1; ++y) {
+    const float2* row = reinterpret_cast<const float2*>(m + (size_t)y * stride);
 #pragma unroll 4
-    for (int x = sx + threadIdx.x; x < ex; x += blockDim.x) {
-      int li = y * stride + x;
-      float v = __ldg(m + li);
-      if (better(v, li, bv, bi)) {
-        bv = v;
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+      const float2 v = __ldg(row + p);
+      const int x = 2 * p, li = y * stride + x;
+      if (x >= sx && better(v.x, li, bv, bi)) {
+        bv = v.x;
         bi = li;
+      }
+      if (x + 1 < ex && better(v.y, li + 1, bv, bi)) {
+        bv = v.y;
+        bi = li + 1;
       }
     }
   }
