@@ -314,9 +314,6 @@ __device__ __forceinline__ void radon_line(const float* __restrict__ proj, int s
 #ifndef MF_RADON_CAND
 #define MF_RADON_CAND 4
 #endif
-#ifndef MF_RADON_LINES_PER_BLOCK
-#define MF_RADON_LINES_PER_BLOCK 0
-#endif
 constexpr int kRadonCand = MF_RADON_CAND;  // candidates (warps) per block
 
 __global__ void __launch_bounds__(32 * kRadonCand)
@@ -326,14 +323,8 @@ __global__ void __launch_bounds__(32 * kRadonCand)
             const float* __restrict__ sxs, const float* __restrict__ sys,
             const int* __restrict__ region, float* __restrict__ lines,
             unsigned long long* __restrict__ samples) {
-#if MF_RADON_LINES_PER_BLOCK
-  // one candidate per block, 32 * kRadonCand consecutive lines
-  const int y = blockIdx.y * (32 * kRadonCand) + threadIdx.x;
-  const int b = blockIdx.x;
-#else
   const int y = blockIdx.y * 32 + (threadIdx.x & 31);
   const int b = blockIdx.x * kRadonCand + (threadIdx.x >> 5);
-#endif
   const int z = blockIdx.z;
   if (y >= L || b >= num) return;
   RadonLine ln;
@@ -570,11 +561,7 @@ int tilt_axis_scores_enqueue(Context* c, cufftHandle plan, const float* stack,
     MF_CHECK_CUDA(cudaEventCreate(&J->ev[1]));
     MF_CHECK_CUDA(cudaEventRecord(J->ev[0], st));
   }
-#if MF_RADON_LINES_PER_BLOCK
-  const dim3 rgrid(num, (L + 32 * kRadonCand - 1) / (32 * kRadonCand), nz);
-#else
   const dim3 rgrid((num + kRadonCand - 1) / kRadonCand, (L + 31) / 32, nz);
-#endif
   k_radon<<<rgrid, 32 * kRadonCand, 0, st>>>(
       stack, stack_t, d_neg, nx, ny, L, num, cs.as<float2>(), tcos.as<float>(),
       d_sx.as<float>(), d_sy.as<float>(), region.as<int>(), lines.as<float>(),
