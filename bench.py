@@ -612,6 +612,13 @@ def run_ours(args):
                            "traffic_reproject.json")
     roof_rep["note"] = ("FP32 FMA-bound on the banded operator; the HBM fraction counts "
                         "compulsory bytes (neighbour rows, operator, output)") if prec == 0 else ""
+    if prec == 0:
+        # the bound that applies: the SIMT FP32 pipe (nominal: 148 SMs x 128 lanes x
+        # 2 flops at the sampled SM clock)
+        mhz = clk.summary().get("sm_mhz") or 1965.0
+        fp32_peak = 148 * 128 * 2 * float(mhz) * 1e6 / 1e12
+        roof_rep["fp32_peak_tflops"] = fp32_peak
+        roof_rep["fp32_frac"] = roof_rep["tflops"] / fp32_peak
     # the tilt-axis Radon kernel, timed on its own in the profiled step: compulsory
     # bytes (each tilt image once, the lines once) over its time, and its gather rate
     n_rad = max(stages["radon_launches"], 1.0)
@@ -628,8 +635,10 @@ def run_ours(args):
                 "samples_per_s": stages["radon_samples"] / max(stages["radon_ms"] / 1e3, 1e-12),
                 "share_of_step": stages["radon_ms"] / max(p_ms, 1e-9),
                 "profiled_ms_per_step": p_ms,
-                "note": "gather-bound: the tilt images are L2-resident while a launch "
-                        "samples them; the HBM fraction counts compulsory bytes only"}
+                "note": "instruction-issue-bound (every sample: six FP32 coordinate ops, "
+                        "the integer byte offset, the gather, the in-order line add); the "
+                        "tilt images are L2/L1-resident while a launch samples them, so the "
+                        "HBM fraction counts compulsory bytes only"}
     # the dominant kernel of the step carries the roofline; the others are kept beside it
     if roof_rad["share_of_step"] >= roof_rep["share_of_step"]:
         roof, others = roof_rad, [roof_rep]
