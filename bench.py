@@ -7,14 +7,16 @@ correlation + tilt-axis search, tilt-angle offset search), the full projection-
 matching schedule, and the aligned output stack.  Seeded synthetic data stands in
 for the reference's simulated phantoms.
 
-  value   series/min of the batched mixed-precision form: one step aligns --batch
-          series (default 8) with FP16 re-projection operands, projection matching
-          in one lockstep group (mf_align_many_device), raw stacks already in HBM and
-          aligned stacks written to HBM; summed over ranks (independent series)
+  value   series/min of the batched form: one step aligns --batch distinct series
+          (default 8) in FP32 (--precision, the reference's arithmetic), projection
+          matching in one lockstep group (mf_align_many_device), raw stacks already
+          in HBM and aligned stacks written to HBM; summed over ranks (independent
+          series).  FP16/BF16 operand forms are reported beside it.
   e2e     the same through the C ABI with host buffers: uploads of the raw stacks
           from pinned memory and downloads of the aligned stacks inside the timed
-          region
-  plain   one series at a time with FP32 operands (the reference's arithmetic)
+          region, overlapped with the neighbouring steps' alignment on a second
+          stream (the serial form is reported beside it)
+  plain   one series at a time in FP32 (mf_align_device)
   served  the serving loop (mf_server_*) on a Poisson stream of mixed-size requests
           at 80% of the measured batched capacity: series/min and p50/p99 latency
 
@@ -514,33 +516,80 @@ def run_ours(args):
     passes_main = last["passes"]
     log("batched timing done")
     # e2e through the C ABI with host buffers: per step B uploads from pinned memory,
-    # the group alignment, B downloads of the aligned stacks
+    # the group alignment, B downloads of the aligned stacks.  Two forms:
+    #  * serial: upload, align, download one after another on the library's stream;
+    #  * pipelined (the reported e2e): a second stream uploads step i+1's stacks and
+    #    downloads step i-1's aligned stacks while step i aligns (inputs and outputs
+    #    double-buffered, events order the three); the timed region starts before
+    #    the first upload and ends after the last download.
     # (built without loop variables: a pinned buffer still referenced when the
     # context's stream is gone would record its release on a destroyed stream)
     h_raws = [torch.empty(d.shape, dtype=torch.float32).pin_memory() for d in d_raws]
     for i in range(B):
         h_raws[i].copy_(d_raws[i])
     h_out = torch.empty((nz, yo, xo), dtype=torch.float32).pin_memory()
-    d_ins = [torch.empty_like(d_raws[0]) for _ in range(B)]
+    d_ins = [[torch.empty_like(d_raws[0]) for _ in range(B)] for _ in range(2)]
+    d_outs2 = [d_outs, [torch.empty_like(d_outs[0]) for _ in range(B)]]
+    copy_stream = torch.cuda.Stream(device=f"cuda:{dev}")
 
     def step_e2e():
         with torch.cuda.stream(stream):
-            for d, h in zip(d_ins, h_raws):
+            for d, h in zip(d_ins[0], h_raws):
                 d.copy_(h, non_blocking=True)
-        mf.align_many_device(ctx, d_ins, nx, ny, nz, angs, d_outs, **kw)
+        mf.align_many_device(ctx, d_ins[0], nx, ny, nz, angs, d_outs, **kw)
         with torch.cuda.stream(stream):
             for d in d_outs:
                 h_out.copy_(d, non_blocking=True)
 
+    def run_pipelined(steps):
+        up = [torch.cuda.Event(), torch.cuda.Event()]
+        done = [torch.cuda.Event(), torch.cuda.Event()]
+        down = [torch.cuda.Event(), torch.cuda.Event()]
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        copy_stream.wait_event(t0)
+
+        def upload(j):
+            with torch.cuda.stream(copy_stream):
+                for d, h in zip(d_ins[j % 2], h_raws):
+                    d.copy_(h, non_blocking=True)
+            up[j % 2].record(copy_stream)
+
+        upload(0)
+        for i in range(steps):
+            k = i % 2
+            if i + 1 < steps:
+                if i >= 1:
+                    copy_stream.wait_event(done[(i + 1) % 2])  # step i-1 read those inputs
+                upload(i + 1)
+            stream.wait_event(up[k])
+            if i >= 2:
+                stream.wait_event(down[k])  # step i-2's outputs have left the device
+            mf.align_many_device(ctx, d_ins[k], nx, ny, nz, angs, d_outs2[k], **kw)
+            done[k].record(stream)
+            copy_stream.wait_event(done[k])
+            with torch.cuda.stream(copy_stream):
+                for d in d_outs2[k]:
+                    h_out.copy_(d, non_blocking=True)
+            down[k].record(copy_stream)
+        stream.wait_event(down[(steps - 1) % 2])
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1)
+
     step_e2e()
     barrier()
-    e_ms = _time_steps(stream, step_e2e, args.steps)
+    es_ms = _time_steps(stream, step_e2e, args.steps)
+    run_pipelined(2)
+    barrier()
+    e_ms = run_pipelined(args.steps)
     log("e2e timing done")
     h2d_bytes = int(sum(h.numel() for h in h_raws) * 4)
     d2h_bytes = int(h_out.numel() * 4 + 3 * nz * 4) * B
     # the pinned buffers recorded their copies on the library's stream: release them
     # while that stream exists
-    del d_ins, h_raws, h_out, step_e2e
+    del d_ins, d_outs2, h_raws, h_out, step_e2e, run_pipelined
     torch.cuda.synchronize()
     k_extra = max(1, min(args.steps, 3))
     # the 16-bit operand forms of the same step, with their distance from the FP32 result
@@ -584,10 +633,11 @@ def run_ours(args):
     barrier()
     pl_ms = _time_steps(stream, step_plain, k_extra)
     log("plain timing done")
-    ms, e_ms, pl_ms = max_over_ranks([ms, e_ms, pl_ms], f"cuda:{dev}", pg)
+    ms, e_ms, es_ms, pl_ms = max_over_ranks([ms, e_ms, es_ms, pl_ms], f"cuda:{dev}", pg)
     ms_step = ms / args.steps
     value = 60000.0 * B / ms_step * world
     e2e_value = 60000.0 * B / (e_ms / args.steps) * world
+    e2e_serial = 60000.0 * B / (es_ms / args.steps) * world
     plain_value = 60000.0 * B / (pl_ms / k_extra) * world
     pk, src = peaks()
 
@@ -658,7 +708,11 @@ def run_ours(args):
             "data": "synthetic (seeded phantom series, BASELINE shapes)",
             "config": cfg,
             "e2e": {"value": e2e_value, "unit": "series/min",
-                    "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
+                    "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+                    "form": "pipelined: a second stream uploads the next step's stacks and "
+                            "downloads the previous step's aligned stacks while a step "
+                            "aligns (double-buffered); first upload to last download timed",
+                    "serial_value": e2e_serial},
             "plain": {"value": plain_value, "unit": "series/min", "steps": k_extra,
                       "what": "the same series one at a time, FP32 (mf_align_device)"},
             "batched_over_plain": value / plain_value,

@@ -49,46 +49,6 @@ __global__ void k_axis_cs(const float* __restrict__ rot, int num, float2* __rest
   cs[b] = make_float2(cosf(a), sinf(a));
 }
 
-// GCalcCommonRegion (Rotate.cu:9-40); entries whose first step already leaves
-// the image stay 0 here (the reference leaves them unset).
-__global__ void k_common_region(int width, int height, int L, const float2* __restrict__ cs,
-                                float shift_x, float shift_y, int* __restrict__ region) {
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (y >= L) return;
-  int i = blockIdx.x * L + y;
-  float fsin = cs[blockIdx.x].y, fcos = cs[blockIdx.x].x;
-  int half = L / 2;
-  float ox = __fmaf_rn((float)width, 0.5f, shift_x);
-  float oy = __fmaf_rn((float)height, 0.5f, shift_y);
-  float fy = __fmaf_rn(-(float)L, 0.5f, (float)y);
-  const float ys = -__fmul_rn(fy, fsin), yc = __fmul_rn(fy, fcos);
-  int left = 0, right = 0;
-  for (int x = 1; x < half; ++x) {
-    float X = lin2((float)(-x), fcos, ys, ox);
-    float Y = lin2((float)(-x), fsin, yc, oy);
-    if (X < 0 || X >= width) break;
-    if (Y < 0 || Y >= height) break;
-    left = -x;
-  }
-  for (int x = 1; x < half; ++x) {
-    float X = lin2((float)x, fcos, ys, ox);
-    float Y = lin2((float)x, fsin, yc, oy);
-    if (X < 0 || X >= width) break;
-    if (Y < 0 || Y >= height) break;
-    right = x;
-  }
-  region[2 * i] = left;
-  region[2 * i + 1] = right;
-}
-
-// Sample coordinates of GRadon (Rotate.cu:62-63, 76-77): X = x cos - y sin + ox,
-// Y = x sin + y cos + oy, contracted as the reference's device code is.
-struct RadonLine {
-  float c, s, ys, yc, ox, oy;  // ys = -(y sin), yc = y cos
-  __device__ __forceinline__ float X(float fx) const { return lin2(fx, c, ys, ox); }
-  __device__ __forceinline__ float Y(float fx) const { return lin2(fx, s, yc, oy); }
-};
-
 // Smallest x in [a, b) with pred(x), for a predicate that is false then true
 // along x; b when it is never true.
 template <class P>
@@ -102,6 +62,44 @@ __device__ __forceinline__ int first_true(int a, int b, P pred) {
   }
   return a;
 }
+
+// GCalcCommonRegion (Rotate.cu:9-40); entries whose first step already leaves
+// the image stay 0 here (the reference leaves them unset).
+__global__ void k_common_region(int width, int height, int L, const float2* __restrict__ cs,
+                                float shift_x, float shift_y, int* __restrict__ region) {
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (y >= L) return;
+  int i = blockIdx.x * L + y;
+  float fsin = cs[blockIdx.x].y, fcos = cs[blockIdx.x].x;
+  int half = L / 2;
+  float ox = __fmaf_rn((float)width, 0.5f, shift_x);
+  float oy = __fmaf_rn((float)height, 0.5f, shift_y);
+  float fy = __fmaf_rn(-(float)L, 0.5f, (float)y);
+  const float ys = -__fmul_rn(fy, fsin), yc = __fmul_rn(fy, fcos);
+  // The reference walks outwards from the centre and stops at the first sample
+  // outside the image.  The sample coordinates are monotone in x (every step is a
+  // correctly rounded monotone operation), so the samples inside the image form
+  // one interval of x and the first one outside on each side is found by
+  // bisection: the same ends as the walk.
+  const float fw = (float)width, fh = (float)height;
+  auto inside = [&](int x) {
+    const float X = lin2((float)x, fcos, ys, ox), Y = lin2((float)x, fsin, yc, oy);
+    return !(X < 0 || X >= fw) && !(Y < 0 || Y >= fh);
+  };
+  int left = 0, right = 0;
+  if (half > 1 && inside(-1)) left = -(first_true(2, half, [&](int x) { return !inside(-x); }) - 1);
+  if (half > 1 && inside(1)) right = first_true(2, half, [&](int x) { return !inside(x); }) - 1;
+  region[2 * i] = left;
+  region[2 * i + 1] = right;
+}
+
+// Sample coordinates of GRadon (Rotate.cu:62-63, 76-77): X = x cos - y sin + ox,
+// Y = x sin + y cos + oy, contracted as the reference's device code is.
+struct RadonLine {
+  float c, s, ys, yc, ox, oy;  // ys = -(y sin), yc = y cos
+  __device__ __forceinline__ float X(float fx) const { return lin2(fx, c, ys, ox); }
+  __device__ __forceinline__ float Y(float fx) const { return lin2(fx, s, yc, oy); }
+};
 
 // Sub-interval of [a, b) on which 0 <= f(x) < lim, for f = rounded (x k + consts):
 // f is monotone in x (non-decreasing for k >= 0, non-increasing for k < 0) because
