@@ -323,22 +323,28 @@ __global__ void k_rweight_group(const GroupSeriesDev* __restrict__ ser,
   float r = __fdiv_rn((float)x, fN);
   float cw = cosf(__fmul_rn(6.2831852f, r));
   r = __fmul_rn(__fmul_rn(2.0f, r), __fmaf_rn(0.45f, cw, 0.55f));
-  for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < rows;
-       row += gridDim.y * blockDim.y) {
-    size_t i = (size_t)row * cmp + x;
-    cufftComplex v = spec[i];
-    v.x = __fdiv_rn(v.x, fN);
-    v.y = __fdiv_rn(v.y, fN);
-    v.x = __fmul_rn(v.x, r);
-    v.y = __fmul_rn(v.y, r);
-    spec[i] = v;
+  // four rows' loads in flight before their stores (the spectrum is updated in place)
+  const int step = gridDim.y * blockDim.y;
+  for (int row = blockIdx.y * blockDim.y + threadIdx.y; row < rows; row += 4 * step) {
+    cufftComplex v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (row + q * step < rows) v[q] = spec[(size_t)(row + q * step) * cmp + x];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (row + q * step < rows) {
+        v[q].x = __fmul_rn(__fdiv_rn(v[q].x, fN), r);
+        v[q].y = __fmul_rn(__fdiv_rn(v[q].y, fN), r);
+        spec[(size_t)(row + q * step) * cmp + x] = v[q];
+      }
   }
 }
 
 int launch_rweight_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
                          const int* active, int nseries, int cmp_max, int rows_max,
                          cudaStream_t st) {
-  dim3 blk(128, 2), grd((cmp_max + 127) / 128, std::min((rows_max + 1) / 2, 16384), nseries);
+  // about eight rows per thread
+  dim3 blk(128, 2), grd((cmp_max + 127) / 128, std::min((rows_max + 15) / 16, 16384), nseries);
   k_rweight_group<<<grd, blk, 0, st>>>(ser, steps, active);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
