@@ -369,21 +369,10 @@ __global__ void k_xcorr_filter(const cufftComplex* __restrict__ ref, size_t ref_
 }
 
 // Group form: blockIdx.z = series; its pair's spectra in its cc buffer.
-__global__ void k_xcorr_filter_group(const GroupSeriesDev* __restrict__ ser,
-                                     const GroupStepDev* __restrict__ steps,
-                                     const int* __restrict__ active, float bfactor) {
-  const int b = blockIdx.z;
-  if (active && active[b] == 0) return;
-  const GroupSeriesDev& S = ser[b];
-  if (steps[b].ip < 0) return;
-  const int cmp = S.cmp, ny = S.yb;
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= cmp || y >= ny) return;
-  size_t i = (size_t)y * cmp + x;
-  const cufftComplex A = reinterpret_cast<const cufftComplex*>(S.cc)[i];
-  cufftComplex* Bp = reinterpret_cast<cufftComplex*>(S.cc + S.ppix) + i;
-  const cufftComplex B = *Bp;
+// Two rows per thread (y and y + ny/2 rounded up), both spectra pairs loaded
+// before the arithmetic.
+__device__ __forceinline__ cufftComplex xcorr_filter_one(cufftComplex A, cufftComplex B, int x,
+                                                         int y, int cmp, int ny, float bfactor) {
   float re = __fmaf_rn(A.x, B.x, __fmul_rn(A.y, B.y));
   float im = __fmaf_rn(A.x, B.y, -__fmul_rn(A.y, B.x));
   int yy = y;
@@ -400,13 +389,39 @@ __global__ void k_xcorr_filter_group(const GroupSeriesDev* __restrict__ ser,
     re = -re;
     im = -im;
   }
-  *Bp = make_cuComplex(re, im);
+  return make_cuComplex(re, im);
+}
+
+__global__ void k_xcorr_filter_group(const GroupSeriesDev* __restrict__ ser,
+                                     const GroupStepDev* __restrict__ steps,
+                                     const int* __restrict__ active, float bfactor) {
+  const int b = blockIdx.z;
+  if (active && active[b] == 0) return;
+  const GroupSeriesDev& S = ser[b];
+  if (steps[b].ip < 0) return;
+  const int cmp = S.cmp, ny = S.yb, half = (ny + 1) / 2;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cmp || y0 >= half) return;
+  const int y1 = y0 + half;
+  const bool two = y1 < ny;
+  const cufftComplex* Ap = reinterpret_cast<const cufftComplex*>(S.cc);
+  cufftComplex* Bp = reinterpret_cast<cufftComplex*>(S.cc + S.ppix);
+  const size_t i0 = (size_t)y0 * cmp + x, i1 = (size_t)y1 * cmp + x;
+  const cufftComplex A0 = Ap[i0], B0 = Bp[i0];
+  cufftComplex A1 = A0, B1 = B0;
+  if (two) {
+    A1 = Ap[i1];
+    B1 = Bp[i1];
+  }
+  Bp[i0] = xcorr_filter_one(A0, B0, x, y0, cmp, ny, bfactor);
+  if (two) Bp[i1] = xcorr_filter_one(A1, B1, x, y1, cmp, ny, bfactor);
 }
 
 int xcorr_filter_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
                        const int* active, int nseries, int cmp_max, int yb_max, float bfactor,
                        cudaStream_t st) {
-  dim3 blk(64, 4), grd((cmp_max + 63) / 64, (yb_max + 3) / 4, nseries);
+  dim3 blk(64, 4), grd((cmp_max + 63) / 64, ((yb_max + 1) / 2 + 3) / 4, nseries);
   k_xcorr_filter_group<<<grd, blk, 0, st>>>(ser, steps, active, bfactor);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
