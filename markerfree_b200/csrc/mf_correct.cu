@@ -112,16 +112,16 @@ __global__ void k_correct_bin(CorrArgs a) {
       res = corr_pixel(img, L, a.nx, a.ny, bx, by, a.out_x, s_sx, s_sy, s_cs, s_sn,
                        a.random_fill);
     } else {
+      // every sample of the bin is fetched (independent loads); a sentinel among
+      // them makes the result the sentinel, as the reference's early exit does
       float sum = 0.0f;
       bool bad = false;
-      for (int iy = 0; iy < a.biny && !bad; ++iy) {
+      for (int iy = 0; iy < a.biny; ++iy) {
+#pragma unroll 2
         for (int ix = 0; ix < a.binx; ++ix) {
           float v = corr_pixel(img, L, a.nx, a.ny, bx * a.binx + ix, by * a.biny + iy, a.out_x,
                                s_sx, s_sy, s_cs, s_sn, a.random_fill);
-          if (v < -1e10f) {
-            bad = true;
-            break;
-          }
+          bad |= v < -1e10f;
           sum = __fadd_rn(sum, v);
         }
       }
@@ -176,16 +176,16 @@ __global__ void k_correct_group(GroupCorrArgs g) {
     if (S.bin == 1) {
       res = corr_pixel(img, L, nx, ny, bx, by, S.out_x, s_sx, s_sy, s_cs, s_sn, g.random_fill);
     } else {
+      // every sample of the bin is fetched (independent loads); a sentinel among
+      // them makes the result the sentinel, as the reference's early exit does
       float sum = 0.0f;
       bool bad = false;
-      for (int iy = 0; iy < biny && !bad; ++iy) {
+      for (int iy = 0; iy < biny; ++iy) {
+#pragma unroll 2
         for (int ix = 0; ix < binx; ++ix) {
           float v = corr_pixel(img, L, nx, ny, bx * binx + ix, by * biny + iy, S.out_x, s_sx,
                                s_sy, s_cs, s_sn, g.random_fill);
-          if (v < -1e10f) {
-            bad = true;
-            break;
-          }
+          bad |= v < -1e10f;
           sum = __fadd_rn(sum, v);
         }
       }

@@ -151,6 +151,7 @@ int make_round_mask(Context* c, int w, int h, float cx, float cy, float msx, flo
 // Normalise with stats, apply GRoundEdge (from `mask` when given), zero the pad
 // columns; reads rows of `src_stride` floats (first w used) and writes rows of
 // `pad` floats.
+// Each thread takes one column of four consecutive rows, all loads issued first.
 __global__ void k_norm_mask(const float* __restrict__ src, const float* __restrict__ src1,
                             int src_stride, size_t src_img_stride, int w, int h, int pad,
                             size_t dst_img_stride, const float2* __restrict__ stats, float cx,
@@ -158,27 +159,39 @@ __global__ void k_norm_mask(const float* __restrict__ src, const float* __restri
                             const float* __restrict__ mask, float* __restrict__ dst,
                             ImgTable tab) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * 4;
   int img = blockIdx.z;
-  if (x >= pad || y >= h || table_skip(tab, img)) return;
-  float* d = dst + (size_t)img * dst_img_stride + (size_t)y * pad + x;
+  if (x >= pad || y0 >= h || table_skip(tab, img)) return;
+  const int nr = min(4, h - y0);
+  float* d = dst + (size_t)img * dst_img_stride + (size_t)y0 * pad + x;
   if (x >= w) {
-    *d = 0.0f;
+    for (int r = 0; r < nr; ++r) d[(size_t)r * pad] = 0.0f;
     return;
   }
-  float v = table_ptr(tab, src, src1, src_img_stride, img)[(size_t)y * src_stride + x];
-  float2 st = stats[img];
-  if (!(v < -1e10f)) {  // GNormalize; a division by 1 (PANorm) is exact and skipped
-    v = __fsub_rn(v, st.x);
-    if (st.y != 1.0f) v = __fdiv_rn(v, st.y);
+  const float* sp = table_ptr(tab, src, src1, src_img_stride, img) + (size_t)y0 * src_stride + x;
+  float v[4], fm[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (r < nr) {
+      v[r] = sp[(size_t)r * src_stride];
+      fm[r] = mask ? __ldg(mask + (size_t)(y0 + r) * w + x) : 0.0f;
+    }
+  const float2 st = stats[img];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (r >= nr) break;
+    float vv = v[r];
+    if (!(vv < -1e10f)) {  // GNormalize; a division by 1 (PANorm) is exact and skipped
+      vv = __fsub_rn(vv, st.x);
+      if (st.y != 1.0f) vv = __fdiv_rn(vv, st.y);
+    }
+    if (vv < -1e10f) {  // GRoundEdge
+      d[(size_t)r * pad] = 0.0f;
+      continue;
+    }
+    const float fr = mask ? fm[r] : round_edge(x, y0 + r, cx, cy, msx, msy, power);
+    d[(size_t)r * pad] = fr < 0.0f ? 0.0f : __fmul_rn(vv, fr);
   }
-  if (v < -1e10f) {  // GRoundEdge
-    *d = 0.0f;
-    return;
-  }
-  const float fr = mask ? __ldg(mask + (size_t)y * w + x)
-                        : round_edge(x, y, cx, cy, msx, msy, power);
-  *d = fr < 0.0f ? 0.0f : __fmul_rn(v, fr);
 }
 
 int moment_parts(int h) { return (h + kMomRows - 1) / kMomRows; }
@@ -193,7 +206,7 @@ int norm_mask_pad(Context* c, const float* src, const float* src1, int src_strid
   k_moments<<<dim3(nb, nimg), 256, 0, st>>>(src, src1, w, h, src_stride, src_img_stride, d_part,
                                             tab);
   k_moments_final<<<nimg, 256, 0, st>>>(d_part, nb, w, h, with_std, d_stats);
-  dim3 blk(64, 4), grd((pad + 63) / 64, (h + 3) / 4, nimg);
+  dim3 blk(64, 4), grd((pad + 63) / 64, (h + 15) / 16, nimg);
   k_norm_mask<<<grd, blk, 0, st>>>(src, src1, src_stride, src_img_stride, w, h, pad,
                                    dst_img_stride, d_stats, cx, cy, msx, msy, power, mask, dst,
                                    tab);
