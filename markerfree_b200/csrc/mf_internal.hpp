@@ -429,6 +429,10 @@ int launch_reproject_exact_group(Context* c, const GroupSeriesDev* ser, const Gr
 // FP32 groups: per-(tilt, 128-row tile, column part) sentinel flags of the
 // corrected stacks (the tflags layout of the 16-bit copies), for all tilts of
 // every series (steps == null) or each series' held-out tilt of a step
+// Per-(tilt, 128-row tile, column part) sentinel flags of one series' FP32
+// corrected stack (xb even): every tilt (d_tilts null) or the listed ones.
+int launch_flag_tiles(Context* c, const float* corr, int xb, int yb, const int* d_tilts,
+                      int ntilts, int* tflags, cudaStream_t st);
 int launch_flag_tiles_group(Context* c, const GroupSeriesDev* ser, const GroupStepDev* steps,
                             const int* active, int nseries, int nz_max, int ytiles_max,
                             cudaStream_t st);
@@ -440,6 +444,9 @@ struct ApplyJob {  // one series of a group at one step of the FP32 apply
   int* rowflags;
   int xb, yb, ntiles;  // ntiles 0: no held-out tilt at this step
 };
+// Sets the group apply's shared-memory attribute for the device (once; call it
+// outside stream capture).
+int prepare_apply_group(Context* c);
 int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
                                  const int* active, int njobs, int ntiles_max, int yb_max,
                                  cudaStream_t st);

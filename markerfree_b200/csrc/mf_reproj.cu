@@ -1346,9 +1346,9 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
-                                 const int* active, int njobs, int ntiles_max, int yb_max,
-                                 cudaStream_t st) {
+// The group apply's shared-memory size, set once per device outside any stream
+// capture (the set-up of a pass calls it before the pass is captured).
+int prepare_apply_group(Context* c) {
   static bool attr_set[64] = {};  // per device ordinal
   if (!attr_set[c->gpu & 63]) {
     MF_CHECK_CUDA(cudaFuncSetAttribute(k_op_apply_group,
@@ -1356,6 +1356,13 @@ int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const Apply
                                        kA2SmemBytes));
     attr_set[c->gpu & 63] = true;
   }
+  return MF_OK;
+}
+
+int launch_reproject_apply_group(Context* c, const ReprojOpSet& set, const ApplyJob* d_jobs,
+                                 const int* active, int njobs, int ntiles_max, int yb_max,
+                                 cudaStream_t st) {
+  MF_TRY(prepare_apply_group(c));
   dim3 grd(ntiles_max, (yb_max + kA2Y - 1) / kA2Y, njobs);
   k_op_apply_group<<<grd, 256, kA2SmemBytes, st>>>(set.coef.as<float>(), set.rowmap.as<int2>(),
                                                    d_jobs, active);
@@ -1402,6 +1409,40 @@ int launch_flag_tiles_group(Context* c, const GroupSeriesDev* ser, const GroupSt
   if (nseries <= 0) return MF_OK;
   dim3 blk(64, 8), grd(kFlagParts, ytiles_max, steps ? nseries : nseries * nz_max);
   k_flag_tiles_group<<<grd, blk, 0, st>>>(ser, steps, active, nz_max);
+  c->launches++;
+  MF_CHECK_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// The same flags for one series' corrected stack: every tilt (tilts == null) or
+// the tilts listed in tilts[0 .. ntilts).
+__global__ void k_flag_tiles(const float* __restrict__ corr, int xb, int yb, int ytiles,
+                             const int* __restrict__ tilts, int* __restrict__ tflags) {
+  const int tz = tilts ? tilts[blockIdx.z] : (int)blockIdx.z;
+  const float* s = corr + (size_t)tz * xb * yb;
+  const int ya = blockIdx.y * kApplyTileY, yz = min(yb, ya + kApplyTileY);
+  const int half_x = xb / 2;
+  const int p0 = half_x * blockIdx.x / kFlagParts, p1 = half_x * (blockIdx.x + 1) / kFlagParts;
+  int bad = 0;
+#pragma unroll 4  // several rows' loads in flight per thread
+  for (int y = ya + threadIdx.y; y < yz; y += blockDim.y) {
+    const float2* row = reinterpret_cast<const float2*>(s + (size_t)y * xb);
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+      const float2 v = row[p];
+      bad |= (v.x < -1e10f) | (v.y < -1e10f);
+    }
+  }
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    tflags[((size_t)tz * ytiles + blockIdx.y) * kFlagParts + blockIdx.x] = bad ? 1 : 0;
+}
+
+int launch_flag_tiles(Context* c, const float* corr, int xb, int yb, const int* d_tilts,
+                      int ntilts, int* tflags, cudaStream_t st) {
+  if (ntilts <= 0) return MF_OK;
+  const int ytiles = (yb + kApplyTileY - 1) / kApplyTileY;
+  dim3 blk(64, 8), grd(kFlagParts, ytiles, ntilts);
+  k_flag_tiles<<<grd, blk, 0, st>>>(corr, xb, yb, ytiles, d_tilts, tflags);
   c->launches++;
   MF_CHECK_CUDA(cudaGetLastError());
   return MF_OK;

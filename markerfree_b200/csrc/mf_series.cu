@@ -609,7 +609,6 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
   MF_TRY(P.d_z0.alloc(sizeof(float)));
   MF_TRY(P.d_maxerr.alloc(sizeof(float)));
   MF_TRY(P.d_meas.alloc(sizeof(float) * 2 * nz));
-  MF_TRY(P.d_rowflags.alloc(sizeof(int) * std::max(1, n * P.ytiles)));
   P.bp_off.assign(n, 0);
   std::vector<float> bp;
   for (int k = 0; k < n; ++k) {
@@ -645,6 +644,26 @@ int projalign_setup(mf_series* s, float zshift, int align_z, int nproj) {
     MF_TRY(build_reproj_ops(c, P.geom, &P.ops, st));
     P.reproj_bytes = P.ops.bytes;
     P.reproj_fma = P.ops.fma;
+    // the group apply with one job per held-out tilt; sentinel flags per tile of
+    // the corrected stack send the tiles that need it to the exact path
+    MF_TRY(P.tflags.alloc(sizeof(int) * (size_t)nz * P.ytiles * kFlagParts));
+    std::vector<ApplyJob> jobs(std::max(n, 1));
+    for (int k = 0; k < n; ++k) {
+      const ReprojOpView& v = P.ops.ops[k];
+      ApplyJob J{};
+      J.tiles = v.tiles;
+      J.colvalid = v.colvalid;
+      J.corr = P.corr.as<float>();
+      J.out = P.reproj.as<float>();
+      J.xb = xb;
+      J.yb = yb;
+      J.ntiles = v.ntiles;
+      jobs[k] = J;
+    }
+    MF_TRY(prepare_apply_group(c));
+    MF_TRY(P.d_applyjobs.alloc(sizeof(ApplyJob) * jobs.size()));
+    MF_CHECK_CUDA(cudaMemcpyAsync(P.d_applyjobs.p, jobs.data(), sizeof(ApplyJob) * jobs.size(),
+                                  cudaMemcpyHostToDevice, st));
   } else {
     // compulsory traffic: the K neighbour images read once, the re-projection written
     for (int k = 0; k < n; ++k) P.reproj_bytes += 4.0 * (double)bpix * (P.geom[k].nk + 1);
@@ -675,7 +694,6 @@ static int pa_enqueue(mf_series* s) {
   double2* mpart = P.part.as<double2>();
   float2* ppart = reinterpret_cast<float2*>(mpart + moment_parts(yb) * 2);
   float2* stats = P.stats.as<float2>();
-  MF_CHECK_CUDA(cudaMemsetAsync(P.d_rowflags.p, 0, sizeof(int) * std::max(1, n * P.ytiles), st));
   // CorrTomoStack::DoIt: resample + bin + R-weight every tilt (CorrStack.cu:353-397)
   MF_TRY(launch_correct_bin(c, s->stack.as<float>(), s->stack_t.as<float>(),
                             s->nx, s->ny, nullptr, nz,
@@ -685,9 +703,12 @@ static int pa_enqueue(mf_series* s) {
   MF_TRY(launch_rweight(c, (cufftComplex*)scratch, cmp, nz * yb, st));
   MF_CHECK_CUFFT(cufftExecC2R(P.rows_inv_all, (cufftComplex*)scratch, corr));
   const bool tc = P.prec != MF_PREC_FP32;
+  const bool op32 = !tc && P.method == 1;
   if (tc)
     MF_TRY(launch_to_half(c, corr, xb, yb, nullptr, 0, nz, P.prec, P.corr16.p, P.xpitch,
                           P.tflags.as<int>(), st));
+  else if (op32)
+    MF_TRY(launch_flag_tiles(c, corr, xb, yb, nullptr, nz, P.tflags.as<int>(), st));
   // FitRotCenterZ + RemoveOffsetZ(-1)
   MF_TRY(fit_z0(c, nz, P.zt, s->d_angles.as<float>(), s->d_sx.as<float>(), s->d_sy.as<float>(),
                 s->dev_sx64(), s->dev_sy64(), s->d_rot.as<float>(), P.d_z0.as<float>(), st));
@@ -695,7 +716,6 @@ static int pa_enqueue(mf_series* s) {
   for (int k = 0; k < n; ++k) {
     const int ip = P.order[k];
     const ReprojGeom& g = P.geom[k];
-    int* rowflags = P.d_rowflags.as<int>() + (size_t)k * P.ytiles;
     float* reproj = P.reproj.as<float>();
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k], st));
     if (tc) {
@@ -704,11 +724,12 @@ static int pa_enqueue(mf_series* s) {
       MF_TRY(launch_reproject_exact_flagged(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k],
                                             g.i0, g.nk, g.fcos, g.fsin, g.ray_len, g.thick,
                                             P.tflags.as<int>(), reproj, st));
-    } else if (P.method == 1) {
-      MF_TRY(launch_reproject_apply(c, P.ops.ops[k], corr, bpix, rowflags, reproj, st));
-      MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
-                                    g.nk, g.fcos, g.fsin, g.ray_len, g.thick, rowflags, reproj,
-                                    st));
+    } else if (op32) {
+      MF_TRY(launch_reproject_apply_group(c, P.ops, P.d_applyjobs.as<ApplyJob>() + k, nullptr, 1,
+                                          P.ops.ops[k].ntiles, yb, st));
+      MF_TRY(launch_reproject_exact_flagged(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k],
+                                            g.i0, g.nk, g.fcos, g.fsin, g.ray_len, g.thick,
+                                            P.tflags.as<int>(), reproj, st));
     } else {
       MF_TRY(launch_reproject_exact(c, corr, xb, yb, bpix, P.d_bp.as<float>() + P.bp_off[k], g.i0,
                                     g.nk, g.fcos, g.fsin, g.ray_len, g.thick, nullptr, reproj,
@@ -740,6 +761,9 @@ static int pa_enqueue(mf_series* s) {
     if (tc)
       MF_TRY(launch_to_half(c, corr, xb, yb, P.d_order.as<int>() + k, 0, 1, P.prec, P.corr16.p,
                             P.xpitch, P.tflags.as<int>(), st));
+    else if (op32)
+      MF_TRY(launch_flag_tiles(c, corr, xb, yb, P.d_order.as<int>() + k, 1, P.tflags.as<int>(),
+                               st));
     if (prof) MF_CHECK_CUDA(cudaEventRecord(P.events[3 * k + 2], st));
   }
   MF_TRY(max_err(c, P.d_err.as<float>(), P.d_order.as<int>(), n, P.d_maxerr.as<float>(), st));

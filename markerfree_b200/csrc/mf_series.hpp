@@ -49,7 +49,8 @@ struct ProjAlignState {
   DevBuf part;      // reduction partials
   DevBuf stats;     // float2 x 2
   DevBuf mask;      // yb x xb round-edge factors of the cross-correlation
-  DevBuf d_order, d_err, d_z0, d_maxerr, d_meas, d_rowflags, d_bp;
+  DevBuf d_order, d_err, d_z0, d_maxerr, d_meas, d_bp;
+  DevBuf d_applyjobs;  // FP32 operator mode: one ApplyJob per held-out tilt
   std::vector<size_t> bp_off;  // float offset of each tilt's geometry table in d_bp
   int ytiles = 0;
   cufftHandle rows_fwd_all = 0, rows_inv_all = 0, rows_fwd_one = 0, rows_inv_one = 0;
