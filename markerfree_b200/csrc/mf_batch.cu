@@ -73,14 +73,8 @@ struct mf_group {
   std::vector<TmaDesc> maps;               // per series
   std::vector<std::vector<TcJob>> tcjobs;  // per step: the series with a tilt at that step
   std::vector<cudaEvent_t> events;         // 3 per step when the context profiles
-  // A pass captured into a CUDA graph per set of active series (the set changes
-  // only when a series stops); its replay is one launch, so a slow or busy host
-  // thread cannot leave the GPU waiting between the pass's ~40 launches per step.
-  std::map<std::vector<int>, std::pair<cudaGraphExec_t, int64_t>> graphs;
-  bool use_graph = true;
   ~mf_group() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
-    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.first);
   }
 };
 
@@ -540,37 +534,7 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
     MF_CHECK_CUDA(cudaEventCreate(&e));
     g->events.push_back(e);
   }
-  // Profiled passes run eagerly (events recorded by graph nodes cannot be timed);
-  // otherwise the pass for this set of active series is captured once and replayed.
-  bool launched = false;
-  if (!c->profiling && g->use_graph) {
-    auto it = g->graphs.find(g->active);
-    if (it == g->graphs.end()) {
-      const int64_t l0 = c->launches;
-      cudaGraph_t gr = nullptr;
-      std::unique_lock<std::recursive_mutex> fft_lock(fft_mutex());
-      MF_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const int rc = group_enqueue(g);
-      const cudaError_t ec = cudaStreamEndCapture(st, &gr);
-      fft_lock.unlock();
-      const int64_t kernels = c->launches - l0;
-      c->launches = l0;
-      cudaGraphExec_t ex = nullptr;
-      if (rc == MF_OK && ec == cudaSuccess && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess) {
-        it = g->graphs.emplace(g->active, std::make_pair(ex, kernels)).first;
-      } else {
-        g->use_graph = false;  // run eagerly from now on
-      }
-      if (gr) cudaGraphDestroy(gr);
-      cudaGetLastError();
-    }
-    if (it != g->graphs.end()) {
-      MF_CHECK_CUDA(cudaGraphLaunch(it->second.first, st));
-      c->launches += it->second.second;
-      launched = true;
-    }
-  }
-  if (!launched) MF_TRY(group_enqueue(g));
+  MF_TRY(group_enqueue(g));
   std::vector<float> me(B);
   int tcerr = 0;
   MF_CHECK_CUDA(cudaMemcpyAsync(me.data(), g->d_maxerr.p, sizeof(float) * B,
