@@ -20,6 +20,7 @@
 //    the K neighbour rows to the output row, the same for every row: a banded
 //    matrix.  It is built once per series (the angles do not change while
 //    projection matching runs) and applied to all Yb rows as a dense-tiled GEMM.
+#include <atomic>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -1349,12 +1350,14 @@ __global__ void __launch_bounds__(256, 2)
 // The group apply's shared-memory size, set once per device outside any stream
 // capture (the set-up of a pass calls it before the pass is captured).
 int prepare_apply_group(Context* c) {
-  static bool attr_set[64] = {};  // per device ordinal
-  if (!attr_set[c->gpu & 63]) {
+  // per device ordinal; serving workers may get here at the same time (setting the
+  // attribute twice is harmless, the flag only saves the call)
+  static std::atomic<bool> attr_set[64] = {};
+  if (!attr_set[c->gpu & 63].load(std::memory_order_acquire)) {
     MF_CHECK_CUDA(cudaFuncSetAttribute(k_op_apply_group,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kA2SmemBytes));
-    attr_set[c->gpu & 63] = true;
+    attr_set[c->gpu & 63].store(true, std::memory_order_release);
   }
   return MF_OK;
 }

@@ -25,7 +25,8 @@
 // other requests hold memory, the request is not failed: what it allocated is
 // given back, it returns to the head of its queue, the budget drops to what the
 // other requests hold (so the scheduler learns where the device really fills),
-// and a group that failed is retried at half the size.  Only a request that
+// and a group that failed is retried at half the size (the size doubles back
+// with every group that goes through).  Only a request that
 // finds the device full with nothing else on it fails.
 #include <algorithm>
 #include <chrono>
@@ -357,6 +358,8 @@ struct mf_server {
         for (int& r : rcs) r = set_error(MF_ERR_CUDA, "stream synchronize failed");
       lk.lock();
       matching--;
+      // a group that went through lets the group size grow back after a shortage
+      if (rc == MF_OK && group_cap < kMaxGroup) group_cap = std::min(kMaxGroup, 2 * group_cap);
       groups++;
       grouped_jobs += (int64_t)group.size();
       for (size_t i = 0; i < group.size(); ++i) finish_locked(group[i], rcs[i]);
