@@ -44,6 +44,13 @@ struct GroupMember {
   // the per-step transforms, one plan per side stream of the context
   static constexpr int kS = mf_context::kFftStreams;
   cufftHandle rows_fwd_one[kS] = {}, rows_inv_one[kS] = {}, cc_fwd[kS] = {}, cc_inv[kS] = {};
+  // The parameters each tilt's corrected image was last made with (valid once a
+  // pass has run), and this pass's start values of the shifts: a pass re-corrects
+  // at its start only the tilts whose (shift, axis) changed since.
+  bool corr_valid = false;
+  std::vector<float> used_sx, used_sy, used_rot, start_sx, start_sy;
+  int pre = 1;         // this pass's start: 0 nothing to redo, 1 every tilt, 2 one tilt
+  int pre_tilt = -1;   // the tilt of pre == 2
 };
 
 }  // namespace
@@ -67,6 +74,7 @@ struct mf_group {
   std::vector<float> z0;
   // device tables
   DevBuf d_ser, d_steps, d_active, d_bp, d_applyjobs, d_maxerr, d_z0, d_err, d_meas, d_tcerr;
+  DevBuf d_full, d_pre;  // per series: re-correct every tilt at the pass start / the one tilt
   DevBuf d_order;
   ReprojOpSet ops;
   TcOpSet tcops;
@@ -216,6 +224,8 @@ static int group_setup(mf_group* g, float zshift, const int* align_z, int nproj)
   MF_TRY(g->d_order.alloc(sizeof(int) * std::max<size_t>(orders.size(), 1)));
   MF_TRY(g->d_bp.alloc(sizeof(float) * std::max<size_t>(bp.size(), 1)));
   MF_TRY(g->d_active.alloc(sizeof(int) * B));
+  MF_TRY(g->d_full.alloc(sizeof(int) * B));
+  MF_TRY(g->d_pre.alloc(sizeof(GroupStepDev) * B));
   MF_TRY(g->d_maxerr.alloc(sizeof(float) * B));
   MF_TRY(g->d_z0.alloc(sizeof(float) * B));
   MF_TRY(g->d_err.alloc(sizeof(float) * g->nz_max * B));
@@ -415,27 +425,6 @@ static int group_enqueue(mf_group* g) {
   const GroupSeriesDev* ser = g->d_ser.as<GroupSeriesDev>();
   const GroupStepDev* steps = g->d_steps.as<GroupStepDev>();
   const int* active = g->d_active.as<int>();
-  // CorrTomoStack::DoIt for every tilt of every active series
-  GroupCorrArgs ca{ser, nullptr, active, g->nz_max, 1};
-  MF_TRY(launch_correct_group(c, ca, B, g->xb_max, g->yb_max, st));
-  for (int b = 0; b < B; ++b)
-    if (g->active[b]) {
-      float* sb = g->m[b]->scratch.as<float>();
-      MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->rows_fwd_all, sb, (cufftComplex*)sb));
-    }
-  MF_TRY(launch_rweight_group(c, ser, nullptr, active, B, g->cmp_max, g->rows_max, st));
-  for (int b = 0; b < B; ++b)
-    if (g->active[b])
-      MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->rows_inv_all,
-                                  (cufftComplex*)g->m[b]->scratch.as<float>(),
-                                  g->m[b]->corr.as<float>()));
-  if (tc)
-    MF_TRY(launch_to_half_group(c, ser, nullptr, active, B, g->nz_max, g->ytiles_max, g->prec,
-                                st));
-  else
-    MF_TRY(launch_flag_tiles_group(c, ser, nullptr, active, B, g->nz_max, g->ytiles_max, st));
-  MF_TRY(fit_z0_group(c, ser, active, B, st));
-  const bool prof = c->profiling && (int)g->events.size() >= 3 * nmax;
   std::vector<TcJob> jobs;
   // A per-step FFT stage: the transforms of the series that take part run on the
   // context's side streams, forked from the stream after the work queued so far
@@ -443,11 +432,13 @@ static int group_enqueue(mf_group* g) {
   // results are those of the transforms run one after another.
   mf_context* ctx = g->ctx;
   const int nfs = mf_context::kFftStreams;
+  // (k < 0: the series whose pass start re-corrects one tilt take part)
   auto fft_stage = [&](int k, const std::function<int(GroupMember&, int)>& exec) -> int {
     MF_CHECK_CUDA(cudaEventRecord(ctx->fork_ev, st));
     int used = 0;
     for (int b = 0; b < B; ++b) {
-      if (!g->active[b] || k >= g->m[b]->n) continue;
+      if (!g->active[b]) continue;
+      if (k < 0 ? g->m[b]->pre != 2 : k >= g->m[b]->n) continue;
       const int slot = used % nfs;
       if (used < nfs) MF_CHECK_CUDA(cudaStreamWaitEvent(ctx->aux[slot], ctx->fork_ev, 0));
       MF_TRY(exec(*g->m[b], slot));
@@ -459,6 +450,54 @@ static int group_enqueue(mf_group* g) {
     }
     return MF_OK;
   };
+  // CorrTomoStack::DoIt at the pass start: every tilt of the series whose
+  // parameters changed beyond one tilt (d_full), the one changed tilt of the
+  // others (d_pre; the same kernels and plans as a step's re-correction), nothing
+  // for a series whose corrected stack is current
+  const int* full = g->d_full.as<int>();
+  GroupCorrArgs ca{ser, nullptr, full, g->nz_max, 1};
+  MF_TRY(launch_correct_group(c, ca, B, g->xb_max, g->yb_max, st));
+  for (int b = 0; b < B; ++b)
+    if (g->active[b] && g->m[b]->pre == 1) {
+      float* sb = g->m[b]->scratch.as<float>();
+      MF_CHECK_CUFFT(cufftExecR2C(g->m[b]->rows_fwd_all, sb, (cufftComplex*)sb));
+    }
+  MF_TRY(launch_rweight_group(c, ser, nullptr, full, B, g->cmp_max, g->rows_max, st));
+  for (int b = 0; b < B; ++b)
+    if (g->active[b] && g->m[b]->pre == 1)
+      MF_CHECK_CUFFT(cufftExecC2R(g->m[b]->rows_inv_all,
+                                  (cufftComplex*)g->m[b]->scratch.as<float>(),
+                                  g->m[b]->corr.as<float>()));
+  if (tc)
+    MF_TRY(launch_to_half_group(c, ser, nullptr, full, B, g->nz_max, g->ytiles_max, g->prec,
+                                st));
+  else
+    MF_TRY(launch_flag_tiles_group(c, ser, nullptr, full, B, g->nz_max, g->ytiles_max, st));
+  bool any_one = false;
+  for (int b = 0; b < B; ++b) any_one |= g->active[b] && g->m[b]->pre == 2;
+  if (any_one) {
+    const GroupStepDev* pre = g->d_pre.as<GroupStepDev>();
+    GroupCorrArgs rc{ser, pre, active, g->nz_max, 1};
+    MF_TRY(launch_correct_group(c, rc, B, g->xb_max, g->yb_max, st));
+    MF_TRY(fft_stage(-1, [&](GroupMember& M, int i) -> int {
+      float* rb = M.recorr.as<float>();
+      MF_CHECK_CUFFT(cufftExecR2C(M.rows_fwd_one[i], rb, (cufftComplex*)rb));
+      return MF_OK;
+    }));
+    MF_TRY(launch_rweight_group(c, ser, pre, active, B, g->cmp_max, g->yb_max, st));
+    MF_TRY(fft_stage(-1, [&](GroupMember& M, int i) -> int {
+      MF_CHECK_CUFFT(cufftExecC2R(M.rows_inv_one[i], (cufftComplex*)M.recorr.as<float>(),
+                                  M.corr.as<float>() + (size_t)M.pre_tilt * M.bpix));
+      return MF_OK;
+    }));
+    if (tc)
+      MF_TRY(launch_to_half_group(c, ser, pre, active, B, g->nz_max, g->ytiles_max, g->prec,
+                                  st));
+    else
+      MF_TRY(launch_flag_tiles_group(c, ser, pre, active, B, g->nz_max, g->ytiles_max, st));
+  }
+  MF_TRY(fit_z0_group(c, ser, active, B, st));
+  const bool prof = c->profiling && (int)g->events.size() >= 3 * nmax;
   for (int k = 0; k < nmax; ++k) {
     const GroupStepDev* sk = steps + (size_t)k * B;
     if (prof) MF_CHECK_CUDA(cudaEventRecord(g->events[3 * k], st));
@@ -529,6 +568,36 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
   for (int b = 0; b < B; ++b) MF_TRY(g->ser[b]->upload_params());
   MF_CHECK_CUDA(cudaMemcpyAsync(g->d_active.p, g->active.data(), sizeof(int) * B,
                                 cudaMemcpyHostToDevice, st));
+  // what the pass start has to re-correct, per active series: the tilts whose
+  // (shift, axis) differ from those their corrected image was made with
+  std::vector<int> full(B, 0);
+  std::vector<GroupStepDev> pre(B);
+  for (int b = 0; b < B; ++b) {
+    GroupMember& M = *g->m[b];
+    const mf_series* s = g->ser[b];
+    memset(&pre[b], 0, sizeof(GroupStepDev));
+    pre[b].ip = -1;
+    if (!active[b]) continue;
+    M.pre = 1;
+    if (M.corr_valid) {
+      int changed = 0, last = -1;
+      for (int i = 0; i < M.nz; ++i)
+        if (s->sx[i] != M.used_sx[i] || s->sy[i] != M.used_sy[i] || s->rot[i] != M.used_rot[i]) {
+          ++changed;
+          last = i;
+        }
+      M.pre = changed == 0 ? 0 : changed == 1 ? 2 : 1;
+      M.pre_tilt = last;
+    }
+    full[b] = M.pre == 1;
+    if (M.pre == 2) pre[b].ip = M.pre_tilt;
+    M.start_sx = s->sx;
+    M.start_sy = s->sy;
+  }
+  MF_CHECK_CUDA(cudaMemcpyAsync(g->d_full.p, full.data(), sizeof(int) * B, cudaMemcpyHostToDevice,
+                                st));
+  MF_CHECK_CUDA(cudaMemcpyAsync(g->d_pre.p, pre.data(), sizeof(GroupStepDev) * B,
+                                cudaMemcpyHostToDevice, st));
   while (c->profiling && (int)g->events.size() < 3 * g->nmax) {
     cudaEvent_t e;
     MF_CHECK_CUDA(cudaEventCreate(&e));
@@ -551,6 +620,16 @@ static int group_doit(mf_group* g, const int* active, float* max_err) {
     if (active[b]) {
       max_err[b] = me[b];
       g->ser[b]->pa.z0 = g->z0[b];
+      // every held-out tilt was re-corrected at its step with its final shift; the
+      // zero tilt keeps the image made at the pass start, with the start shift
+      GroupMember& M = *g->m[b];
+      const mf_series* s = g->ser[b];
+      M.used_sx = s->sx;
+      M.used_sy = s->sy;
+      M.used_rot = s->rot;
+      M.used_sx[M.zt] = M.start_sx[M.zt];
+      M.used_sy[M.zt] = M.start_sy[M.zt];
+      M.corr_valid = true;
     }
   // compulsory bytes and MACs of this pass's re-projection launches: per step, the
   // images and output of every series taking part, each distinct operator once
