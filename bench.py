@@ -126,7 +126,7 @@ SEED0 = 2000  # series j of a step uses seed SEED0 + j
 # Projection-matching passes per series of this workload, the FP32 library path's
 # mean over the seeds SEED0 .. SEED0 + 7 (bench runs report the live count as
 # `passes_per_series`); the CPU restatement's series time is scaled with it.
-PASSES_PER_SERIES = 6.0
+PASSES_PER_SERIES = 6.5
 
 
 def make_batch(n: int, device, scale: float = 1.0):
