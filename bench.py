@@ -705,7 +705,7 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if prec == 0 else f"{args.precision} operands, f32 accumulation",
-            "data": "synthetic (seeded phantom series, BASELINE shapes)",
+            "data": "synthetic (seeded phantom series)",
             "config": cfg,
             "e2e": {"value": e2e_value, "unit": "series/min",
                     "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
