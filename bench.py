@@ -769,7 +769,8 @@ def run_kernel_case(args):
     re-projects one held-out tilt (full size, 10 neighbours) with the banded
     operator; `xcorr` measures one cross-correlation shift; `axis` runs one
     tilt-axis search (100 candidates over 20 degrees); `pass` runs projection-
-    matching passes of a group of --batch series in --precision."""
+    matching passes of a group of --batch series in --precision; `coarse`
+    pre-processes and coarsely aligns one series per step."""
     import torch
     import markerfree_b200 as mf
     s = make_batch(1, "cuda:0", args.scale)[0]
@@ -803,6 +804,16 @@ def run_kernel_case(args):
         grp.close()
         print(json.dumps({"kernel_case": "pass", "series": len(sers), "tilts": nz}))
         return 0
+    if args.kernel_case == "coarse":
+        # pre-processing and coarse alignment of one series per step (stretch
+        # cross-correlations, three tilt-axis searches, the offset search)
+        for _ in range(args.steps):
+            ser = mf.Series(ctx, s.stack, ang)
+            ser.coarse_align(0.0, 0.0)
+            ser.close()
+        ctx.sync()
+        print(json.dumps({"kernel_case": "coarse", "tilts": nz}))
+        return 0
     if args.kernel_case == "axis":
         ser = mf.Series(ctx, s.stack, ang)
         p = ser.get_param()
@@ -826,7 +837,7 @@ def run_kernel_case(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr", "axis", "pass"],
+    ap.add_argument("--kernel-case", default=None, choices=["reproject", "xcorr", "axis", "pass", "coarse"],
                     help="run one stage alone (profiling)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
